@@ -1,0 +1,262 @@
+"""Case generator: emits the reference solver's own setup files.
+
+A case directory holds ``input.txt`` (the positional format parsed by
+``airpore::airpore``, airpore.cpp:17-316) and the axis files
+``coordi_air{1,2,3}.dat`` (header ``IMAX IMAX1 IMAX2 JMAX JMAX1 JMAX2 KMAX
+KMAX1 KMAX2 IJKMAX`` in file 1, then one coordinate per node; read by
+``calculation_2D::calculation_2D``, calculation_2D.cpp:44-204).  When the
+south face is porous (input line 4, second code = 3) the porous grid gets
+``coordi_pore{1,2,3}.dat`` in the same format; the reference repository
+does not ship those files, so they are always generated here.
+
+Axis convention is the reference's: X = i (transverse, Front/Back faces),
+Y = j (range / propagation, West/East faces, moving-frame axis),
+Z = k (height, South = ground, North = top).
+
+The line layout written by :func:`Case.input_text` mirrors the shipped
+``input.txt`` line for line, because the reference parser skips comment
+lines positionally (``infile.ignore(100, '\\n')``).
+"""
+
+from __future__ import annotations
+
+import dataclasses
+import math
+import os
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence, Tuple
+
+# Boundary codes of input line 4 (airpore.cpp:52-159).
+RIGID, PML, POROUS, RADIATION, TDBC = 1, 2, 3, 4, 5
+
+
+def _fmt(x: float) -> str:
+    """Shortest text that parses back to exactly the same double."""
+    if isinstance(x, int):
+        return str(x)
+    r = repr(float(x))
+    return r
+
+
+def uniform_axis(n: int, start: float, step: float) -> List[float]:
+    return [start + i * step for i in range(n)]
+
+
+@dataclass
+class Case:
+    """Every field of input.txt plus the three air axes (and porous axes)."""
+
+    X: List[float]
+    Y: List[float]
+    Z: List[float]
+    # PML node counts in the coordi header (IMAX1, IMAX2, JMAX1, JMAX2, KMAX1, KMAX2)
+    pml_nodes: Tuple[int, int, int, int, int, int] = (0, 0, 0, 0, 0, 0)
+    ijkmax: Optional[int] = None  # whole-domain JMAX for the moving frame; default = len(Y)
+    gauss_width: float = 0.3  # line 1: Gaussian FWHM (m)
+    # line 2: moving frame JMAX lead_DJ trail_DJ Judge ratio
+    mf_jmax: Optional[int] = None
+    mf_lead: int = 11
+    mf_trail: int = 11
+    mf_judge: int = 0
+    mf_ratio: float = 0.75
+    scheme: int = 2  # line 3: 1 FB_v_p, 2 FB_p_v
+    # line 4: North South East West Front Back
+    bc: Tuple[int, int, int, int, int, int] = (PML, RIGID, PML, PML, PML, PML)
+    time_domain: int = 100  # line 6
+    out_difft: int = 100000
+    fft_m: int = 12
+    frequency: float = 300.0
+    velocity_coef: float = 0.0  # line 8
+    velocity_method: int = 4  # 4 = no wind (air.cpp:102-105,170-174,231-235)
+    gamma: float = 1.4  # line 9
+    P0: float = 1.0e5
+    c0: float = 340.0
+    pml_x: Tuple[float, float] = (2.0, 1000.0)  # line 10: alpha, sigma_max
+    pml_y: Tuple[float, float, int] = (2.0, 1000.0, 0)  # line 11: + y1 activation step
+    pml_z: Tuple[float, float] = (2.0, 1000.0)  # line 12
+    pore: Tuple[float, float, float] = (1.3416407864998738, 0.3, 2.0e5)  # line 13: q, porosity, sigma
+    source: Tuple[float, float, float] = (0.0, 0.0, 0.0)  # line 14 (X, Y, Z)
+    receiver: Tuple[float, float, float] = (0.0, 0.0, 0.0)
+    dt: float = 1e-5  # line 16
+    dxyz: Optional[Tuple[float, float, float]] = None  # line 17; default from the axes
+    restart: Tuple[int, int, str] = (0, 1000000, "ct003")  # line 22
+    # line 24: curve_judge a..l curve_points ; lines 25-27 hill/canopy/trunk (q, porosity, sigma)
+    curve: Tuple[float, ...] = (0,) + (0.0,) * 12 + (0,)
+    hill: Tuple[float, float, float] = (1.79, 0.877, 5.0e4)
+    canopy: Tuple[float, float, float] = (1.79, 0.877, 5.0e4)
+    trunk: Tuple[float, float, float] = (0.52, 0.5712, 8.0e4)
+    hill_box: Tuple[float, float, float, float, float, float] = (0.0,) * 6  # line 29
+    # porous grid (only when the south code is POROUS)
+    pore_Z: Optional[List[float]] = None
+    pore_X: Optional[List[float]] = None
+    pore_Y: Optional[List[float]] = None
+    pore_dxyz: Optional[Tuple[float, float, float]] = None  # line 32
+
+    # ------------------------------------------------------------------ #
+    @property
+    def NI(self) -> int:
+        return len(self.X)
+
+    @property
+    def NJ(self) -> int:
+        return len(self.Y)
+
+    @property
+    def NK(self) -> int:
+        return len(self.Z)
+
+    @property
+    def porous_south(self) -> bool:
+        return self.bc[1] == POROUS
+
+    def spacing(self) -> Tuple[float, float, float]:
+        if self.dxyz is not None:
+            return self.dxyz
+        return (self.X[1] - self.X[0], self.Y[1] - self.Y[0], self.Z[1] - self.Z[0])
+
+    def input_text(self) -> str:
+        mf_jmax = self.mf_jmax if self.mf_jmax is not None else self.NJ
+        dx, dy, dz = self.spacing()
+        c = self.curve
+        curve_txt = " ".join([str(int(c[0]))] + [_fmt(v) for v in c[1:13]] + [str(int(c[13]))])
+        lines = [
+            f"{_fmt(self.gauss_width)} //gaussian_width",
+            f"{mf_jmax} {self.mf_lead} {self.mf_trail} {self.mf_judge} {_fmt(self.mf_ratio)} //moving frame",
+            f"{self.scheme} //scheme",
+            " ".join(str(b) for b in self.bc) + " //North South East West Front Back",
+            "//B.C type: 1 rigid 2 PML 3 porous 4 radiation 5 TDBC",
+            f"{self.time_domain} {self.out_difft} {self.fft_m} {_fmt(self.frequency)} //time_domain out_difft FFT_m frequency",
+            "",
+            f"{_fmt(self.velocity_coef)} {self.velocity_method} //wind b, method",
+            f"{_fmt(self.gamma)} {_fmt(self.P0)} {_fmt(self.c0)} //gamma P0 c0",
+            f"{_fmt(self.pml_x[0])} {_fmt(self.pml_x[1])} //PMLx",
+            f"{_fmt(self.pml_y[0])} {_fmt(self.pml_y[1])} {int(self.pml_y[2])} //PMLy",
+            f"{_fmt(self.pml_z[0])} {_fmt(self.pml_z[1])} //PMLz",
+            " ".join(_fmt(v) for v in self.pore) + " //pore q porosity sigma",
+            " ".join(_fmt(v) for v in (*self.source, *self.receiver)) + " //source receiver",
+            "",
+            f"{_fmt(self.dt)} //dt",
+            f"{_fmt(dx)} {_fmt(dy)} {_fmt(dz)} //dx dy dz",
+            "",
+            "1 1 1 //mpi dims",
+            "",
+            "output.data;",
+            f"{self.restart[0]} {self.restart[1]} {self.restart[2]}",
+            "",
+            curve_txt + " //curve",
+            " ".join(_fmt(v) for v in self.hill) + " //hill",
+            " ".join(_fmt(v) for v in self.canopy) + " //canopy",
+            " ".join(_fmt(v) for v in self.trunk) + " //trunk",
+            "",
+            " ".join(_fmt(v) for v in self.hill_box) + " //box",
+            "",
+            "porous_media;",
+        ]
+        if self.porous_south:
+            pd = self.pore_dxyz if self.pore_dxyz is not None else (dx, dy, dz)
+            lines.append(" ".join(_fmt(v) for v in pd) + " //pore dx dy dz")
+        else:
+            lines.append("0 0 0")
+        for ln in lines:
+            # ignore(100, '\n') skips at most 100 characters past the last value
+            assert len(ln) < 95, ln
+        return "\n".join(lines) + "\n"
+
+    def coordi_texts(self, prefix: str = "coordi_air") -> dict:
+        I1, I2, J1, J2, K1, K2 = self.pml_nodes
+        ijk = self.ijkmax if self.ijkmax is not None else self.NJ
+        head = f"{self.NI} {I1} {I2} {self.NJ} {J1} {J2} {self.NK} {K1} {K2} {ijk}"
+        return {
+            f"{prefix}1.dat": head + "\n" + " ".join(_fmt(v) for v in self.X) + "\n",
+            f"{prefix}2.dat": " ".join(_fmt(v) for v in self.Y) + "\n",
+            f"{prefix}3.dat": " ".join(_fmt(v) for v in self.Z) + "\n",
+        }
+
+    def pore_coordi_texts(self) -> dict:
+        Xp = self.pore_X if self.pore_X is not None else self.X
+        Yp = self.pore_Y if self.pore_Y is not None else self.Y
+        Zp = self.pore_Z
+        ijk = self.ijkmax if self.ijkmax is not None else len(Yp)
+        head = f"{len(Xp)} 0 0 {len(Yp)} 0 0 {len(Zp)} 0 0 {ijk}"
+        return {
+            "coordi_pore1.dat": head + "\n" + " ".join(_fmt(v) for v in Xp) + "\n",
+            "coordi_pore2.dat": " ".join(_fmt(v) for v in Yp) + "\n",
+            "coordi_pore3.dat": " ".join(_fmt(v) for v in Zp) + "\n",
+        }
+
+    def write(self, case_dir: str) -> str:
+        os.makedirs(case_dir, exist_ok=True)
+        files = {"input.txt": self.input_text()}
+        files.update(self.coordi_texts())
+        if self.porous_south:
+            if self.pore_Z is None:
+                raise ValueError("porous south face needs pore_Z")
+            files.update(self.pore_coordi_texts())
+        for name, txt in files.items():
+            with open(os.path.join(case_dir, name), "w") as f:
+                f.write(txt)
+        return case_dir
+
+
+def write_receivers(path: str, receivers: Sequence[Tuple[float, float, float]]) -> str:
+    with open(path, "w") as f:
+        for r in receivers:
+            f.write(" ".join(_fmt(v) for v in r) + "\n")
+    return path
+
+
+# ---------------------------------------------------------------------- #
+# Named workloads.  BASELINE "x" (range) maps to reference Y/j, BASELINE "y"
+# (transverse) to X/i, "z" to Z/k.
+# ---------------------------------------------------------------------- #
+
+def plain_box(ni=48, nj=96, nk=48, d=0.05, steps=500, pml=10):
+    """Plain reference method on a Cartesian box: rigid ground, PML on the
+    other five faces, Gaussian pulse (amplitude 1 Pa, FWHM 6 d) at
+    (X, Y, Z) = (1.2, 0.6, 0.3) m, receivers at Z = 0.3 m, X = 1.2 m,
+    Y = 1.5/2.5/3.5/4.2 m.  96 x 48 x 48 nodes, d = 0.05 m, c0 = 343 m/s,
+    rho0 = 1.2 kg/m^3, CFL 0.5, 500 steps."""
+    c0, rho0, gamma = 343.0, 1.2, 1.4
+    P0 = rho0 * c0 * c0 / gamma
+    case = Case(
+        X=uniform_axis(ni, 0.0, d), Y=uniform_axis(nj, 0.0, d), Z=uniform_axis(nk, 0.0, d),
+        pml_nodes=(pml, pml, pml, pml, 0, pml),
+        gauss_width=6 * d, bc=(PML, RIGID, PML, PML, PML, PML), time_domain=steps,
+        gamma=gamma, P0=P0, c0=c0, pml_y=(2.0, 1000.0, 0),
+        source=(1.2, 0.6, 0.3), receiver=(1.2, 1.5, 0.3), dt=0.5 * d / c0,
+    )
+    receivers = [(1.2, y, 0.3) for y in (1.5, 2.5, 3.5, 4.2)]
+    return case, receivers
+
+
+def porous_ground(ni=128, nj=256, nk=96, layer=16, d=0.05, steps=4000, pml=20, seed=0,
+                  sigma=2.0e5, porosity=0.3, tortuosity=1.8):
+    """Air box over a Zwikker-Kosten porous layer coupled through the
+    two-plane airpore interface (calculation_2D.cpp:865-985): 256 x 128 x 96
+    air nodes, a 16-cell-deep porous grid with the same X/Y nodes and
+    layer+2 Z nodes, 20-node PML on the five air faces, 8 receivers on a line
+    at 1 m height.  The source position is drawn from ``seed`` (height
+    uniform in 0.2-1 m)."""
+    import random
+
+    rng = random.Random(seed)
+    c0, rho0, gamma = 343.0, 1.2, 1.4
+    P0 = rho0 * c0 * c0 / gamma
+    Y = uniform_axis(nj, 0.0, d)
+    X = uniform_axis(ni, 0.0, d)
+    Z = uniform_axis(nk, 0.0, d)
+    pore_Z = uniform_axis(layer + 2, -layer * d, d)  # pore k=layer is Z=0 (= air k=0)
+    Xc = X[ni // 2]
+    src = (Xc, Y[pml] + 10 * d + rng.uniform(0.0, 1.0) * 10 * d, rng.uniform(0.2, 1.0))
+    rec_y0 = src[1] + 1.0
+    receivers = [(Xc, min(rec_y0 + r * (Y[nj - pml - 2] - rec_y0) / 7.0, Y[nj - pml - 2]), 1.0)
+                 for r in range(8)]
+    case = Case(
+        X=X, Y=Y, Z=Z, pml_nodes=(pml, pml, pml, pml, 0, pml),
+        gauss_width=6 * d, bc=(PML, POROUS, PML, PML, PML, PML), time_domain=steps,
+        gamma=gamma, P0=P0, c0=c0, pml_y=(2.0, 1000.0, 0),
+        pore=(math.sqrt(tortuosity), porosity, sigma),
+        source=src, receiver=receivers[0], dt=0.5 * d / c0,
+        pore_Z=pore_Z, pore_dxyz=(d, d, d),
+    )
+    return case, receivers

@@ -1,0 +1,156 @@
+"""Small generated cases that exercise every feature of the reference's
+time-marching path.  Shared by the oracle pin tests (CPU) and the GPU parity
+tests.  Each builder returns ``(Case, receivers)``; sizes keep the oracle
+to well under a second per case."""
+
+from __future__ import annotations
+
+import importlib
+import math
+from typing import Callable, Dict, List, Tuple
+
+casegen = importlib.import_module("3d_mpi_test_b200.casegen")
+Case = casegen.Case
+uniform_axis = casegen.uniform_axis
+RIGID, PML, POROUS, TDBC = casegen.RIGID, casegen.PML, casegen.POROUS, casegen.TDBC
+
+D = 0.05
+C0 = 343.0
+
+
+def _base(ni=20, nj=28, nk=18, steps=40, pml=5, bc=(PML, RIGID, PML, PML, PML, PML), **kw) -> Case:
+    gamma, rho0 = 1.4, 1.2
+    P0 = rho0 * C0 * C0 / gamma
+    pml_nodes = kw.pop("pml_nodes", (pml, pml, pml, pml, pml if bc[1] == PML else 0, pml))
+    c = Case(
+        X=uniform_axis(ni, 0.0, D), Y=uniform_axis(nj, 0.0, D), Z=uniform_axis(nk, 0.0, D),
+        pml_nodes=pml_nodes, gauss_width=6 * D, bc=bc, time_domain=steps, gamma=gamma, P0=P0, c0=C0,
+        source=(0.5, 0.55, 0.3), receiver=(0.5, 0.9, 0.3), dt=0.5 * D / C0, **kw,
+    )
+    return c
+
+
+REC = [(0.5, 0.9, 0.3), (0.45, 1.1, 0.4), (0.3, 0.6, 0.15)]
+
+
+def pml_rigid():
+    return _base(), REC
+
+
+def tdbc_east():
+    return _base(bc=(PML, RIGID, TDBC, PML, PML, PML), pore=(1.79, 0.877, 5.1e4)), REC
+
+
+def porous_ground():
+    layer = 6
+    c = _base(bc=(PML, POROUS, PML, PML, PML, PML), pore=(math.sqrt(1.8), 0.3, 2.0e5))
+    c.pore_Z = uniform_axis(layer + 2, -layer * D, D)
+    c.pore_dxyz = (D, D, D)
+    c.source = (0.5, 0.55, 0.15)
+    return c, REC + [(0.5, 0.7, 0.05)]
+
+
+def porous_tdbc_fine_pore():
+    """Porous ground with a finer porous z spacing (ratio 2 < 5 keeps the
+    two-plane coupling) plus the east TDBC."""
+    layer = 8
+    c = _base(bc=(PML, POROUS, TDBC, PML, RIGID, PML), pore=(1.5, 0.5, 3.0e4))
+    c.pore_Z = uniform_axis(layer + 2, -layer * D / 2, D / 2)
+    c.pore_dxyz = (D, D, D / 2)
+    c.source = (0.5, 0.55, 0.1)
+    return c, REC
+
+
+def south_pml_all_faces():
+    return _base(bc=(PML, PML, PML, PML, PML, PML)), REC
+
+
+def front_only_pml():
+    # Front alone selects the x2 slab (high-i side): airpore.cpp:93-95,199-212
+    return _base(bc=(PML, RIGID, PML, PML, PML, RIGID)), REC
+
+
+def back_only_pml():
+    return _base(bc=(RIGID, RIGID, RIGID, PML, RIGID, PML)), REC
+
+
+def all_rigid():
+    return _base(bc=(RIGID,) * 6, pml_nodes=(0,) * 6), REC
+
+
+def wind_linear():
+    return _base(velocity_coef=3.0, velocity_method=1), REC
+
+
+def wind_log():
+    return _base(velocity_coef=1.5, velocity_method=5), REC
+
+
+def wind_vortex():
+    return _base(velocity_coef=0.0, velocity_method=2), REC
+
+
+def hill(judge: int):
+    def build():
+        c = _base(nk=20)
+        box = (0.2, 0.8, 0.7, 1.2, 0.0, 0.5)
+        curves = {
+            1: (1, 0.0, 0.2, 0.5, 0.95, 0.15, 0, 0, 0, 0, 0, 0, 0, 0),  # sphere r=0.2 at (0.5,0.95,0.15)
+            2: (2, 0.35, 0.65, 0.8, 1.05, 0.0, 0.3, 0, 0, 0, 0, 0, 0, 0),  # box
+            3: (3, 0.08, 0.2, 0.4, 0.8, 0.3, 0.6, 0.85, 0.25, 0.5, 0.9, 0.2, 0, 2),  # rows of cylinders
+            4: (4, 0.07, 0.3, 0.8, 0.15, 0.2, 3, 2, 0, 0, 0, 0, 0, 0),  # cylinder array
+        }
+        if judge == 5:
+            # tree centred at (0, 3) m in the reference's hard-coded geometry (air.cpp:1097-1114)
+            c.X = uniform_axis(24, -0.6, D)
+            c.Y = uniform_axis(30, 2.3, D)
+            c.Z = uniform_axis(40, 0.0, D)
+            c.source = (0.0, 2.6, 1.0)
+            box = (-0.55, 0.5, 2.4, 3.6, 0.0, 1.85)
+            c.curve = (5,) + (0.0,) * 12 + (0,)
+            c.hill_box = box
+            rec = [(0.0, 3.3, 1.0), (0.1, 2.9, 0.8)]
+            return c, rec
+        c.curve = curves[judge]
+        c.hill_box = box
+        return c, REC
+
+    build.__name__ = f"hill{judge}"
+    return build
+
+
+def moving_frame():
+    """Window of 24 j-nodes over a 44-node range, frames of trail_DJ-1 = 5
+    cells (calculation_2D.cpp:405-496, air.cpp:2447-2730)."""
+    c = _base(nj=24, steps=60, pml_nodes=(5, 5, 5, 5, 0, 5))
+    c.Y = uniform_axis(44, 0.0, D)
+    c.mf_jmax, c.mf_lead, c.mf_trail, c.mf_judge, c.mf_ratio = 24, 6, 6, 1, 0.75
+    c.ijkmax = 44
+    c.source = (0.5, 0.4, 0.3)
+    return c, [(0.5, 0.8, 0.3), (0.5, 1.4, 0.3), (0.5, 1.9, 0.35)]
+
+
+def fb_v_p():
+    c = _base(scheme=1, bc=(PML, RIGID, TDBC, PML, PML, PML))
+    return c, REC
+
+
+def delayed_y1():
+    return _base(pml_y=(2.0, 1000.0, 17)), REC
+
+
+def stretched():
+    """Non-uniform axes: the 1D metric terms X_over_x etc. vary per node."""
+    c = _base()
+    c.X = [0.05 * i + 0.002 * math.sin(0.7 * i) for i in range(20)]
+    c.Y = [0.05 * j + 0.01 * (j / 27.0) ** 2 for j in range(28)]
+    c.Z = [0.05 * k * (1.0 + 0.01 * k) for k in range(18)]
+    return c, REC
+
+
+CASES: Dict[str, Callable[[], Tuple[Case, List]]] = {
+    f.__name__: f
+    for f in [pml_rigid, tdbc_east, porous_ground, porous_tdbc_fine_pore, south_pml_all_faces, front_only_pml,
+              back_only_pml, all_rigid, wind_linear, wind_log, wind_vortex, hill(1), hill(2), hill(3), hill(4),
+              hill(5), moving_frame, fb_v_p, delayed_y1, stretched]
+}
