@@ -1,0 +1,217 @@
+"""B200-native time-marching path of the azhang22/3D_MPI_TEST outdoor-sound
+FDTD solver (linearized Euler with mean wind, Zwikker-Kosten porous ground,
+PML, 6-pole TDBC, moving frame), behind the C ABI in include/fdtd_b200.h.
+
+Python here is a thin host mirror of the reference's ``airpore`` driver
+(airpore.h:24-68): :class:`Airpore` is built from a reference case directory
+(``input.txt`` + ``coordi_*.dat``) and exposes ``get_output`` (the time loop,
+airpore.cpp:400-641), ``Cal_pressure`` / ``Cal_velocity`` (the half steps,
+airpore.cpp:324-398) and field read-out.  All compute runs in the native
+library ``lib/libfdtd_b200.so`` on an sm_100a device; there is no CPU path.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional, Sequence, Tuple
+
+import numpy as np
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG_DIR, "lib", "libfdtd_b200.so")
+
+FDTD_OK = 0
+FDTD_ERR_INPUT = -1
+FDTD_ERR_UNSUPPORTED = -2
+FDTD_ERR_CUDA = -3
+FDTD_ERR_NONFINITE = -4
+FDTD_ERR_ARG = -5
+FDTD_ERR_STATE = -6
+F64, F32 = 0, 1
+
+# Every function declared in include/fdtd_b200.h.
+EXPORTS = (
+    "fdtd_create", "fdtd_destroy", "fdtd_dims", "fdtd_last_error", "fdtd_set_receivers", "fdtd_reset",
+    "fdtd_run", "fdtd_advance", "fdtd_step_pressure", "fdtd_step_velocity", "fdtd_get_field",
+    "fdtd_set_field", "fdtd_get_psi", "fdtd_get_slab", "fdtd_state_elems", "fdtd_copy_state",
+    "fdtd_launch_count", "fdtd_last_device_ms",
+)
+
+
+class FdtdError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+_LIBS = {}
+
+
+def load_library(path: Optional[str] = None) -> ctypes.CDLL:
+    """Load the native library and declare the C ABI signatures.  Raises if
+    the library has not been built: there is no fallback implementation."""
+    path = path or LIB_PATH
+    if path in _LIBS:
+        return _LIBS[path]
+    if not os.path.exists(path):
+        raise FdtdError(FDTD_ERR_CUDA, f"native library missing: {path} (run __graft_entry__.build())")
+    L = ctypes.CDLL(path)
+    vp, ip, dp, i, cp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double), \
+        ctypes.c_int, ctypes.c_char_p
+    sig = {
+        "fdtd_create": ([cp, i, i, ctypes.POINTER(vp)], i),
+        "fdtd_destroy": ([vp], i),
+        "fdtd_dims": ([vp, ip], i),
+        "fdtd_last_error": ([], cp),
+        "fdtd_set_receivers": ([vp, i, dp, ip], i),
+        "fdtd_reset": ([vp, i], i),
+        "fdtd_run": ([vp, i, dp], i),
+        "fdtd_advance": ([vp, i, dp], i),
+        "fdtd_step_pressure": ([vp], i),
+        "fdtd_step_velocity": ([vp], i),
+        "fdtd_get_field": ([vp, i, i, dp], i),
+        "fdtd_set_field": ([vp, i, i, dp], i),
+        "fdtd_get_psi": ([vp, dp], i),
+        "fdtd_get_slab": ([vp, i, i, dp, ip], i),
+        "fdtd_state_elems": ([vp], ctypes.c_size_t),
+        "fdtd_copy_state": ([vp, i, vp], i),
+        "fdtd_launch_count": ([vp], ctypes.c_longlong),
+        "fdtd_last_device_ms": ([vp, dp], i),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+    _LIBS[path] = L
+    return L
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+_COMP = {"p": 0, "u": 1, "v": 2, "w": 3}
+_SLABS = ("x1", "x2", "y1", "y2", "z1", "z2")
+
+
+class Airpore:
+    """Host mirror of the reference's ``airpore`` object on one device.
+
+    ``precision``: "f64" (parity path) or "f32" (FP32 fields and stencil,
+    FP64 TDBC state and receiver series)."""
+
+    def __init__(self, case_dir: str, precision: str = "f64", device: int = 0, lib_path: Optional[str] = None):
+        self._L = load_library(lib_path)
+        self._h = ctypes.c_void_p()
+        prec = {"f64": F64, "f32": F32}[precision]
+        self._check(self._L.fdtd_create(case_dir.encode(), prec, device, ctypes.byref(self._h)))
+        self.precision = precision
+        d = (ctypes.c_int * 12)()
+        self._check(self._L.fdtd_dims(self._h, d))
+        (self.I, self.J, self.K, self.has_pore, self.pI, self.pJ, self.pK, self.NG, self.time_domain, _,
+         self.scheme, _) = list(d)
+        self.nrec = 0
+
+    # ------------------------------------------------------------------
+    def _check(self, rc: int) -> int:
+        if rc < 0:
+            raise FdtdError(rc, self._L.fdtd_last_error().decode())
+        return rc
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            self._L.fdtd_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ------------------------------------------------------------------
+    def set_receivers(self, xyz: Sequence[Tuple[float, float, float]]) -> np.ndarray:
+        """calculation_2D::get_position for each (X, Y, Z); returns indices."""
+        a = np.ascontiguousarray(np.asarray(xyz, dtype=np.float64).reshape(-1, 3))
+        idx = np.zeros((a.shape[0], 3), dtype=np.int32)
+        self._check(self._L.fdtd_set_receivers(self._h, a.shape[0], _dp(a),
+                                               idx.ctypes.data_as(ctypes.POINTER(ctypes.c_int))))
+        self.nrec = a.shape[0]
+        return idx
+
+    def reset(self, horizon: int = 0) -> None:
+        self._check(self._L.fdtd_reset(self._h, horizon))
+
+    def get_output(self, nsteps: Optional[int] = None) -> np.ndarray:
+        """The reference time loop (airpore::get_output) for ``nsteps`` steps
+        (default: input.txt's time_domain) from t = 0; returns receiver p(t)
+        as [nsteps, n_receivers] FP64."""
+        n = self.time_domain if nsteps is None else nsteps
+        out = np.zeros((n, max(self.nrec, 1)), dtype=np.float64)
+        self._check(self._L.fdtd_run(self._h, n, _dp(out)))
+        return out[:, : self.nrec]
+
+    def advance(self, nsteps: int) -> np.ndarray:
+        out = np.zeros((nsteps, max(self.nrec, 1)), dtype=np.float64)
+        self._check(self._L.fdtd_advance(self._h, nsteps, _dp(out)))
+        return out[:, : self.nrec]
+
+    def Cal_pressure(self) -> None:
+        self._check(self._L.fdtd_step_pressure(self._h))
+
+    def Cal_velocity(self) -> None:
+        self._check(self._L.fdtd_step_velocity(self._h))
+
+    # ------------------------------------------------------------------
+    def field(self, name: str, medium: str = "air", level: str = "n") -> np.ndarray:
+        m = {"air": 0, "pore": 1}[medium]
+        comp = _COMP[name] + (4 if level == "nn" else 0)
+        shape = (self.I, self.J, self.K) if m == 0 else (self.pI, self.pJ, self.pK)
+        out = np.zeros(shape, dtype=np.float64)
+        self._check(self._L.fdtd_get_field(self._h, m, comp, _dp(out)))
+        return out
+
+    def set_field(self, name: str, arr: np.ndarray, medium: str = "air") -> None:
+        m = {"air": 0, "pore": 1}[medium]
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        self._check(self._L.fdtd_set_field(self._h, m, _COMP[name], _dp(a)))
+
+    def psi(self) -> np.ndarray:
+        out = np.zeros((self.I, self.K, 6), dtype=np.float64)
+        self._check(self._L.fdtd_get_psi(self._h, _dp(out)))
+        return out
+
+    def slabs(self):
+        res = {}
+        for s, name in enumerate(_SLABS):
+            dims = (ctypes.c_int * 3)()
+            if not self._check(self._L.fdtd_get_slab(self._h, s, 0, None, dims)):
+                continue
+            q = {}
+            for c, cname in enumerate("uvwp"):
+                a = np.zeros(tuple(dims), dtype=np.float64)
+                self._check(self._L.fdtd_get_slab(self._h, s, c, _dp(a), dims))
+                q[cname] = a
+            res[name] = q
+        return res
+
+    def state_elems(self) -> int:
+        return int(self._L.fdtd_state_elems(self._h))
+
+    def copy_state(self, host: np.ndarray, to_device: bool) -> None:
+        self._check(self._L.fdtd_copy_state(self._h, 1 if to_device else 0, host.ctypes.data_as(ctypes.c_void_p)))
+
+    def launch_count(self) -> int:
+        return int(self._L.fdtd_launch_count(self._h))
+
+    def last_device_ms(self) -> float:
+        v = ctypes.c_double()
+        self._check(self._L.fdtd_last_device_ms(self._h, ctypes.byref(v)))
+        return v.value

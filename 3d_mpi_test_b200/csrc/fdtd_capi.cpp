@@ -1,0 +1,146 @@
+// extern "C" boundary of the B200 FDTD path (declarations: include/fdtd_b200.h).
+// Maps C++ exceptions to status codes and keeps a per-thread error message.
+#include <cstring>
+#include <exception>
+#include <new>
+#include <string>
+
+#include "../../include/fdtd_b200.h"
+#include "fdtd_solver.hpp"
+
+struct fdtd_solver {
+    fdtd::Solver* s;
+};
+
+namespace {
+thread_local std::string g_last_error;
+
+template <typename F>
+int guard(F&& f) {
+    try {
+        f();
+        return FDTD_OK;
+    } catch (const fdtd::SolverError& e) {
+        g_last_error = e.msg;
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        g_last_error = "host allocation failed";
+        return FDTD_ERR_CUDA;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return FDTD_ERR_ARG;
+    }
+}
+
+int bad(const char* msg) {
+    g_last_error = msg;
+    return FDTD_ERR_ARG;
+}
+}  // namespace
+
+extern "C" {
+
+const char* fdtd_last_error(void) { return g_last_error.c_str(); }
+
+int fdtd_create(const char* case_dir, int precision, int device, fdtd_solver** out) {
+    if (!case_dir || !out) return bad("null argument");
+    *out = nullptr;
+    return guard([&] {
+        fdtd::Solver* s = new fdtd::Solver(case_dir, precision, device);
+        *out = new fdtd_solver{s};
+    });
+}
+
+int fdtd_destroy(fdtd_solver* h) {
+    if (!h) return FDTD_OK;
+    int rc = guard([&] { delete h->s; });
+    delete h;
+    return rc;
+}
+
+int fdtd_dims(const fdtd_solver* h, int* dims) {
+    if (!h || !dims) return bad("null argument");
+    return guard([&] {
+        const auto d = h->s->dims();
+        for (int q = 0; q < FDTD_NDIMS; ++q) dims[q] = d[q];
+    });
+}
+
+int fdtd_set_receivers(fdtd_solver* h, int n, const double* xyz, int* idx_out) {
+    if (!h || (n > 0 && !xyz) || n < 0) return bad("bad receiver arguments");
+    return guard([&] {
+        std::vector<double> v(xyz, xyz + 3 * n);
+        const std::vector<int> idx = h->s->set_receivers(v);
+        if (idx_out) std::memcpy(idx_out, idx.data(), sizeof(int) * idx.size());
+    });
+}
+
+int fdtd_reset(fdtd_solver* h, int horizon) {
+    if (!h) return bad("null handle");
+    return guard([&] { h->s->reset(horizon); });
+}
+
+int fdtd_run(fdtd_solver* h, int nsteps, double* rec_out) {
+    if (!h || nsteps < 0) return bad("bad run arguments");
+    return guard([&] { h->s->run(nsteps, rec_out); });
+}
+
+int fdtd_advance(fdtd_solver* h, int nsteps, double* rec_out) {
+    if (!h || nsteps < 0) return bad("bad advance arguments");
+    int taken = 0;
+    int rc = guard([&] { taken = h->s->advance(nsteps, rec_out); });
+    if (rc == FDTD_OK && taken < nsteps) {
+        g_last_error = "time loop reached its horizon";
+        return FDTD_ERR_STATE;
+    }
+    return rc;
+}
+
+int fdtd_step_pressure(fdtd_solver* h) {
+    if (!h) return bad("null handle");
+    return guard([&] { h->s->step_pressure(); });
+}
+
+int fdtd_step_velocity(fdtd_solver* h) {
+    if (!h) return bad("null handle");
+    return guard([&] { h->s->step_velocity(); });
+}
+
+int fdtd_get_field(fdtd_solver* h, int medium, int comp, double* out) {
+    if (!h || !out) return bad("null argument");
+    return guard([&] { h->s->get_field(medium, comp, out); });
+}
+
+int fdtd_set_field(fdtd_solver* h, int medium, int comp, const double* in) {
+    if (!h || !in) return bad("null argument");
+    return guard([&] { h->s->set_field(medium, comp, in); });
+}
+
+int fdtd_get_psi(fdtd_solver* h, double* out) {
+    if (!h || !out) return bad("null argument");
+    return guard([&] { h->s->get_psi(out); });
+}
+
+int fdtd_get_slab(fdtd_solver* h, int s, int comp, double* out, int* dims) {
+    if (!h || !dims) return bad("null argument");
+    int present = 0;
+    int rc = guard([&] { present = h->s->get_slab(s, comp, out, dims); });
+    return rc == FDTD_OK ? present : rc;
+}
+
+size_t fdtd_state_elems(const fdtd_solver* h) { return h ? h->s->state_elems() : 0; }
+
+int fdtd_copy_state(fdtd_solver* h, int dir, void* host) {
+    if (!h || !host || (dir != 0 && dir != 1)) return bad("bad copy_state arguments");
+    return guard([&] { h->s->copy_state(dir, host); });
+}
+
+long long fdtd_launch_count(const fdtd_solver* h) { return h ? h->s->launch_count() : 0; }
+
+int fdtd_last_device_ms(const fdtd_solver* h, double* ms) {
+    if (!h || !ms) return bad("null argument");
+    *ms = h->s->last_device_ms();
+    return FDTD_OK;
+}
+
+}  // extern "C"

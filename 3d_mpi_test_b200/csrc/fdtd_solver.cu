@@ -1,0 +1,1016 @@
+// Host side of the B200 FDTD time-marching path: builds one device-resident
+// domain from the reference's setup files and drives the time loop.
+//
+// Setup restates, in host FP64, the reference's per-frame geometry:
+// calculation_2D::SetMovingFrame metrics (calculation_2D.cpp:405-433),
+// air::cal_PML_var (air.cpp:509-937), air::cal_hill_var (air.cpp:938-1122),
+// air::SetWindProfile (air.cpp:1286-1304), the porous constants
+// (porous.cpp:40-51) and the TDBC constants (calculation_2D.cpp:1012-1028,
+// airpore.cpp:252-254). Only 1D profiles, 2D wind and a box mask go to the
+// device; the per-node 3D Jacobian and wind arrays of the reference are not
+// materialised.
+#include "fdtd_solver.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <cuda_runtime.h>
+
+#include "fdtd_device.cuh"
+
+namespace fdtd {
+
+namespace {
+
+#define FDTD_CK(x)                                                                                   \
+    do {                                                                                             \
+        cudaError_t e_ = (x);                                                                        \
+        if (e_ != cudaSuccess)                                                                       \
+            throw SolverError{-3, std::string(#x) + ": " + cudaGetErrorString(e_)};                 \
+    } while (0)
+
+[[noreturn]] void fail(int code, const std::string& msg) { throw SolverError{code, msg}; }
+
+// TDBC poles of the reference (calculation_2D.h:73-75)
+const double kTdA[6] = {8.226223820e-01, 3.732304064e-01, 9.106232372e-02,
+                        4.819445335e-02, 4.225250937e-01, 1.837970986e-01};
+const double kTdR[6] = {8.681310138e-01, 1.953722814e-01, 1.108067950e-02,
+                        2.566498621e-03, 1.457297589e-04, 4.648583789e-02};
+
+struct Medium {
+    int I = 0, J = 0, K = 0;
+    double dx = 1, dy = 1, dz = 1;
+    std::vector<double> X, Z, axY, Y;  // axY: file axis (window), Y: current frame
+    std::vector<double> fx, fy, fz;    // derivative factors x_over_X*rdx etc.
+
+    void compute_x() { fx = factor(X, dx); }
+    void compute_y() { fy = factor(Y, dy); }
+    void compute_z() { fz = factor(Z, dz); }
+    // X_over_x = (X[i+1]-X[i-1]) * (1/dx) * 0.5; with fixed-zero cross
+    // metrics x_over_X = 1/X_over_x (calculation_2D.cpp:416-433, df_over_var.cpp:5-9)
+    static std::vector<double> factor(const std::vector<double>& a, double d) {
+        const int n = static_cast<int>(a.size());
+        std::vector<double> f(n, 0.0);
+        const double rd = 1.0 / d;
+        for (int q = 1; q < n - 1; ++q) {
+            const double m = (a[q + 1] - a[q - 1]) * rd * 0.5;
+            f[q] = rd / m;
+        }
+        return f;
+    }
+};
+
+// SpeedProfile (air.cpp:71-253) for the methods whose parameters the
+// reference initialises. Returns false for methods 3 and 6, which read
+// members the reference never sets.
+bool wind_at(int method, double b, double y, double z, double& U, double& V, double& W) {
+    U = V = W = 0.0;
+    switch (method) {
+        case 1:
+            V = z >= 2.8 ? b * 2.8 : (z >= 0.0 ? b * z : 0.0);
+            return true;
+        case 2: {
+            const double Rr = std::sqrt(std::pow(y - 5.0, 2) + std::pow(z - 2.0, 2));
+            double alpha;
+            if (std::fabs(y - 5.0) <= 1.0e-6 && std::fabs(z - 2.0) <= 1.0e-6) alpha = 0.0;
+            else if (y - 5.0 >= 0.0) alpha = std::asin((y - 5.0) / Rr);
+            else alpha = std::asin((y - 5.0) / Rr) + 3.1415926;
+            V = -1.0 * 2.0 / (Rr + 2.0) * std::sin(alpha);
+            W = 1.0 * 2.0 / (Rr + 2.0) * std::cos(alpha);
+            return true;
+        }
+        case 3:
+        case 6:
+            return false;
+        case 5:
+            U = b * y;
+            V = b * std::log(std::fabs(z) / 0.1 + 1);
+            W = b * y;
+            return true;
+        default:
+            return true;  // 4 and any other code: no wind
+    }
+}
+
+template <typename T>
+T* dalloc(size_t n) {
+    T* p = nullptr;
+    if (n == 0) n = 1;
+    FDTD_CK(cudaMalloc(&p, n * sizeof(T)));
+    FDTD_CK(cudaMemset(p, 0, n * sizeof(T)));
+    return p;
+}
+
+}  // namespace
+
+class SolverImplBase {
+   public:
+    virtual ~SolverImplBase() = default;
+    ReferenceInput in;
+    virtual std::array<int, 12> dims() const = 0;
+    virtual std::vector<int> set_receivers(const std::vector<double>& xyz) = 0;
+    virtual int n_receivers() const = 0;
+    virtual void reset(int horizon) = 0;
+    virtual int advance(int nsteps, double* rec_out) = 0;
+    virtual void step_pressure() = 0;
+    virtual void step_velocity() = 0;
+    virtual void get_field(int medium, int comp, double* out) = 0;
+    virtual void set_field(int medium, int comp, const double* in) = 0;
+    virtual void get_psi(double* out) = 0;
+    virtual int get_slab(int s, int comp, double* out, int* dims) = 0;
+    virtual size_t state_elems() const = 0;
+    virtual void copy_state(int dir, void* host) = 0;
+    virtual long long launch_count() const = 0;
+    virtual double last_device_ms() const = 0;
+};
+
+template <typename R>
+class SolverImpl final : public SolverImplBase {
+   public:
+    SolverImpl(const std::string& dir, int device) {
+        std::string e = parse_reference_case(dir, in);
+        if (!e.empty()) fail(-1, e);
+        device_ = device;
+        FDTD_CK(cudaSetDevice(device_));
+        cudaDeviceProp prop{};
+        FDTD_CK(cudaGetDeviceProperties(&prop, device_));
+        if (prop.major != 10) fail(-3, "this build targets sm_100a (B200); device is sm_" + std::to_string(prop.major) +
+                                           std::to_string(prop.minor));
+        validate_and_build_geometry();
+        allocate();
+        FDTD_CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+        FDTD_CK(cudaEventCreate(&ev0_));
+        FDTD_CK(cudaEventCreate(&ev1_));
+        reset(in.time_domain);
+    }
+
+    ~SolverImpl() override {
+        cudaSetDevice(device_);
+        if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+        for (void* p : allocs_) cudaFree(p);
+        if (ev0_) cudaEventDestroy(ev0_);
+        if (ev1_) cudaEventDestroy(ev1_);
+        if (stream_) cudaStreamDestroy(stream_);
+    }
+
+    // ----------------------------------------------------------- setup
+    void validate_and_build_geometry() {
+        if (in.case_no != 1) fail(-2, "north face must be rigid or PML (the reference only steps CaseNo 1)");
+        if (in.scheme != FB_P_V && in.scheme != FB_V_P)
+            fail(-2, "only the forward-backward schemes (1 FB_v_p, 2 FB_p_v) are implemented by the reference");
+        if (in.south != BT_RIGID && in.south != BT_ABSORBING && in.south != BT_POROUS)
+            fail(-2, "south face must be rigid, PML or porous ground");
+        if (in.mf.lead_DJ < 2) fail(-2, "moving-frame lead_DJ must be >= 2");
+        if (in.mf.Judge == 1 && (in.mf.trail_DJ < 1 || in.mf.trail_DJ > in.mf.lead_DJ))
+            fail(-2, "moving frame needs 1 <= trail_DJ <= lead_DJ (the reference shift reads past the window otherwise)");
+        if (in.velocity_method == 3 || in.velocity_method == 6)
+            fail(-2, "wind methods 3 and 6 read uninitialised profile parameters in the reference");
+        const AxisFile& A = in.air;
+        mf_ = in.mf;
+        int J = A.JMAX, IJK = A.IJKMAX;
+        if (mf_.Judge == 1) {  // calculation_2D.cpp:58-68
+            if ((IJK - mf_.JMAX) % (mf_.lead_DJ - 1) != 0) {
+                const int nl = (IJK - mf_.JMAX) / (mf_.lead_DJ - 1);
+                IJK = mf_.JMAX + (nl + 1) * (mf_.lead_DJ - 1);
+            }
+            J = mf_.JMAX;
+            if (J > A.JMAX) fail(-1, "coordi_air2.dat holds fewer nodes than the moving-frame window");
+        } else {
+            mf_.JMAX = J;
+            IJK = J;
+        }
+        ijkmax_ = IJK;
+        air_.I = A.IMAX; air_.J = J; air_.K = A.KMAX;
+        if (air_.I < 3 || air_.J < 5 || air_.K < 3) fail(-2, "air grid needs at least 3 x 5 x 3 nodes");
+        air_.dx = in.dx; air_.dy = in.dy; air_.dz = in.dz;
+        air_.X = A.X;
+        air_.Z = A.Z;
+        air_.axY.assign(A.Y.begin(), A.Y.begin() + J);
+        air_.Y = air_.axY;
+        air_.compute_x(); air_.compute_y(); air_.compute_z();
+        porous_ = in.has_pore;
+        if (porous_) {
+            const AxisFile& P = in.pore_axes;
+            if (P.IMAX != air_.I || (mf_.Judge == 1 ? P.JMAX < J : P.JMAX != J))
+                fail(-2, "porous grid must share the air grid's I and J node counts");
+            if (P.KMAX < 3) fail(-2, "porous grid needs at least 3 z nodes");
+            if (static_cast<int>(in.dz / in.pdz) >= 5)
+                fail(-2, "air/porous z-spacing ratio >= 5: the reference's coarse/fine coupling is disabled code");
+            pore_.I = P.IMAX; pore_.J = J; pore_.K = P.KMAX;
+            pore_.dx = in.pdx; pore_.dy = in.pdy; pore_.dz = in.pdz;
+            pore_.X = P.X;
+            pore_.Z = P.Z;
+            pore_.axY.assign(P.Y.begin(), P.Y.begin() + J);
+            pore_.Y = pore_.axY;
+            pore_.compute_x(); pore_.compute_y(); pore_.compute_z();
+        }
+        NI_ = air_.I;
+        NJ_ = air_.J;
+        Kair_ = air_.K;
+        if (porous_) {
+            gAir0_ = pore_.K - 1;
+            gOff_ = pore_.K - 2;
+            NG_ = (pore_.K - 1) + (air_.K - 1);
+        } else {
+            gAir0_ = 0;
+            gOff_ = 0;
+            NG_ = air_.K;
+        }
+        build_pml_static();
+        build_hill();
+        // TDBC constants: t_bar = dt / tau (airpore.cpp:333, calculation_2D.cpp:1012-1028)
+        tdbc_ = in.east == BT_TDBC;
+        const double tb = in.dt / in.tau;
+        double at = 0.0;
+        for (int q = 0; q < 6; ++q) {
+            td_e_[q] = std::exp(-1 * kTdR[q] * tb);
+            td_adt_[q] = kTdA[q] * tb;
+            at += kTdA[q] * tb;
+        }
+        td_den_ = 1.0 / (1 + at);
+        // wind presence (any non-zero value on frame 0)
+        wind_on_ = false;
+        for (int k = 0; k < Kair_ && !wind_on_; ++k)
+            for (int j = 0; j < NJ_ && !wind_on_; ++j) {
+                double U, V, W;
+                wind_at(in.velocity_method, in.velocity_coef, air_.Y[j], air_.Z[k], U, V, W);
+                if (U != 0.0 || V != 0.0 || W != 0.0) wind_on_ = true;
+            }
+    }
+
+    void build_pml_static() {
+        const AxisFile& A = in.air;
+        jx_ = in.pml_judge_x; jy_ = in.pml_judge_y; jz_ = in.pml_judge_z;
+        I1_ = A.IMAX1; I2_ = A.IMAX2; Y1_ = A.JMAX1; Y2_ = A.JMAX2; K1_ = A.KMAX1; K2_ = A.KMAX2;
+        if (jx_ == 0) I1_ = I2_ = 0;
+        if (jx_ == 1) I2_ = 0;
+        if (jx_ == 2) I1_ = 0;
+        if (jy_ == 0) Y1_ = Y2_ = 0;
+        if (jy_ == 1) Y2_ = 0;
+        if (jy_ == 2) Y1_ = 0;
+        if (jz_ == 0) K1_ = K2_ = 0;
+        if (jz_ == 1) K2_ = 0;
+        if (jz_ == 2) K1_ = 0;
+        auto chk = [&](int n1, int n2, int N, const char* ax) {
+            if ((n1 != 0 && n1 < 2) || (n2 != 0 && n2 < 2))
+                fail(-2, std::string("PML along ") + ax + " needs at least 2 nodes per layer");
+            if (n1 + n2 > N - 1) fail(-2, std::string("PML layers along ") + ax + " overlap");
+        };
+        chk(I1_, I2_, NI_, "x");
+        chk(Y1_, Y2_, NJ_, "y");
+        chk(K1_, K2_, Kair_, "z");
+        // widths and layer starts from the file axes (air.cpp:534-869)
+        const std::vector<double>& X = air_.X;
+        const std::vector<double>& Z = air_.Z;
+        const std::vector<double>& aY = air_.axY;
+        if (I1_) { W1_ = 1.0 / std::fabs(X[I1_ - 1] - X[0]); x1_ = X[I1_ - 1]; }
+        if (I2_) { W2_ = 1.0 / std::fabs(X[NI_ - 1] - X[NI_ - I2_]); x2_ = X[NI_ - I2_]; }
+        if (Y1_) { L1_ = 1.0 / std::fabs(aY[Y1_ - 1] - aY[0]); }
+        if (Y2_) { L2_ = 1.0 / std::fabs(aY[NJ_ - 1] - aY[NJ_ - Y2_]); }
+        if (K1_) { H1_ = 1.0 / std::fabs(Z[K1_ - 1] - Z[0]); z1_ = Z[K1_ - 1]; }
+        if (K2_) { H2_ = 1.0 / std::fabs(Z[Kair_ - 1] - Z[Kair_ - K2_]); z2_ = Z[Kair_ - K2_]; }
+        pml_y_time_ = (jy_ == 1 || jy_ == 3) ? in.pml_y_time : 0;
+        // x and z profiles never change with the frame
+        prof(NI_, I1_, I2_, in.pml_x_sigma, in.pml_x_alpha,
+             [&](int i) { return (x1_ - X[i]) * W1_; }, [&](int i) { return (X[i] - x2_) * W2_; }, sx_, fx_, gx_, sdx_);
+        prof(Kair_, K1_, K2_, in.pml_z_sigma, in.pml_z_alpha,
+             [&](int k) { return (z1_ - Z[k]) * H1_; }, [&](int k) { return (Z[k] - z2_) * H2_; }, sz_, fz_, gz_, sdz_);
+    }
+
+    template <typename F1, typename F2>
+    static void prof(int n, int n1, int n2, double smax, double alpha, F1 d1, F2 d2, std::vector<double>& s,
+                     std::vector<double>& f, std::vector<double>& g, std::vector<int8_t>& side) {
+        s.assign(n, 0.0); f.assign(n, 0.0); g.assign(n, 0.0); side.assign(n, 0);
+        for (int q = 0; q < n; ++q) {
+            double dn;
+            int sd;
+            if (q < n1) { dn = d1(q); sd = 1; }
+            else if (n2 > 0 && q >= n - n2) { dn = d2(q); sd = 2; }
+            else continue;
+            const double pw = std::pow(dn, alpha);
+            const double sig = smax * pw;
+            const double beta = 1.0 + 25.0 * pw;
+            s[q] = sig;
+            f[q] = 1.0 - 1.0 / beta;
+            g[q] = 1.0 / beta - 1.0;
+            side[q] = static_cast<int8_t>(sd);
+        }
+    }
+
+    // y profile and layer starts for frame N (air::SetWindProfile shifts PML_y1/y2, air.cpp:1289-1292)
+    void build_pml_y(int N) {
+        const double sh = N * (mf_.trail_DJ - 1) * air_.dy;
+        const std::vector<double>& aY = air_.axY;
+        if (Y1_) y1_ = (N != 0) ? aY[Y1_ - 1] + sh : aY[Y1_ - 1];
+        if (Y2_) y2_ = (N != 0) ? aY[NJ_ - Y2_] + sh : aY[NJ_ - Y2_];
+        const std::vector<double>& Y = air_.Y;
+        prof(NJ_, Y1_, Y2_, in.pml_y_sigma, in.pml_y_alpha, [&](int j) { return (y1_ - Y[j]) * L1_; },
+             [&](int j) { return (Y[j] - y2_) * L2_; }, sy_, fy_, gy_, sdy_);
+    }
+
+    // porous inclusion mask, air::cal_hill_var (air.cpp:938-1122)
+    void build_hill() {
+        mask_on_ = false;
+        if (in.curve_judge == 0) return;
+        const double* c = in.curve;
+        const std::vector<double>& X = air_.X;
+        const std::vector<double>& Y = air_.axY;
+        const std::vector<double>& Z = air_.Z;
+        int is = 0, ie = 0, js = 0, je = 0, ks = 0, ke = 0;
+        for (int i = 0; i < NI_; i++) {
+            if (std::fabs(X[i] - in.hill_box[0]) <= in.dx / 8.0) is = i;
+            if (std::fabs(X[i] - in.hill_box[1]) <= in.dx / 8.0) { ie = i; break; }
+        }
+        for (int j = 0; j < NJ_; j++) {
+            if (std::fabs(Y[j] - in.hill_box[2]) <= in.dy / 8.0) js = j;
+            if (std::fabs(Y[j] - in.hill_box[3]) <= in.dy / 8.0) { je = j; break; }
+        }
+        for (int k = 0; k < Kair_; k++) {
+            if (std::fabs(Z[k] - in.hill_box[4]) <= in.dz / 8.0) ks = k;
+            if (std::fabs(Z[k] - in.hill_box[5]) <= in.dz / 8.0) { ke = k; break; }
+        }
+        if (ie < is || je < js || ke < ks) return;
+        mi0_ = is; mi1_ = ie; mj0_ = js; mj1_ = je; mk0_ = ks; mk1_ = ke;
+        const int ni = ie - is + 1, nj = je - js + 1, nk = ke - ks + 1;
+        mask_.assign(static_cast<size_t>(ni) * nj * nk, 0);
+        auto at = [&](int i, int j, int k) -> int8_t& {
+            return mask_[(static_cast<size_t>(k - ks) * ni + (i - is)) * nj + (j - js)];
+        };
+        int ii = 0, jj = 0;
+        for (int i = is; i <= ie; i++)
+            for (int j = js; j <= je; j++)
+                for (int k = ks; k <= ke; k++) {
+                    int8_t& m = at(i, j, k);
+                    double len;
+                    switch (in.curve_judge) {
+                        case 1:  // sphere (c, d, e), radius b
+                            len = std::pow(X[i] - c[2], 2) + std::pow(Y[j] - c[3], 2) + std::pow(Z[k] - c[4], 2);
+                            if (std::sqrt(len) <= c[1]) m = 1;
+                            break;
+                        case 2:  // axis-aligned box
+                            if (X[i] >= c[0] && X[i] <= c[1] && Y[j] >= c[2] && Y[j] <= c[3] && Z[k] >= c[4] &&
+                                Z[k] <= c[5])
+                                m = 1;
+                            break;
+                        case 3:  // three rows of vertical cylinders, spacing b, radius a
+                            for (jj = 0; jj < in.curve_points; jj++) {
+                                len = std::pow(X[i] - c[2], 2) + std::pow(Y[j] - (c[3] + jj * c[1]), 2);
+                                if (std::sqrt(len) <= c[0] && Z[k] <= c[4]) m = 1;
+                                len = std::pow(X[i] - c[5], 2) + std::pow(Y[j] - (c[6] + jj * c[1]), 2);
+                                if (std::sqrt(len) <= c[0] && Z[k] <= c[7]) m = 1;
+                                len = std::pow(X[i] - c[8], 2) + std::pow(Y[j] - (c[9] + jj * c[1]), 2);
+                                if (std::sqrt(len) <= c[0] && Z[k] <= c[10]) m = 1;
+                            }
+                            break;
+                        case 4:  // g x f array of cylinders
+                            for (ii = 0; ii < c[6]; ii++)
+                                for (jj = 0; jj < c[5]; jj++) {
+                                    len = std::pow(X[i] - (c[1] + ii * c[4]), 2) +
+                                          std::pow(Y[j] - (c[2] + jj * c[3]), 2);
+                                    if (std::sqrt(len) <= c[0]) m = 1;
+                                }
+                            break;
+                        case 5:  // one tree at (0, 3): cone canopy (1) and trunk (2)
+                            for (ii = 0; ii < 1; ii++)
+                                for (jj = 0; jj < 1; jj++) {
+                                    len = std::pow(X[i] - (0.0 + ii * 2.0), 2) + std::pow(Y[j] - (3.0 + jj * 2.0), 2);
+                                    const double h = -25 / (9 - 1e-50) * std::sqrt(len) + 3.0;
+                                    if (std::sqrt(len) <= 0.9 && Z[k] <= h && Z[k] >= 0.5) m = 1;
+                                    if (std::sqrt(len) <= 0.1 && Z[k] <= 1.5) m = 2;
+                                }
+                            break;
+                        default:
+                            break;
+                    }
+                }
+        if (in.curve_judge == 5) {
+            // the reference's second trunk sweep reuses the finished loop counters (ii = jj = 1)
+            for (int i = is; i <= ie; i++)
+                for (int j = js; j <= je; j++)
+                    for (int k = ks; k <= ke; k++) {
+                        const double len =
+                            std::pow(X[i] - (0.0 + ii * 2.0), 2) + std::pow(Y[j] - (3.0 + jj * 2.0), 2);
+                        if (std::sqrt(len) <= 0.1 && Z[k] <= 1.5) at(i, j, k) = 2;
+                    }
+        }
+        if (in.curve_judge < 1 || in.curve_judge > 5) return;
+        mask_on_ = true;
+        // mask 1 uses the canopy parameters and mask 2 the trunk's (air.cpp:966-980, 1910-1944)
+        const double dt = in.dt;
+        const double e1 = 1.0 / in.canopy.eff_density, e2 = 1.0 / in.trunk.eff_density;
+        const double ib1 = 1.0 / (1.0 + in.canopy.resistivity * dt * e1);
+        const double ib2 = 1.0 / (1.0 + in.trunk.resistivity * dt * e2);
+        m1_ = {ib1 * dt * e1, ib1, dt / in.canopy.Kp / in.canopy.porosity};
+        m2_ = {ib2 * dt * e2, ib2, dt / in.trunk.Kp / in.trunk.porosity};
+    }
+
+    // ------------------------------------------------------- device
+    template <typename T>
+    T* track(T* p) {
+        allocs_.push_back(p);
+        return p;
+    }
+
+    void allocate() {
+        const size_t N = static_cast<size_t>(NI_) * NJ_ * NG_;
+        nodes_ = N;
+        for (int b = 0; b < 2; ++b)
+            for (int c = 0; c < 4; ++c) F_[b][c] = track(dalloc<R>(N));
+        // slabs: x1 x2 y1 y2 z1 z2
+        SlabDesc sd[6];
+        sd[0] = {0, 0, 0, I1_ ? I1_ + 1 : 0, NJ_, Kair_};
+        sd[1] = {NI_ - 1 - I2_, 0, 0, I2_ ? I2_ + 1 : 0, NJ_, Kair_};
+        sd[2] = {0, 0, 0, NI_, Y1_ ? Y1_ + 1 : 0, Kair_};
+        sd[3] = {0, NJ_ - 1 - Y2_, 0, NI_, Y2_ ? Y2_ + 1 : 0, Kair_};
+        sd[4] = {0, 0, 0, NI_, NJ_, K1_ ? K1_ + 1 : 0};
+        sd[5] = {0, 0, Kair_ - 1 - K2_, NI_, NJ_, K2_ ? K2_ + 1 : 0};
+        for (int s = 0; s < 6; ++s) {
+            slab_[s] = sd[s];
+            const size_t n = static_cast<size_t>(sd[s].ni) * sd[s].nj * sd[s].nk;
+            slab_n_[s] = n;
+            for (int b = 0; b < 2; ++b)
+                for (int c = 0; c < 4; ++c) Q_[s][b][c] = n ? track(dalloc<R>(n)) : nullptr;
+        }
+        d_axA_ = track(dalloc<R>(NI_)); d_ayA_ = track(dalloc<R>(NJ_));
+        d_axP_ = track(dalloc<R>(NI_)); d_ayP_ = track(dalloc<R>(NJ_));
+        d_azG_ = track(dalloc<R>(NG_));
+        for (int q = 0; q < 3; ++q) {
+            d_sx_[q] = track(dalloc<R>(NI_));
+            d_sy_[q] = track(dalloc<R>(NJ_));
+            d_sz_[q] = track(dalloc<R>(Kair_));
+        }
+        d_sdx_ = track(dalloc<int8_t>(NI_)); d_sdy_ = track(dalloc<int8_t>(NJ_)); d_sdz_ = track(dalloc<int8_t>(Kair_));
+        const size_t W = static_cast<size_t>(NJ_) * Kair_;
+        d_Uw_ = track(dalloc<R>(W)); d_Vw_ = track(dalloc<R>(W)); d_Ww_ = track(dalloc<R>(W));
+        d_mask_ = mask_on_ ? track(dalloc<int8_t>(mask_.size())) : nullptr;
+        if (mask_on_) FDTD_CK(cudaMemcpy(d_mask_, mask_.data(), mask_.size(), cudaMemcpyHostToDevice));
+        const size_t P = static_cast<size_t>(NI_) * Kair_ * 6;
+        d_psi_[0] = track(dalloc<double>(P)); d_psi_[1] = track(dalloc<double>(P));
+        d_rec_node_ = track(dalloc<long long>(kMaxRec));
+        d_counters_ = track(dalloc<int>(2));
+        d_status_ = track(dalloc<int>(1));
+        // static profiles
+        upload(d_axA_, air_.fx);
+        upload(d_axP_, porous_ ? pore_.fx : air_.fx);
+        upload(d_sx_[0], sx_); upload(d_sx_[1], fx_); upload(d_sx_[2], gx_);
+        upload(d_sz_[0], sz_); upload(d_sz_[1], fz_); upload(d_sz_[2], gz_);
+        FDTD_CK(cudaMemcpy(d_sdx_, sdx_.data(), NI_, cudaMemcpyHostToDevice));
+        FDTD_CK(cudaMemcpy(d_sdz_, sdz_.data(), Kair_, cudaMemcpyHostToDevice));
+        std::vector<double> az(NG_, 0.0);
+        for (int g = 0; g < NG_; ++g) az[g] = (g < gAir0_) ? pore_.fz[g] : air_.fz[g - gOff_];
+        upload(d_azG_, az);
+    }
+
+    void upload(R* dst, const std::vector<double>& src) {
+        std::vector<R> t(src.begin(), src.end());
+        FDTD_CK(cudaMemcpy(dst, t.data(), t.size() * sizeof(R), cudaMemcpyHostToDevice));
+    }
+
+    // frame-dependent data: Y, y metrics, y PML profile, wind, receivers
+    void upload_frame(int N) {
+        const double sh = N * (mf_.trail_DJ - 1);
+        for (int j = 0; j < NJ_; ++j) air_.Y[j] = (N != 0) ? air_.axY[j] + sh * air_.dy : air_.axY[j];
+        air_.compute_y();
+        upload(d_ayA_, air_.fy);
+        if (porous_) {
+            for (int j = 0; j < NJ_; ++j) pore_.Y[j] = (N != 0) ? pore_.axY[j] + sh * pore_.dy : pore_.axY[j];
+            pore_.compute_y();
+            upload(d_ayP_, pore_.fy);
+        } else {
+            upload(d_ayP_, air_.fy);
+        }
+        build_pml_y(N);
+        upload(d_sy_[0], sy_); upload(d_sy_[1], fy_); upload(d_sy_[2], gy_);
+        FDTD_CK(cudaMemcpy(d_sdy_, sdy_.data(), NJ_, cudaMemcpyHostToDevice));
+        if (wind_on_) {
+            const size_t W = static_cast<size_t>(NJ_) * Kair_;
+            std::vector<double> U(W), V(W), Wv(W);
+            for (int k = 0; k < Kair_; ++k)
+                for (int j = 0; j < NJ_; ++j) {
+                    const size_t q = static_cast<size_t>(k) * NJ_ + j;
+                    wind_at(in.velocity_method, in.velocity_coef, air_.Y[j], air_.Z[k] - 0.0, U[q], V[q], Wv[q]);
+                }
+            upload(d_Uw_, U); upload(d_Vw_, V); upload(d_Ww_, Wv);
+        }
+        frame_N_ = N;
+        upload_receivers();
+    }
+
+    void upload_receivers() {
+        std::vector<long long> node(kMaxRec, -1);
+        const int sh = frame_N_ * (mf_.trail_DJ - 1);
+        for (size_t r = 0; r < rec_idx_.size(); ++r) {
+            const int ii = rec_idx_[r][0], jj = rec_idx_[r][1], kk = rec_idx_[r][2];
+            // calculation_2D::get_pressure: strict interior of the current window
+            if (jj >= sh && jj < NJ_ + sh) {
+                const int jl = jj - sh;
+                if (jl > 0 && jl < NJ_ - 1 && ii > 0 && ii < NI_ - 1 && kk > 0 && kk < Kair_ - 1)
+                    node[r] = static_cast<long long>((static_cast<size_t>(kk + gOff_) * NI_ + ii) * NJ_ + jl);
+            }
+        }
+        FDTD_CK(cudaMemcpy(d_rec_node_, node.data(), sizeof(long long) * kMaxRec, cudaMemcpyHostToDevice));
+    }
+
+    std::vector<int> set_receivers(const std::vector<double>& xyz) override {
+        const int n = static_cast<int>(xyz.size() / 3);
+        if (n > kMaxRec) fail(-5, "at most 64 receivers");
+        rec_idx_.assign(n, {0, 0, 0});
+        std::vector<int> out(3 * n);
+        const std::vector<double>& X = air_.X;
+        const std::vector<double>& Y = air_.axY;
+        const std::vector<double>& Z = air_.Z;
+        const double Yf = Y[NJ_ - 1] - Y[0];
+        for (int r = 0; r < n; ++r) {  // calculation_2D::get_position + airpore.cpp:454-457
+            const double rx = xyz[3 * r], ry = xyz[3 * r + 1], rz = xyz[3 * r + 2];
+            int ii = 0, jj = 0, kk = 0;
+            const int N = static_cast<int>(ry / Yf + 1.0e-6);
+            for (int i = 0; i < NI_; i++)
+                if (rx - X[i] <= in.dx / 8.0) { ii = i; break; }
+            const int NN = N * (NJ_ - 1);
+            bool found_k = false;
+            if (NN < ijkmax_) {
+                for (int j = NN; j < ijkmax_ && j - NN < NJ_; j++)
+                    if (ry - N * Yf - Y[j - NN] <= in.dy / 8.0) { jj = j; break; }
+                for (int k = 0; k < Kair_; k++)
+                    if (rz - Z[k] <= in.dz / 8.0) { kk = k; found_k = true; break; }
+            }
+            if (!found_k) ii = jj = kk = 0;
+            if (ii == 0 && jj == 0 && kk == 0) ii = jj = kk = 1;
+            if (ii > NI_ || jj > ijkmax_ || kk > Kair_) ii = jj = kk = 1;
+            rec_idx_[r] = {ii, jj, kk};
+            out[3 * r] = ii; out[3 * r + 1] = jj; out[3 * r + 2] = kk;
+        }
+        upload_receivers();
+        realloc_rec();
+        graph_dirty_ = true;  // nrec is a captured kernel argument
+        return out;
+    }
+    int n_receivers() const override { return static_cast<int>(rec_idx_.size()); }
+
+    void realloc_rec() {
+        const size_t n = static_cast<size_t>(std::max(horizon_, 1)) * std::max<size_t>(rec_idx_.size(), 1);
+        if (n > rec_cap_) {
+            if (d_rec_out_) cudaFree(d_rec_out_);
+            d_rec_out_ = dalloc<double>(n);
+            rec_cap_ = n;
+            graph_dirty_ = true;
+        }
+    }
+
+    // initial condition: Gaussian pulse, calculation_2D.cpp:292-314
+    void reset(int horizon) override {
+        FDTD_CK(cudaSetDevice(device_));
+        horizon_ = horizon;
+        realloc_rec();
+        const size_t N = nodes_;
+        std::vector<R> p(N), z(N, R(0));
+        const double gc = 4.0 * std::log(2.0) / std::pow(in.gauss_width, 2);
+        for (int g = 0; g < NG_; ++g) {
+            const bool pore = g < gAir0_;
+            const Medium& m = pore ? pore_ : air_;
+            const int k = pore ? g : g - gOff_;
+            for (int i = 0; i < NI_; ++i)
+                for (int j = 0; j < NJ_; ++j) {
+                    const double x = m.X[i] - in.source[0], y = m.axY[j] - in.source[1], zz = m.Z[k] - in.source[2];
+                    const double rr = std::sqrt(std::pow(x, 2) + std::pow(y, 2) + std::pow(zz, 2));
+                    p[(static_cast<size_t>(g) * NI_ + i) * NJ_ + j] = static_cast<R>(1.0 * std::exp(-gc * rr * rr));
+                }
+        }
+        FDTD_CK(cudaMemcpy(F_[0][3], p.data(), N * sizeof(R), cudaMemcpyHostToDevice));
+        for (int c = 0; c < 3; ++c) FDTD_CK(cudaMemset(F_[0][c], 0, N * sizeof(R)));
+        for (int c = 0; c < 4; ++c) FDTD_CK(cudaMemset(F_[1][c], 0, N * sizeof(R)));
+        for (int s = 0; s < 6; ++s)
+            for (int b = 0; b < 2; ++b)
+                for (int c = 0; c < 4; ++c)
+                    if (Q_[s][b][c]) FDTD_CK(cudaMemset(Q_[s][b][c], 0, slab_n_[s] * sizeof(R)));
+        const size_t P = static_cast<size_t>(NI_) * Kair_ * 6;
+        FDTD_CK(cudaMemset(d_psi_[0], 0, P * sizeof(double)));
+        FDTD_CK(cudaMemset(d_psi_[1], 0, P * sizeof(double)));
+        FDTD_CK(cudaMemset(d_counters_, 0, 2 * sizeof(int)));
+        FDTD_CK(cudaMemset(d_status_, 0, sizeof(int)));
+        par_ = 0;
+        steps_ = 0;
+        mf_count_ = 0;
+        temp_time_ = 0;
+        n_in_frame_ = 0;
+        frame_started_ = false;
+        done_ = false;
+        upload_frame(0);
+    }
+
+    // params of one pass at parity par
+    Dev<R> params(bool pressure, int par) const {
+        Dev<R> d{};
+        d.NI = NI_; d.NJ = NJ_; d.NG = NG_;
+        d.porous = porous_; d.gAir0 = gAir0_; d.gOff = gOff_; d.Kair = Kair_;
+        d.rigid_south = !porous_;
+        d.tdbc = tdbc_;
+        d.fbvp = in.scheme == FB_V_P;
+        const bool fbpv = in.scheme == FB_P_V;
+        const int o = par, nw = 1 - par;
+        if (pressure) {
+            const int ub = fbpv ? o : nw;  // FB_v_p: pressure uses the new velocity
+            d.u_in = F_[ub][0]; d.v_in = F_[ub][1]; d.w_in = F_[ub][2];
+            d.pold = F_[o][3];
+            d.p_in = F_[o][3];
+            d.p_out = F_[nw][3];
+        } else {
+            d.u_in = F_[o][0]; d.v_in = F_[o][1]; d.w_in = F_[o][2];
+            d.p_in = fbpv ? F_[nw][3] : F_[o][3];
+            d.pold = F_[o][3];
+            d.u_out = F_[nw][0]; d.v_out = F_[nw][1]; d.w_out = F_[nw][2];
+        }
+        d.axA = d_axA_; d.ayA = d_ayA_; d.axP = d_axP_; d.ayP = d_ayP_; d.azG = d_azG_;
+        const double dt = in.dt, gP0 = in.gamma * in.P0;
+        d.dt = R(dt); d.gP0dt = R(in.gamma * in.P0 * dt); d.gdt = R(in.gamma * dt);
+        d.Aavdt = R(in.Aav * dt); d.Aav = R(in.Aav); d.gP0 = R(gP0);
+        if (porous_) {
+            const double eff = 1.0 / in.pore.eff_density;
+            const double beta = in.pore.resistivity * dt * eff;
+            const double ib = 1.0 / (beta + 1.0);
+            d.pGama = R(dt / in.pore.Kp / in.pore.porosity);
+            d.pInvB = R(ib);
+            d.pIBdtEff = R(ib * dt * eff);
+        }
+        d.sxI = d_sx_[0]; d.fxI = d_sx_[1]; d.gxI = d_sx_[2];
+        d.syJ = d_sy_[0]; d.fyJ = d_sy_[1]; d.gyJ = d_sy_[2];
+        d.szK = d_sz_[0]; d.fzK = d_sz_[1]; d.gzK = d_sz_[2];
+        d.sdI = d_sdx_; d.sdJ = d_sdy_; d.sdK = d_sdz_;
+        d.pml_y_time = pml_y_time_;
+        for (int s = 0; s < 6; ++s) {
+            Slab<R>& S = d.sl[s];
+            S.i0 = slab_[s].i0; S.j0 = slab_[s].j0; S.k0 = slab_[s].k0;
+            S.ni = slab_n_[s] ? slab_[s].ni : 0; S.nj = slab_[s].nj; S.nk = slab_[s].nk;
+            if (!slab_n_[s]) continue;
+            // Qp: pressure pass reads old (o) writes new (nw); velocity pass reads the
+            // Qp the pressure pass of this step wrote. Qu/Qv/Qw mirror that.
+            const int qp_cur = pressure ? o : (fbpv ? nw : o);
+            const int quvw_cur = pressure ? (fbpv ? o : nw) : o;
+            for (int c = 0; c < 3; ++c) { S.rd[c] = Q_[s][quvw_cur][c]; S.wr[c] = Q_[s][nw][c]; }
+            S.rd[3] = Q_[s][qp_cur][3];
+            S.wr[3] = Q_[s][nw][3];
+        }
+        d.Uw = d_Uw_; d.Vw = d_Vw_; d.Ww = d_Ww_;
+        d.mask = mask_on_ ? d_mask_ : nullptr;
+        d.mi0 = mi0_; d.mi1 = mi1_; d.mj0 = mj0_; d.mj1 = mj1_; d.mk0 = mk0_; d.mk1 = mk1_;
+        d.m1_ibdteff = R(m1_[0]); d.m1_ib = R(m1_[1]); d.m1_gama = R(m1_[2]);
+        d.m2_ibdteff = R(m2_[0]); d.m2_ib = R(m2_[1]); d.m2_gama = R(m2_[2]);
+        d.psi_in = d_psi_[o];
+        d.psi_out = d_psi_[nw];
+        for (int q = 0; q < 6; ++q) { d.td_e[q] = td_e_[q]; d.td_adt[q] = td_adt_[q]; }
+        d.td_den = td_den_;
+        d.td_z = in.Z_inf;
+        d.nrec = static_cast<int>(rec_idx_.size());
+        d.rec_node = d_rec_node_;
+        d.rec_out = d_rec_out_;
+        d.counters = d_counters_;
+        d.status = d_status_;
+        return d;
+    }
+
+    void launch_pass(bool pressure, int par, bool first) {
+        const dim3 blk(32, 8, 1);
+        const dim3 grd((NJ_ + 31) / 32, (NI_ + 7) / 8, NG_);
+        const Dev<R> d = params(pressure, par);
+        const int fp = first ? 1 : 0;
+        if (pressure) {
+            if (wind_on_) k_pressure<R, true><<<grd, blk, 0, stream_>>>(d, fp);
+            else k_pressure<R, false><<<grd, blk, 0, stream_>>>(d, fp);
+        } else {
+            if (wind_on_) k_velocity<R, true><<<grd, blk, 0, stream_>>>(d, fp);
+            else k_velocity<R, false><<<grd, blk, 0, stream_>>>(d, fp);
+        }
+        FDTD_CK(cudaGetLastError());
+        ++launches_;
+    }
+
+    void enqueue_step(int par) {
+        if (in.scheme == FB_P_V) {
+            launch_pass(true, par, true);
+            launch_pass(false, par, false);
+        } else {
+            launch_pass(false, par, true);
+            launch_pass(true, par, false);
+        }
+    }
+
+    static constexpr int kGraphSteps = 16;  // even: parity pattern repeats
+
+    void ensure_graph() {
+        if (graph_exec_ && !graph_dirty_) return;
+        if (graph_exec_) { cudaGraphExecDestroy(graph_exec_); graph_exec_ = nullptr; }
+        cudaGraph_t g;
+        const long long before = launches_;
+        FDTD_CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+        for (int s = 0; s < kGraphSteps; ++s) enqueue_step(s & 1);
+        FDTD_CK(cudaStreamEndCapture(stream_, &g));
+        launches_ = before;
+        FDTD_CK(cudaGraphInstantiate(&graph_exec_, g, 0));
+        cudaGraphDestroy(g);
+        graph_dirty_ = false;
+    }
+
+    // n steps of the current frame, parity-aware, graphs for the bulk
+    void run_steps(int n) {
+        while (n > 0 && (par_ & 1)) { enqueue_step(par_); par_ ^= 1; --n; ++steps_; }
+        if (n >= kGraphSteps) {
+            ensure_graph();
+            while (n >= kGraphSteps) {
+                FDTD_CK(cudaGraphLaunch(graph_exec_, stream_));
+                launches_ += 2 * kGraphSteps;
+                n -= kGraphSteps;
+                steps_ += kGraphSteps;
+            }
+        }
+        while (n > 0) { enqueue_step(par_); par_ ^= 1; --n; ++steps_; }
+    }
+
+    // moving-frame shift of fields and the x/z PML slabs along j
+    void shift_frame() {
+        const int sh = mf_.trail_DJ - 1, lead = mf_.lead_DJ, tempJ = mf_.JMAX - mf_.lead_DJ;
+        // fields (all media) and p's west copy: calculation_2D.cpp:458-481
+        const int rows = NI_ * NG_;
+        for (int c = 0; c < 4; ++c) {
+            k_shift_rows<R><<<(rows + 127) / 128, 128, 0, stream_>>>(F_[par_][c], rows, NJ_, sh, lead, tempJ, NJ_,
+                                                                     c == 3 ? 1 : 0);
+            FDTD_CK(cudaGetLastError());
+            ++launches_;
+        }
+        // air::SetQMove: x1, x2, z1, z2 slabs (the y slabs are not moved), air.cpp:2522-2729
+        for (int s : {0, 1, 4, 5}) {
+            if (!slab_n_[s]) continue;
+            const int r = slab_[s].ni * slab_[s].nk;
+            for (int c = 0; c < 4; ++c) {
+                k_shift_rows<R><<<(r + 127) / 128, 128, 0, stream_>>>(Q_[s][par_][c], r, slab_[s].nj, sh, lead, tempJ,
+                                                                      NJ_, 0);
+                FDTD_CK(cudaGetLastError());
+                ++launches_;
+            }
+        }
+    }
+
+    int frame_limit() const {  // airpore.cpp:542-560
+        const int JMAX = ijkmax_;
+        const double dy = in.dy, c0 = in.c0, dt = in.dt;
+        const int last = static_cast<int>((JMAX - mf_.JMAX) / (mf_.lead_DJ - 1) + 1.e-6);
+        int lim;
+        if (mf_count_ == last || JMAX == mf_.JMAX) {
+            lim = horizon_ - temp_time_;
+        } else if (mf_count_ == 0) {
+            lim = static_cast<int>((mf_.JMAX - 1) * dy / c0 / dt * mf_.ratio);
+        } else {
+            lim = static_cast<int>((mf_.trail_DJ - 1) * dy / c0 / dt);
+            double lt1 = 0.0, lt2 = 0.0;
+            if (mf_count_ % 10 == 0) {
+                lt1 = (mf_.trail_DJ - 1) * dy / c0 / dt - lim;
+                lt1 = lt1 * 10.0;
+            }
+            if (mf_count_ % 100 == 0) {
+                lt2 = (mf_.trail_DJ - 1) * dy / c0 / dt - lim;
+                lt2 = lt2 * 100 - static_cast<int>(lt2 * 10) * 10;
+            }
+            lim = lim + static_cast<int>(lt1) + static_cast<int>(lt2);
+            if (temp_time_ + lim > horizon_) lim = horizon_ - temp_time_;
+        }
+        return lim;
+    }
+
+    int advance(int nsteps, double* rec_out) override {
+        FDTD_CK(cudaSetDevice(device_));
+        const int start = steps_;
+        FDTD_CK(cudaEventRecord(ev0_, stream_));
+        int left = nsteps;
+        while (left > 0 && !done_) {
+            if (!frame_started_) {
+                mf_limit_ = frame_limit();
+                if (mf_count_ != 0) shift_frame();
+                upload_frame(mf_count_);
+                frame_started_ = true;
+                n_in_frame_ = 0;
+            }
+            const int todo = std::min(left, mf_limit_ - n_in_frame_);
+            if (todo > 0) run_steps(todo);
+            left -= std::max(todo, 0);
+            n_in_frame_ += std::max(todo, 0);
+            if (n_in_frame_ >= mf_limit_) {
+                mf_count_ += 1;
+                temp_time_ += mf_limit_;
+                frame_started_ = false;
+                const int last = static_cast<int>((ijkmax_ - mf_.JMAX) / (mf_.lead_DJ - 1) + 1.e-6);
+                if (!(mf_count_ <= last && temp_time_ < horizon_ && mf_.Judge == 1)) done_ = true;
+            }
+        }
+        FDTD_CK(cudaEventRecord(ev1_, stream_));
+        FDTD_CK(cudaStreamSynchronize(stream_));
+        float ms = 0.f;
+        FDTD_CK(cudaEventElapsedTime(&ms, ev0_, ev1_));
+        last_ms_ = ms;
+        int st = 0;
+        FDTD_CK(cudaMemcpy(&st, d_status_, sizeof(int), cudaMemcpyDeviceToHost));
+        const int taken = steps_ - start;
+        if (rec_out && !rec_idx_.empty() && taken > 0) {
+            FDTD_CK(cudaMemcpy(rec_out, d_rec_out_ + static_cast<size_t>(start) * rec_idx_.size(),
+                               sizeof(double) * taken * rec_idx_.size(), cudaMemcpyDeviceToHost));
+        }
+        if (st & 1) fail(-4, "pressure became non-finite");
+        return taken;
+    }
+
+    // half steps (FB_p_v): airpore::Cal_pressure, then Cal_velocity + UpdateInitialCond
+    void step_pressure() override {
+        FDTD_CK(cudaSetDevice(device_));
+        if (in.scheme != FB_P_V) fail(-2, "half steps are exposed for FB_p_v only");
+        if (!frame_started_) {
+            mf_limit_ = frame_limit();
+            upload_frame(mf_count_);
+            frame_started_ = true;
+        }
+        launch_pass(true, par_, true);
+        FDTD_CK(cudaStreamSynchronize(stream_));
+    }
+    void step_velocity() override {
+        FDTD_CK(cudaSetDevice(device_));
+        if (in.scheme != FB_P_V) fail(-2, "half steps are exposed for FB_p_v only");
+        launch_pass(false, par_, false);
+        par_ ^= 1;
+        ++steps_;
+        ++n_in_frame_;
+        FDTD_CK(cudaStreamSynchronize(stream_));
+    }
+
+    // ------------------------------------------------------- read-out
+    std::vector<R> fetch(const R* d, size_t n) {
+        std::vector<R> h(n);
+        FDTD_CK(cudaMemcpy(h.data(), d, n * sizeof(R), cudaMemcpyDeviceToHost));
+        return h;
+    }
+
+    void medium_dims(int medium, int& I, int& J, int& K, int& g0) const {
+        I = NI_; J = NJ_;
+        if (medium == 0) { K = Kair_; g0 = gOff_; }
+        else if (porous_) { K = pore_.K; g0 = 0; }
+        else fail(-5, "no porous ground in this case");
+    }
+
+    // comp 0..3: p u v w at the current level; 4..7: the other ("nn") level
+    const R* field_ptr(int comp) const {
+        const int lvl = comp >= 4 ? 1 - par_ : par_;
+        static const int map[4] = {3, 0, 1, 2};
+        return F_[lvl][map[comp & 3]];
+    }
+
+    void get_field(int medium, int comp, double* out) override {
+        if (comp < 0 || comp > 7) fail(-5, "comp must be 0..7");
+        int I, J, K, g0;
+        medium_dims(medium, I, J, K, g0);
+        const std::vector<R> h = fetch(field_ptr(comp), nodes_);
+        for (int i = 0; i < I; ++i)
+            for (int j = 0; j < J; ++j)
+                for (int k = 0; k < K; ++k)
+                    out[(static_cast<size_t>(i) * J + j) * K + k] =
+                        static_cast<double>(h[(static_cast<size_t>(k + g0) * NI_ + i) * NJ_ + j]);
+    }
+
+    void set_field(int medium, int comp, const double* src) override {
+        if (comp < 0 || comp > 3) fail(-5, "comp must be 0..3");
+        int I, J, K, g0;
+        medium_dims(medium, I, J, K, g0);
+        R* dptr = const_cast<R*>(field_ptr(comp));
+        std::vector<R> h = fetch(dptr, nodes_);
+        for (int i = 0; i < I; ++i)
+            for (int j = 0; j < J; ++j)
+                for (int k = 0; k < K; ++k)
+                    h[(static_cast<size_t>(k + g0) * NI_ + i) * NJ_ + j] =
+                        static_cast<R>(src[(static_cast<size_t>(i) * J + j) * K + k]);
+        FDTD_CK(cudaMemcpy(dptr, h.data(), nodes_ * sizeof(R), cudaMemcpyHostToDevice));
+    }
+
+    void get_psi(double* out) override {
+        FDTD_CK(cudaMemcpy(out, d_psi_[par_], sizeof(double) * NI_ * Kair_ * 6, cudaMemcpyDeviceToHost));
+    }
+
+    int get_slab(int s, int comp, double* out, int* dims) override {
+        if (s < 0 || s > 5 || comp < 0 || comp > 3) fail(-5, "slab 0..5, comp 0..3");
+        if (!slab_n_[s]) { dims[0] = dims[1] = dims[2] = 0; return 0; }
+        const SlabDesc& S = slab_[s];
+        dims[0] = S.ni; dims[1] = S.nj; dims[2] = S.nk;
+        if (out) {
+            const std::vector<R> h = fetch(Q_[s][par_][comp], slab_n_[s]);
+            for (int a = 0; a < S.ni; ++a)
+                for (int b = 0; b < S.nj; ++b)
+                    for (int c = 0; c < S.nk; ++c)
+                        out[(static_cast<size_t>(a) * S.nj + b) * S.nk + c] =
+                            static_cast<double>(h[(static_cast<size_t>(c) * S.ni + a) * S.nj + b]);
+        }
+        return 1;
+    }
+
+    size_t state_elems() const override { return nodes_; }
+
+    void copy_state(int dir, void* host) override {
+        FDTD_CK(cudaSetDevice(device_));
+        static const int order[4] = {0, 1, 2, 3};  // u v w p
+        char* h = static_cast<char*>(host);
+        const size_t bytes = nodes_ * sizeof(R);
+        for (int c : order) {
+            if (dir == 0)
+                FDTD_CK(cudaMemcpyAsync(h + c * bytes, F_[par_][c], bytes, cudaMemcpyDeviceToHost, stream_));
+            else
+                FDTD_CK(cudaMemcpyAsync(F_[par_][c], h + c * bytes, bytes, cudaMemcpyHostToDevice, stream_));
+        }
+        FDTD_CK(cudaStreamSynchronize(stream_));
+    }
+
+    std::array<int, 12> dims() const override {
+        return {NI_, NJ_, Kair_, porous_ ? 1 : 0, porous_ ? pore_.I : 0, porous_ ? pore_.J : 0,
+                porous_ ? pore_.K : 0, NG_, in.time_domain, static_cast<int>(sizeof(R) == 4),
+                in.scheme == FB_V_P ? 1 : 0, steps_};
+    }
+    long long launch_count() const override { return launches_; }
+    double last_device_ms() const override { return last_ms_; }
+
+   private:
+    struct SlabDesc {
+        int i0, j0, k0, ni, nj, nk;
+    };
+
+    int device_ = 0;
+    MovingFrameCfg mf_;
+    int ijkmax_ = 0;
+    Medium air_, pore_;
+    bool porous_ = false;
+    int NI_ = 0, NJ_ = 0, NG_ = 0, Kair_ = 0, gAir0_ = 0, gOff_ = 0;
+    size_t nodes_ = 0;
+    // PML
+    int jx_ = 0, jy_ = 0, jz_ = 0, I1_ = 0, I2_ = 0, Y1_ = 0, Y2_ = 0, K1_ = 0, K2_ = 0, pml_y_time_ = 0;
+    double W1_ = 0, W2_ = 0, L1_ = 0, L2_ = 0, H1_ = 0, H2_ = 0, x1_ = 0, x2_ = 0, y1_ = 0, y2_ = 0, z1_ = 0, z2_ = 0;
+    std::vector<double> sx_, fx_, gx_, sy_, fy_, gy_, sz_, fz_, gz_;
+    std::vector<int8_t> sdx_, sdy_, sdz_;
+    SlabDesc slab_[6]{};
+    size_t slab_n_[6]{};
+    // hill
+    bool mask_on_ = false;
+    std::vector<int8_t> mask_;
+    int mi0_ = 0, mi1_ = -1, mj0_ = 0, mj1_ = -1, mk0_ = 0, mk1_ = -1;
+    std::array<double, 3> m1_{0, 0, 0}, m2_{0, 0, 0};
+    // TDBC
+    bool tdbc_ = false;
+    double td_e_[6]{}, td_adt_[6]{}, td_den_ = 0;
+    bool wind_on_ = false;
+    // device
+    std::vector<void*> allocs_;
+    R* F_[2][4]{};
+    R* Q_[6][2][4]{};
+    R *d_axA_ = nullptr, *d_ayA_ = nullptr, *d_axP_ = nullptr, *d_ayP_ = nullptr, *d_azG_ = nullptr;
+    R *d_sx_[3]{}, *d_sy_[3]{}, *d_sz_[3]{};
+    int8_t *d_sdx_ = nullptr, *d_sdy_ = nullptr, *d_sdz_ = nullptr, *d_mask_ = nullptr;
+    R *d_Uw_ = nullptr, *d_Vw_ = nullptr, *d_Ww_ = nullptr;
+    double* d_psi_[2]{};
+    long long* d_rec_node_ = nullptr;
+    double* d_rec_out_ = nullptr;
+    size_t rec_cap_ = 0;
+    int* d_counters_ = nullptr;
+    int* d_status_ = nullptr;
+    cudaStream_t stream_ = nullptr;
+    cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+    cudaGraphExec_t graph_exec_ = nullptr;
+    bool graph_dirty_ = true;
+    // receivers
+    std::vector<std::array<int, 3>> rec_idx_;
+    // time loop
+    int par_ = 0, steps_ = 0, horizon_ = 0;
+    int mf_count_ = 0, temp_time_ = 0, n_in_frame_ = 0, mf_limit_ = 0, frame_N_ = 0;
+    bool frame_started_ = false, done_ = false;
+    long long launches_ = 0;
+    double last_ms_ = 0;
+};
+
+// ---------------------------------------------------------------- Solver
+Solver::Solver(const std::string& case_dir, int precision, int device) : precision_(precision) {
+    if (precision == 0) impl_.reset(new SolverImpl<double>(case_dir, device));
+    else if (precision == 1) impl_.reset(new SolverImpl<float>(case_dir, device));
+    else fail(-5, "precision must be 0 (FP64) or 1 (FP32)");
+}
+Solver::~Solver() = default;
+const ReferenceInput& Solver::input() const { return impl_->in; }
+std::array<int, 12> Solver::dims() const { return impl_->dims(); }
+std::vector<int> Solver::set_receivers(const std::vector<double>& xyz) { return impl_->set_receivers(xyz); }
+int Solver::n_receivers() const { return impl_->n_receivers(); }
+void Solver::reset(int horizon) { impl_->reset(horizon > 0 ? horizon : impl_->in.time_domain); }
+int Solver::run(int nsteps, double* rec_out) {
+    impl_->reset(nsteps);
+    return impl_->advance(nsteps, rec_out);
+}
+int Solver::advance(int nsteps, double* rec_out) { return impl_->advance(nsteps, rec_out); }
+void Solver::step_pressure() { impl_->step_pressure(); }
+void Solver::step_velocity() { impl_->step_velocity(); }
+void Solver::get_field(int m, int c, double* out) { impl_->get_field(m, c, out); }
+void Solver::set_field(int m, int c, const double* in) { impl_->set_field(m, c, in); }
+void Solver::get_psi(double* out) { impl_->get_psi(out); }
+int Solver::get_slab(int s, int c, double* out, int* dims) { return impl_->get_slab(s, c, out, dims); }
+size_t Solver::state_elems() const { return impl_->state_elems(); }
+void Solver::copy_state(int dir, void* host) { impl_->copy_state(dir, host); }
+long long Solver::launch_count() const { return impl_->launch_count(); }
+double Solver::last_device_ms() const { return impl_->last_device_ms(); }
+
+}  // namespace fdtd

@@ -1,0 +1,60 @@
+// Host side of the B200 time-marching path: one device-resident domain per
+// Solver, built from the reference's setup files.
+#pragma once
+
+#include <array>
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "fdtd_input.hpp"
+
+namespace fdtd {
+
+struct SolverError {
+    int code;
+    std::string msg;
+};
+
+class SolverImplBase;
+
+class Solver {
+   public:
+    // precision: 0 FP64, 1 FP32. Throws SolverError.
+    Solver(const std::string& case_dir, int precision, int device);
+    ~Solver();
+    Solver(const Solver&) = delete;
+    Solver& operator=(const Solver&) = delete;
+
+    const ReferenceInput& input() const;
+    std::array<int, 12> dims() const;
+    int precision() const { return precision_; }
+
+    // receivers at reference coordinates; returns whole-domain indices (3 per receiver)
+    std::vector<int> set_receivers(const std::vector<double>& xyz);
+    int n_receivers() const;
+
+    // back to t = 0; horizon = planned steps (<= 0: input.txt's time_domain)
+    void reset(int horizon = 0);
+    // time loop; rec_out: [n][nrec] host FP64 or nullptr. Returns steps taken.
+    int run(int nsteps, double* rec_out);
+    int advance(int nsteps, double* rec_out);
+    void step_pressure();
+    void step_velocity();
+
+    void get_field(int medium, int comp, double* out);
+    void set_field(int medium, int comp, const double* in);
+    void get_psi(double* out);
+    int get_slab(int s, int comp, double* out, int* dims);
+    size_t state_elems() const;
+    void copy_state(int dir, void* host);
+    long long launch_count() const;
+    double last_device_ms() const;
+
+   private:
+    int precision_;
+    std::unique_ptr<SolverImplBase> impl_;
+};
+
+}  // namespace fdtd

@@ -1,0 +1,386 @@
+#!/usr/bin/env python
+"""Throughput benchmark of the B200 FDTD time-marching path.
+
+Workload (N=1): porous ground under air, 256 (range, Y/j) x 128 (X/i) x 96
+(Z/k) air nodes over a 16-cell Zwikker-Kosten layer (sigma 200 kPa s/m^2,
+porosity 0.3, tortuosity 1.8) with the two-plane airpore interface, 20-node
+PML on the five air faces, FB_p_v, 8 receivers; synthetic setup generated
+from a seed.  One bench step = ``--inner`` forward-backward time steps of
+the whole domain with the state resident in HBM; L2 is flushed (a 512 MB
+write) between bench steps.  The headline ``value`` is FP32; the FP64 path
+is reported beside it.
+
+``--impl reference`` times the reference solver itself (the unmodified
+sources compiled under oracle/_ref/, driven through airpore's own loop) on
+the host cores: one independent single-rank process per core (the
+reference's MPI decomposition has no MPI here), aggregate throughput.
+
+Multi-GPU: replicas only -- each rank runs its own independent solve, no
+collective on the data path; value = all ranks' cell updates / max time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Gcell-upd/s & % HBM peak, FP32 vs FP64 at <=1e-4 rel err; surrogate speedup"
+UNIT = "Gcell-upd/s"
+WORKLOAD = "porous ground + 20-node PML, 256x128x96 air + 256x128x18 porous nodes, FB_p_v"
+
+
+def make_case(tmp: str):
+    casegen = importlib.import_module("3d_mpi_test_b200.casegen")
+    case, rec = casegen.porous_ground(ni=128, nj=256, nk=96, layer=16, d=0.05, steps=4000, pml=20, seed=0)
+    d = os.path.join(tmp, "porous_ground")
+    case.write(d)
+    casegen.write_receivers(os.path.join(d, "rec.txt"), rec)
+    air = case.NI * case.NJ * case.NK
+    pore = case.NI * case.NJ * len(case.pore_Z)
+    return d, rec, air + pore, case
+
+
+def algorithmic_bytes(case, word: int) -> dict:
+    """Per FB step: every node's u,v,w,p read once and written once (8 words),
+    plus 8 words (Qu,Qv,Qw,Qp read+write) per PML slab storage node, plus
+    the TDBC state and receiver words."""
+    I, J, K = case.NI, case.NJ, case.NK
+    I1, I2, J1, J2, K1, K2 = case.pml_nodes
+    cells = I * J * K + I * J * len(case.pore_Z or [])
+    slab = 0
+    slab += (I1 + 1) * J * K if I1 else 0
+    slab += (I2 + 1) * J * K if I2 else 0
+    slab += I * (J1 + 1) * K if J1 else 0
+    slab += I * (J2 + 1) * K if J2 else 0
+    slab += I * J * (K2 + 1) if K2 else 0
+    tdbc = I * K if case.bc[2] == 5 else 0
+    b = cells * 8 * word + slab * 8 * word + tdbc * 12 * 8 + 8 * 8
+    return {"bytes_per_step": b, "cells": cells, "slab_nodes": slab}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi"):
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        return self
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[4:8]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------- CPU side
+def ref_harness_path():
+    p = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+    return p if os.path.exists(p) else None
+
+
+def time_reference(case_dir: str, cells: int, steps: int, warmup: int, replicas: int):
+    """Run `replicas` independent reference processes; returns aggregate
+    Gcell-upd/s and the per-process ms/step."""
+    exe = ref_harness_path()
+    if exe is None:
+        return None
+    procs = [subprocess.Popen([exe, case_dir, "--time", str(warmup), str(steps)], stdout=subprocess.PIPE,
+                              stderr=subprocess.DEVNULL, text=True) for _ in range(replicas)]
+    ms = []
+    for p in procs:
+        out, _ = p.communicate()
+        for ln in out.splitlines():
+            if ln.startswith("{"):
+                ms.append(json.loads(ln)["ms_per_step"])
+    if len(ms) != replicas:
+        return None
+    worst = max(ms)
+    return {"value": replicas * cells / (worst * 1e-3) / 1e9, "ms_per_step": worst, "cores": replicas}
+
+
+def host_replicas(bytes_per_process=700e6) -> int:
+    n = os.cpu_count() or 1
+    try:
+        with open("/proc/meminfo") as f:
+            for ln in f:
+                if ln.startswith("MemAvailable"):
+                    avail = float(ln.split()[1]) * 1024
+                    n = max(1, min(n, int(0.6 * avail / bytes_per_process)))
+    except OSError:
+        pass
+    return n
+
+
+def cpu_baseline(case_dir: str, cells: int):
+    """Bounded sample on rank 0: the reference (or, if its build is absent,
+    the oracle restatement) over 3 steps after 1 warm-up step, all cores."""
+    reps = host_replicas()
+    r = time_reference(case_dir, cells, steps=3, warmup=1, replicas=reps)
+    if r is not None:
+        return {"value": round(r["value"], 6), "unit": UNIT, "cores": r["cores"], "kind": "reference",
+                "sample": f"{reps} independent single-rank reference processes x 3 FB steps of the bench workload "
+                          f"(after 1 warm-up step); {r['ms_per_step']:.0f} ms/step each"}
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle  # the checker's own CPU restatement, timed only as the baseline
+
+    oc = oracle.OracleCase(case_dir)
+    oc.run(1)
+    t0 = time.perf_counter()
+    oc.run(3)
+    dt = (time.perf_counter() - t0) / 3
+    return {"value": round(cells / dt / 1e9, 6), "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": "oracle restatement, 1 core, 3 FB steps of the bench workload"}
+
+
+# ---------------------------------------------------------------- GPU side
+def run_gpu(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+
+    pkg = importlib.import_module("3d_mpi_test_b200")
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist  # noqa: F811
+    tmp = tempfile.mkdtemp(prefix=f"bench_r{rank}_")
+    case_dir, rec, cells, case = make_case(tmp)
+    inner = args.inner
+    horizon = max(4000, (args.warmup + args.steps + 2) * inner + 10)
+    flush = torch.empty(128 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 512 MB > L2
+    hbm_peak, peak_kind = peaks()
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    results = {}
+    for prec in ("f32", "f64"):
+        word = 4 if prec == "f32" else 8
+        a = pkg.Airpore(case_dir, prec, device=local_rank)
+        a.set_receivers(rec)
+        a.reset(horizon)
+        for _ in range(args.warmup):
+            flush.zero_()
+            torch.cuda.synchronize()
+            a.advance(inner)
+        barrier()
+        launches0 = a.launch_count()
+        dev_ms = 0.0
+        t0 = time.perf_counter()
+        sampler = ClockSampler(local_rank) if prec == "f32" else None
+        if sampler:
+            sampler.__enter__()
+        try:
+            for _ in range(args.steps):
+                flush.zero_()
+                torch.cuda.synchronize()
+                a.advance(inner)
+                dev_ms += a.last_device_ms()
+        finally:
+            if sampler:
+                sampler.__exit__(None, None, None)
+        barrier()
+        wall = time.perf_counter() - t0
+        launches = a.launch_count() - launches0
+        dev_ms = max_over_ranks(dev_ms)
+        steps_total = args.steps * inner
+        gcell = world * cells * steps_total / (dev_ms * 1e-3) / 1e9
+        ab = algorithmic_bytes(case, word)
+        achieved = ab["bytes_per_step"] / (dev_ms * 1e-3 / steps_total) / 1e9
+        results[prec] = {"gcell": gcell, "ms_per_bench_step": dev_ms / args.steps, "wall_s": wall,
+                         "launches": launches, "achieved_gbs": achieved, "bytes_per_step": ab["bytes_per_step"],
+                         "clocks": sampler.summary() if sampler else None}
+        # end to end through the public API with host buffers (FP32 headline only)
+        if prec == "f32":
+            n = a.state_elems()
+            host = torch.empty(4 * n, dtype=torch.float32, pin_memory=True)
+            a.copy_state(host.numpy(), to_device=False)
+            a.reset(horizon)
+            barrier()
+            t1 = time.perf_counter()
+            for _ in range(args.steps):
+                a.copy_state(host.numpy(), to_device=True)  # H2D: the step's input state
+                r = a.advance(inner)  # receivers come back D2H inside the call
+            torch.cuda.synchronize()
+            e2e_s = max_over_ranks(time.perf_counter() - t1)
+            results["e2e"] = {"value": world * cells * steps_total / e2e_s / 1e9, "unit": UNIT,
+                              "h2d_bytes_per_step": int(host.numel() * 4),
+                              "d2h_bytes_per_step": int(r.size * 8)}
+        a.close()
+    shutil.rmtree(tmp, ignore_errors=True)
+
+    if rank != 0:
+        return None
+    f32, f64 = results["f32"], results["f64"]
+    roof = {"bound": "hbm", "achieved": round(f32["achieved_gbs"], 1), "peak": hbm_peak, "unit": "GB/s",
+            "frac": round(f32["achieved_gbs"] / hbm_peak, 4), "traffic": None,
+            "peak_kind": peak_kind,
+            "kernel": "one FB step (pressure pass + velocity pass), FP32",
+            "algorithmic_bytes_per_step": f32["bytes_per_step"]}
+    prof = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(prof):
+        with open(prof) as fh:
+            roof["traffic"] = json.load(fh).get("f32_bytes_per_step")
+    line = {
+        "metric": METRIC, "value": round(f32["gcell"], 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(f32["ms_per_bench_step"], 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded case generator)",
+        "config": {"workload": WORKLOAD, "inner_fb_steps_per_bench_step": args.inner,
+                   "cells_per_fb_step": cells, "l2": "flushed (512 MB write) between bench steps",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single device-resident domain"},
+        "fp64": {"value": round(f64["gcell"], 3), "ms_per_step": round(f64["ms_per_bench_step"], 4),
+                 "achieved_gbs": round(f64["achieved_gbs"], 1),
+                 "frac": round(f64["achieved_gbs"] / hbm_peak, 4),
+                 "fp32_speedup": round(f32["gcell"] / f64["gcell"], 3)},
+        "roofline": roof,
+        "e2e": {k: (round(v, 3) if isinstance(v, float) else v) for k, v in results["e2e"].items()},
+        "gpu_launches": int(f32["launches"]),
+        "clocks": f32["clocks"],
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(case_dir_for_cpu(), cells)
+    return line
+
+
+def case_dir_for_cpu():
+    tmp = tempfile.mkdtemp(prefix="bench_cpu_")
+    return make_case(tmp)[0]
+
+
+def run_reference_arm(args, world, rank):
+    if rank != 0:
+        return None
+    tmp = tempfile.mkdtemp(prefix="bench_ref_")
+    case_dir, rec, cells, case = make_case(tmp)
+    exe = ref_harness_path()
+    if exe is None:
+        return {"impl": "reference", "unavailable": "oracle/_ref/ref_harness not built (needs the reference sources)"}
+    reps = host_replicas()
+    t0 = time.perf_counter()
+    r = time_reference(case_dir, cells, steps=args.steps, warmup=args.warmup, replicas=reps)
+    wall = time.perf_counter() - t0
+    if r is None:
+        return {"impl": "reference", "unavailable": "reference harness failed"}
+    v = round(r["value"], 6)
+    return {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(r["ms_per_step"], 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded case generator)",
+        "config": {"workload": WORKLOAD, "inner_fb_steps_per_bench_step": 1, "cells_per_fb_step": cells,
+                   "parallelism": f"{reps} single-rank host processes"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": reps, "kind": "reference",
+                         "sample": f"{reps} independent single-rank reference processes, {args.steps} timed FB steps "
+                                   f"each after {args.warmup} warm-up steps ({wall:.0f} s wall)"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--inner", type=int, default=50)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        line = run_reference_arm(args, world, rank)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        line = run_gpu(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,115 @@
+/*
+ * fdtd_b200.h -- C ABI of the B200 (sm_100a) time-marching path of the
+ * outdoor-sound FDTD solver whose reference is azhang22/3D_MPI_TEST.
+ *
+ * One handle = one device-resident domain (air + optional porous ground)
+ * built from a reference case directory (input.txt + coordi_*.dat). The
+ * library owns all device memory; host buffers are caller-owned. Every
+ * function returns an int status (FDTD_OK or a negative FDTD_ERR_*);
+ * fdtd_last_error() returns the message of the calling thread's last
+ * failure. A handle is not thread-safe: use one handle per host thread.
+ *
+ * Reference interfaces replaced (file:line in the reference repository):
+ *   fdtd_create        airpore::airpore (airpore.cpp:17-316) +
+ *                      airpore::SetInitialCond (airpore.cpp:936-964) +
+ *                      air::air / porous::porous constructors
+ *   fdtd_set_receivers calculation_2D::get_position (calculation_2D.cpp:317-352)
+ *                      with the out-of-domain rule of airpore.cpp:454-457
+ *   fdtd_run           airpore::get_output time loop (airpore.cpp:539-624):
+ *                      SetMovingFrame + per step get_pressure, Cal_pressure,
+ *                      Cal_velocity, UpdateInitialCond
+ *   fdtd_advance       the same loop, continued from the current state
+ *   fdtd_step_pressure airpore::Cal_pressure (airpore.cpp:366-398)
+ *   fdtd_step_velocity airpore::Cal_velocity + UpdateInitialCond
+ *                      (airpore.cpp:324-364, 648-662)
+ *   fdtd_get_field     read-out of calculation_2D::p_n/u_n/v_n/w_n
+ *                      (calculation_2D.h:33-34) in the reference [i][j][k] order
+ *   fdtd_set_field     write of the same arrays (restart input,
+ *                      calculation_2D.cpp:522-545)
+ *   fdtd_get_psi       calculation_2D::Psi (TDBC state, calculation_2D.h:71)
+ *   fdtd_get_slab      air::Qux1..Qpz2 PML integrals (air.h:40-42)
+ */
+#ifndef FDTD_B200_H
+#define FDTD_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FDTD_OK 0
+#define FDTD_ERR_INPUT (-1)       /* unreadable or malformed case files */
+#define FDTD_ERR_UNSUPPORTED (-2) /* a configuration the reference itself cannot run */
+#define FDTD_ERR_CUDA (-3)        /* CUDA runtime failure or no sm_100 device */
+#define FDTD_ERR_NONFINITE (-4)   /* a pressure value became Inf/NaN */
+#define FDTD_ERR_ARG (-5)         /* bad argument (null pointer, range) */
+#define FDTD_ERR_STATE (-6)       /* time loop finished; call fdtd_reset */
+
+#define FDTD_F64 0
+#define FDTD_F32 1
+
+typedef struct fdtd_solver fdtd_solver;
+
+/* dims[0..11]: air I J K, has_pore, pore I J K, unified NG, time_domain,
+ * precision, scheme (0 FB_p_v, 1 FB_v_p), steps taken so far */
+#define FDTD_NDIMS 12
+
+int fdtd_create(const char *case_dir, int precision, int device, fdtd_solver **out);
+int fdtd_destroy(fdtd_solver *h);
+int fdtd_dims(const fdtd_solver *h, int *dims);
+const char *fdtd_last_error(void);
+
+/* Receivers at reference coordinates (X, Y, Z triples); idx_out (3n ints,
+ * may be NULL) receives the whole-domain node indices. n <= 64. */
+int fdtd_set_receivers(fdtd_solver *h, int n, const double *xyz, int *idx_out);
+
+/* Back to the initial condition at t = 0, frame 0. horizon = the planned
+ * number of steps (the reference's time_domain, which sets the last frame's
+ * length and the receiver buffer); <= 0 keeps input.txt's value. */
+int fdtd_reset(fdtd_solver *h, int horizon);
+
+/* Reset, then run the reference time loop for nsteps steps (nsteps takes the
+ * place of input.txt's time_domain). rec_out: host [nsteps][n_receivers]
+ * FP64 pressure sampled before each step, or NULL. */
+int fdtd_run(fdtd_solver *h, int nsteps, double *rec_out);
+
+/* Continue the time loop by nsteps (frame schedule from input.txt's
+ * time_domain); rec_out as above for the new steps, or NULL. */
+int fdtd_advance(fdtd_solver *h, int nsteps, double *rec_out);
+
+/* One half step each, for per-half-step parity: pressure then velocity
+ * (FB_p_v). fdtd_step_velocity also swaps the time levels. */
+int fdtd_step_pressure(fdtd_solver *h);
+int fdtd_step_velocity(fdtd_solver *h);
+
+/* medium 0 air, 1 porous ground; comp 0 p, 1 u, 2 v, 3 w. Host FP64 array
+ * in [i][j][k] order (k fastest) of that medium's grid. */
+int fdtd_get_field(fdtd_solver *h, int medium, int comp, double *out);
+int fdtd_set_field(fdtd_solver *h, int medium, int comp, const double *in);
+
+/* TDBC state [i][k][6] of the air grid (FP64). */
+int fdtd_get_psi(fdtd_solver *h, double *out);
+
+/* PML integral slab s (0 x1, 1 x2, 2 y1, 3 y2, 4 z1, 5 z2), comp 0 u 1 v 2 w
+ * 3 p, in the reference slab shape [d0][d1][d2]. dims receives the shape;
+ * returns 1 if the slab exists, 0 if not. out may be NULL. */
+int fdtd_get_slab(fdtd_solver *h, int s, int comp, double *out, int *dims);
+
+/* Whole device state in the native layout ([g][i][j], precision of the
+ * handle): 4 fields u v w p, each fdtd_state_elems() elements. dir 0:
+ * device -> host, 1: host -> device. Used for end-to-end timing with host
+ * buffers. */
+size_t fdtd_state_elems(const fdtd_solver *h);
+int fdtd_copy_state(fdtd_solver *h, int dir, void *host);
+
+/* Kernel launches issued since creation (both passes, graphs included). */
+long long fdtd_launch_count(const fdtd_solver *h);
+
+/* CUDA events around the last fdtd_advance's device work: milliseconds. */
+int fdtd_last_device_ms(const fdtd_solver *h, double *ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

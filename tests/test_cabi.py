@@ -1,0 +1,75 @@
+"""C ABI surface checks that need no GPU: the library loads, exports every
+function include/fdtd_b200.h declares, and rejects bad case directories
+before touching the device."""
+
+import ctypes
+import importlib
+import os
+import re
+
+import pytest
+
+import cases
+
+pkg = importlib.import_module("3d_mpi_test_b200")
+build = importlib.import_module("3d_mpi_test_b200.build")
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    txt = open(os.path.join(ROOT, "include", "fdtd_b200.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(fdtd_[a-z_]+)\s*\(", txt)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    if not os.path.exists(pkg.LIB_PATH):
+        build.build()
+    return pkg.load_library()
+
+
+def test_every_declared_symbol_is_exported(lib):
+    names = declared_functions()
+    assert len(names) >= 15
+    assert set(names) == set(pkg.EXPORTS)
+    for n in names:
+        assert hasattr(lib, n), n
+
+
+def test_library_is_sm100a_only():
+    # the fatbin is built for sm_100a alone (no PTX for JIT to other archs)
+    assert "arch=compute_100a,code=sm_100a" in " ".join(build.ARCH)
+
+
+def test_missing_case_is_input_error(lib, tmp_path):
+    h = ctypes.c_void_p()
+    rc = lib.fdtd_create(str(tmp_path / "nope").encode(), 0, 0, ctypes.byref(h))
+    assert rc == pkg.FDTD_ERR_INPUT
+    assert b"input.txt" in lib.fdtd_last_error()
+    assert not h.value
+
+
+def test_malformed_axis_file_is_input_error(lib, tmp_path):
+    c, _ = cases.pml_rigid()
+    d = str(tmp_path / "bad")
+    c.write(d)
+    with open(os.path.join(d, "coordi_air3.dat"), "w") as f:
+        f.write("0 0.05\n")  # far fewer Z nodes than the header promises
+    h = ctypes.c_void_p()
+    rc = lib.fdtd_create(d.encode(), 0, 0, ctypes.byref(h))
+    assert rc == pkg.FDTD_ERR_INPUT
+    assert b"Z coordinates" in lib.fdtd_last_error()
+
+
+def test_null_arguments(lib):
+    assert lib.fdtd_create(None, 0, 0, None) == pkg.FDTD_ERR_ARG
+    assert lib.fdtd_destroy(None) == pkg.FDTD_OK
+    assert lib.fdtd_state_elems(None) == 0
+
+
+def test_package_fails_loudly_without_library(tmp_path):
+    with pytest.raises(pkg.FdtdError) as e:
+        pkg.load_library(str(tmp_path / "libfdtd_b200.so"))
+    assert e.value.code == pkg.FDTD_ERR_CUDA

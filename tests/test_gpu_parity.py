@@ -1,0 +1,167 @@
+"""B200 parity: the CUDA path against the oracle, through the C ABI.
+
+FP64: relative L2 <= 1e-10 for receiver p(t), final p/u/v/w of both media,
+the TDBC state and every PML integral slab (the bar the north star sets).
+FP32: relative L2 <= 1e-4 for receivers and final pressure against the FP64
+oracle (FP32 fields and stencil; FP64 TDBC state and receiver series)."""
+
+import importlib
+
+import numpy as np
+import pytest
+
+import cases
+import oracle
+
+pkg = importlib.import_module("3d_mpi_test_b200")
+
+pytestmark = pytest.mark.gpu
+
+TOL_F64 = 1e-10
+TOL_F32 = 1e-4
+
+
+def rel_l2(x, y):
+    n = np.linalg.norm(y)
+    return float(np.linalg.norm(x - y) / n) if n > 0 else float(np.linalg.norm(x - y))
+
+
+def _gpu_run(case_dir, rec, nsteps, precision):
+    with pkg.Airpore(case_dir, precision) as a:
+        idx = a.set_receivers(rec)
+        r = a.get_output(nsteps)
+        out = {"receivers": r, "rec_index": idx}
+        for f in "puvw":
+            out[f] = a.field(f)
+            if a.has_pore:
+                out["pore_" + f] = a.field(f, "pore")
+        out["psi"] = a.psi()
+        out["slabs"] = a.slabs()
+        out["launches"] = a.launch_count()
+    return out
+
+
+@pytest.fixture(scope="module")
+def case_dirs(tmp_path_factory):
+    root = tmp_path_factory.mktemp("cases")
+    made = {}
+    for name, fn in cases.CASES.items():
+        c, rec = fn()
+        d = str(root / name)
+        c.write(d)
+        made[name] = (d, rec, c.time_domain)
+    return made
+
+
+@pytest.mark.parametrize("name", sorted(cases.CASES))
+def test_fp64_matches_oracle(name, case_dirs):
+    d, rec, n = case_dirs[name]
+    ref = oracle.run_case(d, rec, n)
+    got = _gpu_run(d, rec, n, "f64")
+    np.testing.assert_array_equal(got["rec_index"], ref["rec_index"])
+    errs = {"receivers": rel_l2(got["receivers"], ref["receivers"])}
+    for f in "puvw":
+        errs[f] = rel_l2(got[f], ref[f])
+        if "pore_" + f in ref:
+            errs["pore_" + f] = rel_l2(got["pore_" + f], ref["pore_" + f])
+    errs["psi"] = rel_l2(got["psi"], ref["psi"])
+    assert set(got["slabs"]) == set(ref["slabs"])
+    for s, q in ref["slabs"].items():
+        for c in "uvwp":
+            errs[f"Q{c}_{s}"] = rel_l2(got["slabs"][s][c], q[c])
+    assert max(errs.values()) <= TOL_F64, errs
+    assert got["launches"] >= 2 * n  # two passes per step ran on the device
+
+
+@pytest.mark.parametrize("name", ["pml_rigid", "porous_ground", "tdbc_east", "moving_frame", "wind_log", "hill1"])
+def test_fp32_within_tolerance(name, case_dirs):
+    d, rec, n = case_dirs[name]
+    ref = oracle.run_case(d, rec, n)
+    got = _gpu_run(d, rec, n, "f32")
+    assert rel_l2(got["receivers"], ref["receivers"]) <= TOL_F32
+    assert rel_l2(got["p"], ref["p"]) <= TOL_F32
+
+
+def test_half_steps_match_full_step(case_dirs):
+    """Cal_pressure + Cal_velocity (half steps) equal one time-loop step."""
+    d, rec, _ = case_dirs["tdbc_east"]
+    with pkg.Airpore(d, "f64") as a:
+        a.reset(10)
+        for _ in range(5):
+            a.Cal_pressure()
+            a.Cal_velocity()
+        p_half = a.field("p")
+    with pkg.Airpore(d, "f64") as b:
+        b.get_output(5)
+        p_full = b.field("p")
+    assert np.array_equal(p_half, p_full)
+
+
+def test_pressure_half_step_matches_oracle(case_dirs):
+    """After one Cal_pressure, the new pressure level (p_nn) equals the
+    oracle's p after one full step (the velocity half step does not touch p)."""
+    d, rec, _ = case_dirs["porous_ground"]
+    ref = oracle.run_case(d, rec, 1)
+    with pkg.Airpore(d, "f64") as a:
+        a.reset(1)
+        a.Cal_pressure()
+        assert rel_l2(a.field("p", level="nn"), ref["p"]) <= TOL_F64
+        assert rel_l2(a.field("p", "pore", level="nn"), ref["pore_p"]) <= TOL_F64
+
+
+def test_linearity_exact(case_dirs):
+    """The update is linear and x2 is exact in binary floating point, so
+    doubling the initial pressure doubles every output bit for bit."""
+    d, rec, n = case_dirs["porous_tdbc_fine_pore"]
+    with pkg.Airpore(d, "f64") as a:
+        a.set_receivers(rec)
+        a.reset(n)
+        r1 = a.advance(n)
+        p1 = a.field("p")
+        a.reset(n)
+        pa, pp = a.field("p"), a.field("p", "pore")  # read both before writing: they share two rows
+        a.set_field("p", 2.0 * pa)
+        a.set_field("p", 2.0 * pp, "pore")
+        r2 = a.advance(n)
+        p2 = a.field("p")
+    assert np.array_equal(r2, 2.0 * r1)
+    assert np.array_equal(p2, 2.0 * p1)
+
+
+def test_errors_are_reported(tmp_path):
+    with pytest.raises(pkg.FdtdError) as e:
+        pkg.Airpore(str(tmp_path / "missing"), "f64")
+    assert e.value.code == pkg.FDTD_ERR_INPUT
+    c, rec = cases.pml_rigid()
+    c.scheme = 5  # RK4: the reference prints "wrong with scheme name" and never steps
+    d = str(tmp_path / "rk4")
+    c.write(d)
+    with pytest.raises(pkg.FdtdError) as e:
+        pkg.Airpore(d, "f64")
+    assert e.value.code == pkg.FDTD_ERR_UNSUPPORTED
+
+
+def test_horizon_state_error(case_dirs):
+    d, rec, _ = case_dirs["pml_rigid"]
+    with pkg.Airpore(d, "f64") as a:
+        a.reset(3)
+        a.advance(3)
+        with pytest.raises(pkg.FdtdError) as e:
+            a.advance(1)
+        assert e.value.code == pkg.FDTD_ERR_STATE
+
+
+def test_nonfinite_watchdog(case_dirs):
+    """A non-finite pressure is reported with FDTD_ERR_NONFINITE (host-side
+    check of a device flag; the context stays usable)."""
+    d, rec, _ = case_dirs["pml_rigid"]
+    with pkg.Airpore(d, "f64") as a:
+        a.reset(5)
+        p = a.field("p")
+        p[5, 10, 5] = np.inf
+        a.set_field("p", p)
+        with pytest.raises(pkg.FdtdError) as e:
+            a.advance(2)
+        assert e.value.code == pkg.FDTD_ERR_NONFINITE
+        a.reset(5)
+        a.advance(2)  # usable after the error
