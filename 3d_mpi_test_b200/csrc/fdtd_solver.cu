@@ -98,6 +98,7 @@ T* dalloc(size_t n) {
     if (n == 0) n = 1;
     FDTD_CK(cudaMalloc(&p, n * sizeof(T)));
     FDTD_CK(cudaMemset(p, 0, n * sizeof(T)));
+    FDTD_CK(cudaDeviceSynchronize());  // the legacy-stream memset completes before any stream work
     return p;
 }
 
@@ -137,10 +138,14 @@ class SolverImpl final : public SolverImplBase {
         if (prop.major != 10) fail(-3, "this build targets sm_100a (B200); device is sm_" + std::to_string(prop.major) +
                                            std::to_string(prop.minor));
         validate_and_build_geometry();
-        allocate();
+        // every transfer below is ordered on this stream, so host uploads at
+        // frame boundaries never overtake kernels still queued for the
+        // previous frame
         FDTD_CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
         FDTD_CK(cudaEventCreate(&ev0_));
         FDTD_CK(cudaEventCreate(&ev1_));
+        allocate();
+        FDTD_CK(cudaDeviceSynchronize());
         reset(in.time_domain);
     }
 
@@ -443,7 +448,7 @@ class SolverImpl final : public SolverImplBase {
         const size_t W = static_cast<size_t>(NJ_) * Kair_;
         d_Uw_ = track(dalloc<R>(W)); d_Vw_ = track(dalloc<R>(W)); d_Ww_ = track(dalloc<R>(W));
         d_mask_ = mask_on_ ? track(dalloc<int8_t>(mask_.size())) : nullptr;
-        if (mask_on_) FDTD_CK(cudaMemcpy(d_mask_, mask_.data(), mask_.size(), cudaMemcpyHostToDevice));
+        if (mask_on_) h2d(d_mask_, mask_.data(), mask_.size());
         const size_t P = static_cast<size_t>(NI_) * Kair_ * 6;
         d_psi_[0] = track(dalloc<double>(P)); d_psi_[1] = track(dalloc<double>(P));
         d_rec_node_ = track(dalloc<long long>(kMaxRec));
@@ -454,8 +459,8 @@ class SolverImpl final : public SolverImplBase {
         upload(d_axP_, porous_ ? pore_.fx : air_.fx);
         upload(d_sx_[0], sx_); upload(d_sx_[1], fx_); upload(d_sx_[2], gx_);
         upload(d_sz_[0], sz_); upload(d_sz_[1], fz_); upload(d_sz_[2], gz_);
-        FDTD_CK(cudaMemcpy(d_sdx_, sdx_.data(), NI_, cudaMemcpyHostToDevice));
-        FDTD_CK(cudaMemcpy(d_sdz_, sdz_.data(), Kair_, cudaMemcpyHostToDevice));
+        h2d(d_sdx_, sdx_.data(), NI_);
+        h2d(d_sdz_, sdz_.data(), Kair_);
         std::vector<double> az(NG_, 0.0);
         for (int g = 0; g < NG_; ++g) az[g] = (g < gAir0_) ? pore_.fz[g] : air_.fz[g - gOff_];
         upload(d_azG_, az);
@@ -463,8 +468,19 @@ class SolverImpl final : public SolverImplBase {
 
     void upload(R* dst, const std::vector<double>& src) {
         std::vector<R> t(src.begin(), src.end());
-        FDTD_CK(cudaMemcpy(dst, t.data(), t.size() * sizeof(R), cudaMemcpyHostToDevice));
+        h2d(dst, t.data(), t.size() * sizeof(R));
     }
+
+    // stream-ordered host -> device copy; pageable sources are staged before
+    // the call returns, so the host buffer may be released right after
+    void h2d(void* dst, const void* src, size_t bytes) {
+        FDTD_CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream_));
+    }
+    void d2h(void* dst, const void* src, size_t bytes) {
+        FDTD_CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, stream_));
+        FDTD_CK(cudaStreamSynchronize(stream_));
+    }
+    void zero(void* dst, size_t bytes) { FDTD_CK(cudaMemsetAsync(dst, 0, bytes, stream_)); }
 
     // frame-dependent data: Y, y metrics, y PML profile, wind, receivers
     void upload_frame(int N) {
@@ -481,7 +497,7 @@ class SolverImpl final : public SolverImplBase {
         }
         build_pml_y(N);
         upload(d_sy_[0], sy_); upload(d_sy_[1], fy_); upload(d_sy_[2], gy_);
-        FDTD_CK(cudaMemcpy(d_sdy_, sdy_.data(), NJ_, cudaMemcpyHostToDevice));
+        h2d(d_sdy_, sdy_.data(), NJ_);
         if (wind_on_) {
             const size_t W = static_cast<size_t>(NJ_) * Kair_;
             std::vector<double> U(W), V(W), Wv(W);
@@ -508,7 +524,7 @@ class SolverImpl final : public SolverImplBase {
                     node[r] = static_cast<long long>((static_cast<size_t>(kk + gOff_) * NI_ + ii) * NJ_ + jl);
             }
         }
-        FDTD_CK(cudaMemcpy(d_rec_node_, node.data(), sizeof(long long) * kMaxRec, cudaMemcpyHostToDevice));
+        h2d(d_rec_node_, node.data(), sizeof(long long) * kMaxRec);
     }
 
     std::vector<int> set_receivers(const std::vector<double>& xyz) override {
@@ -560,6 +576,7 @@ class SolverImpl final : public SolverImplBase {
     // initial condition: Gaussian pulse, calculation_2D.cpp:292-314
     void reset(int horizon) override {
         FDTD_CK(cudaSetDevice(device_));
+        FDTD_CK(cudaStreamSynchronize(stream_));
         horizon_ = horizon;
         realloc_rec();
         const size_t N = nodes_;
@@ -576,18 +593,18 @@ class SolverImpl final : public SolverImplBase {
                     p[(static_cast<size_t>(g) * NI_ + i) * NJ_ + j] = static_cast<R>(1.0 * std::exp(-gc * rr * rr));
                 }
         }
-        FDTD_CK(cudaMemcpy(F_[0][3], p.data(), N * sizeof(R), cudaMemcpyHostToDevice));
-        for (int c = 0; c < 3; ++c) FDTD_CK(cudaMemset(F_[0][c], 0, N * sizeof(R)));
-        for (int c = 0; c < 4; ++c) FDTD_CK(cudaMemset(F_[1][c], 0, N * sizeof(R)));
+        h2d(F_[0][3], p.data(), N * sizeof(R));
+        for (int c = 0; c < 3; ++c) zero(F_[0][c], N * sizeof(R));
+        for (int c = 0; c < 4; ++c) zero(F_[1][c], N * sizeof(R));
         for (int s = 0; s < 6; ++s)
             for (int b = 0; b < 2; ++b)
                 for (int c = 0; c < 4; ++c)
-                    if (Q_[s][b][c]) FDTD_CK(cudaMemset(Q_[s][b][c], 0, slab_n_[s] * sizeof(R)));
+                    if (Q_[s][b][c]) zero(Q_[s][b][c], slab_n_[s] * sizeof(R));
         const size_t P = static_cast<size_t>(NI_) * Kair_ * 6;
-        FDTD_CK(cudaMemset(d_psi_[0], 0, P * sizeof(double)));
-        FDTD_CK(cudaMemset(d_psi_[1], 0, P * sizeof(double)));
-        FDTD_CK(cudaMemset(d_counters_, 0, 2 * sizeof(int)));
-        FDTD_CK(cudaMemset(d_status_, 0, sizeof(int)));
+        zero(d_psi_[0], P * sizeof(double));
+        zero(d_psi_[1], P * sizeof(double));
+        zero(d_counters_, 2 * sizeof(int));
+        zero(d_status_, sizeof(int));
         par_ = 0;
         steps_ = 0;
         mf_count_ = 0;
@@ -806,11 +823,11 @@ class SolverImpl final : public SolverImplBase {
         FDTD_CK(cudaEventElapsedTime(&ms, ev0_, ev1_));
         last_ms_ = ms;
         int st = 0;
-        FDTD_CK(cudaMemcpy(&st, d_status_, sizeof(int), cudaMemcpyDeviceToHost));
+        d2h(&st, d_status_, sizeof(int));
         const int taken = steps_ - start;
         if (rec_out && !rec_idx_.empty() && taken > 0) {
-            FDTD_CK(cudaMemcpy(rec_out, d_rec_out_ + static_cast<size_t>(start) * rec_idx_.size(),
-                               sizeof(double) * taken * rec_idx_.size(), cudaMemcpyDeviceToHost));
+            d2h(rec_out, d_rec_out_ + static_cast<size_t>(start) * rec_idx_.size(),
+                sizeof(double) * taken * rec_idx_.size());
         }
         if (st & 1) fail(-4, "pressure became non-finite");
         return taken;
@@ -841,7 +858,7 @@ class SolverImpl final : public SolverImplBase {
     // ------------------------------------------------------- read-out
     std::vector<R> fetch(const R* d, size_t n) {
         std::vector<R> h(n);
-        FDTD_CK(cudaMemcpy(h.data(), d, n * sizeof(R), cudaMemcpyDeviceToHost));
+        d2h(h.data(), d, n * sizeof(R));
         return h;
     }
 
@@ -882,11 +899,12 @@ class SolverImpl final : public SolverImplBase {
                 for (int k = 0; k < K; ++k)
                     h[(static_cast<size_t>(k + g0) * NI_ + i) * NJ_ + j] =
                         static_cast<R>(src[(static_cast<size_t>(i) * J + j) * K + k]);
-        FDTD_CK(cudaMemcpy(dptr, h.data(), nodes_ * sizeof(R), cudaMemcpyHostToDevice));
+        h2d(dptr, h.data(), nodes_ * sizeof(R));
+        FDTD_CK(cudaStreamSynchronize(stream_));
     }
 
     void get_psi(double* out) override {
-        FDTD_CK(cudaMemcpy(out, d_psi_[par_], sizeof(double) * NI_ * Kair_ * 6, cudaMemcpyDeviceToHost));
+        d2h(out, d_psi_[par_], sizeof(double) * NI_ * Kair_ * 6);
     }
 
     int get_slab(int s, int comp, double* out, int* dims) override {
