@@ -35,7 +35,7 @@ EXPORTS = (
     "fdtd_create", "fdtd_destroy", "fdtd_dims", "fdtd_last_error", "fdtd_set_receivers", "fdtd_reset",
     "fdtd_run", "fdtd_advance", "fdtd_step_pressure", "fdtd_step_velocity", "fdtd_get_field",
     "fdtd_set_field", "fdtd_get_psi", "fdtd_get_slab", "fdtd_state_elems", "fdtd_copy_state",
-    "fdtd_launch_count", "fdtd_last_device_ms",
+    "fdtd_launch_count", "fdtd_last_device_ms", "fdtd_fb_step_noalloc",
 )
 
 
@@ -78,6 +78,7 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
         "fdtd_copy_state": ([vp, i, vp], i),
         "fdtd_launch_count": ([vp], ctypes.c_longlong),
         "fdtd_last_device_ms": ([vp, dp], i),
+        "fdtd_fb_step_noalloc": ([i, i, i, i, dp, dp, dp] + [ctypes.c_double] * 7 + [vp] * 9, i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)

@@ -38,6 +38,11 @@ int bad(const char* msg) {
 }
 }  // namespace
 
+namespace fdtd {
+// lets entry points outside this file report through fdtd_last_error()
+void set_last_error(const char* msg) { g_last_error = msg; }
+}  // namespace fdtd
+
 extern "C" {
 
 const char* fdtd_last_error(void) { return g_last_error.c_str(); }

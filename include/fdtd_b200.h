@@ -109,6 +109,28 @@ long long fdtd_launch_count(const fdtd_solver *h);
 /* CUDA events around the last fdtd_advance's device work: milliseconds. */
 int fdtd_last_device_ms(const fdtd_solver *h, double *ms);
 
+/* Allocation-free single FB_p_v step. No counterpart in the reference: it
+ * serves callers that cannot allocate device memory (a host that owns all
+ * device memory through its own pool, or code that must avoid the implicit
+ * synchronisation of cudaMalloc/cudaFree). One forward-backward step of a
+ * rigid-walled air box (no PML, wind, TDBC or porous ground), the same
+ * kernels as the handle path, on caller-owned device buffers in the native
+ * layout [k][i][j] (j fastest), FDTD_F64 or FDTD_F32 elements. X, Y, Z are
+ * host coordinate arrays (NI, NJ, NK nodes); dx dy dz the input.txt
+ * spacings; stream a cudaStream_t (NULL: legacy default stream). It
+ * allocates nothing: its scratch is a fixed 128 KiB __device__ array
+ * compiled into the library, so each axis is limited to 4096 nodes
+ * (larger grids return FDTD_ERR_ARG). The first call on a device resolves
+ * that array's device address (make it before any stream capture). All
+ * calls share the array and reset it themselves; calls that overlap on the
+ * GPU race and must be serialised by the caller. Synchronises the stream
+ * before returning; FDTD_ERR_NONFINITE if the new pressure is not finite. */
+int fdtd_fb_step_noalloc(int precision, int NI, int NJ, int NK, const double *X, const double *Y,
+                         const double *Z, double dx, double dy, double dz, double dt, double gamma,
+                         double P0, double c0, const void *u_in, const void *v_in, const void *w_in,
+                         const void *p_in, void *u_out, void *v_out, void *w_out, void *p_out,
+                         void *stream);
+
 #ifdef __cplusplus
 }
 #endif
