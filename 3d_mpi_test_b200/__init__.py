@@ -35,7 +35,7 @@ EXPORTS = (
     "fdtd_create", "fdtd_destroy", "fdtd_dims", "fdtd_last_error", "fdtd_set_receivers", "fdtd_reset",
     "fdtd_run", "fdtd_advance", "fdtd_step_pressure", "fdtd_step_velocity", "fdtd_get_field",
     "fdtd_set_field", "fdtd_get_psi", "fdtd_get_slab", "fdtd_state_elems", "fdtd_copy_state",
-    "fdtd_launch_count", "fdtd_last_device_ms", "fdtd_fb_step_noalloc",
+    "fdtd_launch_count", "fdtd_last_device_ms", "fdtd_fb_step_noalloc", "fdtd_set_tiling", "fdtd_autotune",
 )
 
 
@@ -79,6 +79,8 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
         "fdtd_launch_count": ([vp], ctypes.c_longlong),
         "fdtd_last_device_ms": ([vp, dp], i),
         "fdtd_fb_step_noalloc": ([i, i, i, i, dp, dp, dp] + [ctypes.c_double] * 7 + [vp] * 9, i),
+        "fdtd_set_tiling": ([vp, i, i, i, i], i),
+        "fdtd_autotune": ([vp, i, ip], i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -208,6 +210,16 @@ class Airpore:
 
     def copy_state(self, host: np.ndarray, to_device: bool) -> None:
         self._check(self._L.fdtd_copy_state(self._h, 1 if to_device else 0, host.ctypes.data_as(ctypes.c_void_p)))
+
+    def set_tiling(self, rows_per_block: int, planes_per_block: int, threads_per_block: int,
+                   variant: int = 1) -> None:
+        """Tile of the fused pass; variant 0 plain loads, 1 bulk-copy staging."""
+        self._check(self._L.fdtd_set_tiling(self._h, rows_per_block, planes_per_block, threads_per_block, variant))
+
+    def autotune(self, nsteps: int = 20) -> Tuple[int, int, int, int]:
+        best = (ctypes.c_int * 4)()
+        self._check(self._L.fdtd_autotune(self._h, nsteps, best))
+        return tuple(best)
 
     def launch_count(self) -> int:
         return int(self._L.fdtd_launch_count(self._h))

@@ -140,6 +140,19 @@ int fdtd_copy_state(fdtd_solver* h, int dir, void* host) {
     return guard([&] { h->s->copy_state(dir, host); });
 }
 
+int fdtd_set_tiling(fdtd_solver* h, int rows_per_block, int planes_per_block, int threads_per_block, int variant) {
+    if (!h) return bad("null handle");
+    return guard([&] { h->s->set_tiling(rows_per_block, planes_per_block, threads_per_block, variant); });
+}
+
+int fdtd_autotune(fdtd_solver* h, int nsteps, int* best) {
+    if (!h || !best || nsteps <= 0) return bad("bad autotune arguments");
+    return guard([&] {
+        const auto b = h->s->autotune(nsteps);
+        for (int q = 0; q < 4; ++q) best[q] = b[q];
+    });
+}
+
 long long fdtd_launch_count(const fdtd_solver* h) { return h ? h->s->launch_count() : 0; }
 
 int fdtd_last_device_ms(const fdtd_solver* h, double* ms) {

@@ -41,6 +41,7 @@ struct Slab {
 template <typename R>
 struct Dev {
     int NI, NJ, NG;
+    int NJP;     // row pitch of the field arrays (>= NJ; 16-byte rows for bulk copies)
     int porous;  // porous ground stacked below the air
     int gAir0;   // first g owned by the air medium
     int gOff;    // air k = g - gOff
@@ -90,8 +91,19 @@ struct Dev {
     int* status;                // bit 0: non-finite pressure seen
 
     __device__ __forceinline__ size_t ix(int g, int i, int j) const {
-        return (static_cast<size_t>(g) * NI + i) * NJ + j;
+        return (static_cast<size_t>(g) * NI + i) * NJP + j;
     }
+};
+
+// Reads of the step's input fields (u, v, w and the old pressure) at
+// (i, j, g) straight from global memory.
+template <typename R>
+struct GlobalFields {
+    const Dev<R>& d;
+    __device__ __forceinline__ R u(int i, int j, int g) const { return d.u_in[d.ix(g, i, j)]; }
+    __device__ __forceinline__ R v(int i, int j, int g) const { return d.v_in[d.ix(g, i, j)]; }
+    __device__ __forceinline__ R w(int i, int j, int g) const { return d.w_in[d.ix(g, i, j)]; }
+    __device__ __forceinline__ R p(int i, int j, int g) const { return d.pold[d.ix(g, i, j)]; }
 };
 
 // ---------------------------------------------------------------- helpers
@@ -109,23 +121,18 @@ __device__ __forceinline__ int y_side(const Dev<R>& d, int j, bool y1_on) {
 // Pressure at an interior node of either medium: p_n + increment.
 // Air: air::cal_fp (air.cpp:1953-2322); pore: porous::cal_fp (porous.cpp:107-143);
 // accumulation: calculation_2D::Cal_pressure (calculation_2D.cpp:581-613).
-template <typename R, bool WIND>
-__device__ R fresh_p(const Dev<R>& d, int i, int j, int g, bool y1_on) {
-    const size_t c = d.ix(g, i, j);
-    const size_t sI = d.NJ, sG = static_cast<size_t>(d.NI) * d.NJ;
-    const R* u = d.u_in;
-    const R* v = d.v_in;
-    const R* w = d.w_in;
-    const R u0 = u[c], v0 = v[c], w0 = w[c];
+template <typename R, bool WIND, typename F>
+__device__ R fresh_p(const Dev<R>& d, const F& f, int i, int j, int g, bool y1_on) {
+    const R u0 = f.u(i, j, g), v0 = f.v(i, j, g), w0 = f.w(i, j, g);
     const R az = ldg(d.azG + g);
-    const R pn = d.pold[c];
+    const R pn = f.p(i, j, g);
     if (g < d.gAir0) {  // porous ground
         const R ax = ldg(d.axP + i), ay = ldg(d.ayP + j);
-        const R div = ax * (u[c + sI] - u0) + ay * (v[c + 1] - v0) + az * (w[c + sG] - w0);
+        const R div = ax * (f.u(i + 1, j, g) - u0) + ay * (f.v(i, j + 1, g) - v0) + az * (f.w(i, j, g + 1) - w0);
         return pn - d.pGama * div;
     }
     const R ax = ldg(d.axA + i), ay = ldg(d.ayA + j);
-    const R gu = ax * (u[c + sI] - u0), gv = ay * (v[c + 1] - v0), gw = az * (w[c + sG] - w0);
+    const R gu = ax * (f.u(i + 1, j, g) - u0), gv = ay * (f.v(i, j + 1, g) - v0), gw = az * (f.w(i, j, g + 1) - w0);
     const int k = g - d.gOff;
     const int8_t* m = d.mask;
     if (m && i >= d.mi0 && i <= d.mi1 && j >= d.mj0 && j <= d.mj1 && k >= d.mk0 && k <= d.mk1) {
@@ -138,7 +145,7 @@ __device__ R fresh_p(const Dev<R>& d, int i, int j, int g, bool y1_on) {
     if (WIND) {
         const size_t wk = static_cast<size_t>(k) * d.NJ + j, wS = d.NJ;
         const R U = ldg(d.Uw + wk), V = ldg(d.Vw + wk), W = ldg(d.Ww + wk);
-        const R pim = d.pold[c - sI], pjm = d.pold[c - 1], pkm = d.pold[c - sG];
+        const R pim = f.p(i - 1, j, g), pjm = f.p(i, j - 1, g), pkm = f.p(i, j, g - 1);
         dp += -(U * ax * d.dt) * (pn - pim) - (V * ay * d.dt) * (pn - pjm) - (W * az * d.dt) * (pn - pkm);
         const R dVdY = ay * (ldg(d.Vw + wk + 1) - ldg(d.Vw + wk - 1)) * R(0.5);
         const R dWdZ = az * (ldg(d.Ww + wk + wS) - ldg(d.Ww + wk - wS)) * R(0.5);
@@ -199,14 +206,16 @@ struct Vel3 {
 // scheme prescribes (p_nn for FB_p_v). Air: air::cal_fuvw (air.cpp:1476-1949);
 // pore: porous::cal_fuvw (porous.cpp:58-104); accumulation:
 // calculation_2D::Cal_velocity (calculation_2D.cpp:548-579).
-template <typename R, bool WIND>
-__device__ Vel3<R> fresh_vel(const Dev<R>& d, int i, int j, int g, bool y1_on) {
-    const size_t c = d.ix(g, i, j);
-    const size_t sI = d.NJ, sG = static_cast<size_t>(d.NI) * d.NJ;
-    const R* p = d.p_in;
-    const R u0 = d.u_in[c], v0 = d.v_in[c], w0 = d.w_in[c];
-    const R p0 = p[c];
-    const R bpi = p0 - p[c - sI], bpj = p0 - p[c - 1], bpk = p0 - p[c - sG];
+//
+// p0, pim, pjm, pkm: the scheme's pressure at the node and its i-1, j-1,
+// g-1 neighbours. qp_old: the slabs' Qp buffers still hold the values from
+// before this step's pressure update (fused pass), so the advanced Qp is
+// formed here as Qp + dt * p, the expression of air::Update_PML_Qp.
+template <typename R, bool WIND, typename F>
+__device__ Vel3<R> fresh_vel_core(const Dev<R>& d, const F& f, int i, int j, int g, bool y1_on, R p0, R pim, R pjm,
+                                  R pkm, bool qp_old) {
+    const R u0 = f.u(i, j, g), v0 = f.v(i, j, g), w0 = f.w(i, j, g);
+    const R bpi = p0 - pim, bpj = p0 - pjm, bpk = p0 - pkm;
     const R az = ldg(d.azG + g);
     Vel3<R> r;
     if (g < d.gAir0) {
@@ -233,15 +242,12 @@ __device__ Vel3<R> fresh_vel(const Dev<R>& d, int i, int j, int g, bool y1_on) {
     }
     R du = -d.Aavdt * gpX, dv = -d.Aavdt * gpY, dw = -d.Aavdt * gpZ;
     if (WIND) {
-        const R* u = d.u_in;
-        const R* v = d.v_in;
-        const R* w = d.w_in;
         const size_t wk = static_cast<size_t>(k) * d.NJ + j, wS = d.NJ;
         const R U = ldg(d.Uw + wk), V = ldg(d.Vw + wk), W = ldg(d.Ww + wk);
         const R c1 = U * ax * d.dt, c2 = V * ay * d.dt, c3 = W * az * d.dt;
-        du += -c1 * (u[c + sI] - u0) - c2 * (u[c + 1] - u0) - c3 * (u[c + sG] - u0);
-        dv += -c1 * (v[c + sI] - v0) - c2 * (v[c + 1] - v0) - c3 * (v[c + sG] - v0);
-        dw += -c1 * (w[c + sI] - w0) - c2 * (w[c + 1] - w0) - c3 * (w[c + sG] - w0);
+        du += -c1 * (f.u(i + 1, j, g) - u0) - c2 * (f.u(i, j + 1, g) - u0) - c3 * (f.u(i, j, g + 1) - u0);
+        dv += -c1 * (f.v(i + 1, j, g) - v0) - c2 * (f.v(i, j + 1, g) - v0) - c3 * (f.v(i, j, g + 1) - v0);
+        dw += -c1 * (f.w(i + 1, j, g) - w0) - c2 * (f.w(i, j + 1, g) - w0) - c3 * (f.w(i, j, g + 1) - w0);
         const R h = R(0.5);
         const R dUdY = ay * (ldg(d.Uw + wk + 1) - ldg(d.Uw + wk - 1)) * h;
         const R dUdZ = az * (ldg(d.Uw + wk + wS) - ldg(d.Uw + wk - wS)) * h;
@@ -260,13 +266,20 @@ __device__ Vel3<R> fresh_vel(const Dev<R>& d, int i, int j, int g, bool y1_on) {
         const Slab<R>* SY = ys ? &d.sl[ys + 1] : nullptr;
         const Slab<R>* SZ = zs ? &d.sl[zs + 3] : nullptr;
         const R A = d.Aav, dt = d.dt;
-        // backward differences of the slab's Qp (already advanced this step)
+        // backward differences of the slab's Qp advanced to this step
         auto bq = [&](const Slab<R>* S, size_t q, R& bx, R& by, R& bz) {
             const R* Q = S->rd[3];
-            const R q0 = Q[q];
-            bx = ax * (q0 - Q[q - S->nj]);
-            by = ay * (q0 - Q[q - 1]);
-            bz = az * (q0 - Q[q - static_cast<size_t>(S->ni) * S->nj]);
+            const size_t sk = static_cast<size_t>(S->ni) * S->nj;
+            R q0 = Q[q], qi = Q[q - S->nj], qj = Q[q - 1], qk = Q[q - sk];
+            if (qp_old) {
+                q0 = q0 + dt * p0;
+                qi = qi + dt * pim;
+                qj = qj + dt * pjm;
+                qk = qk + dt * pkm;
+            }
+            bx = ax * (q0 - qi);
+            by = ay * (q0 - qj);
+            bz = az * (q0 - qk);
         };
         R bxX = 0, byX = 0, bzX = 0, bxY = 0, byY = 0, bzY = 0, bxZ = 0, byZ = 0, bzZ = 0;
         size_t qx = 0, qy = 0;
@@ -315,6 +328,15 @@ __device__ Vel3<R> fresh_vel(const Dev<R>& d, int i, int j, int g, bool y1_on) {
     return r;
 }
 
+// Velocity with the scheme's pressure read from global memory and the Qp
+// slabs already advanced (two-pass path).
+template <typename R, bool WIND>
+__device__ Vel3<R> fresh_vel(const Dev<R>& d, int i, int j, int g, bool y1_on) {
+    const R* p = d.p_in;
+    return fresh_vel_core<R, WIND>(d, GlobalFields<R>{d}, i, j, g, y1_on, p[d.ix(g, i, j)], p[d.ix(g, i - 1, j)],
+                                   p[d.ix(g, i, j - 1)], p[d.ix(g - 1, i, j)], false);
+}
+
 // ------------------------------------------------ boundary resolution
 // Final pressure at any node. Faces copy from the inward neighbour and the
 // east face extrapolates 15/8, -5/4, 3/8 (calculation_2D.cpp:646-721), so
@@ -333,12 +355,13 @@ __device__ R final_p(const Dev<R>& d, int i, int j, int g, bool y1_on) {
     }
     const int jc = j < 1 ? 1 : j;
     if (jc == d.NJ - 1) {
-        const R a = fresh_p<R, WIND>(d, ic, d.NJ - 2, gc, y1_on);
-        const R b = fresh_p<R, WIND>(d, ic, d.NJ - 3, gc, y1_on);
-        const R e = fresh_p<R, WIND>(d, ic, d.NJ - 4, gc, y1_on);
+        const GlobalFields<R> gf{d};
+        const R a = fresh_p<R, WIND>(d, gf, ic, d.NJ - 2, gc, y1_on);
+        const R b = fresh_p<R, WIND>(d, gf, ic, d.NJ - 3, gc, y1_on);
+        const R e = fresh_p<R, WIND>(d, gf, ic, d.NJ - 4, gc, y1_on);
         return R(15.0 / 8.0) * a - R(5.0 / 4.0) * b + R(3.0 / 8.0) * e;
     }
-    return fresh_p<R, WIND>(d, ic, jc, gc, y1_on);
+    return fresh_p<R, WIND>(d, GlobalFields<R>{d}, ic, jc, gc, y1_on);
 }
 
 // TDBC normal velocity at east-face node (i, air k), Cal_TDBC
@@ -357,8 +380,15 @@ __device__ double tdbc_v(const Dev<R>& d, int i, int k, double p) {
 // calculation_2D.cpp:387-403) and advances the Qp slabs (air::Update_PML_Qp,
 // air.cpp:2388-2439).
 template <typename R, bool WIND>
-__global__ void __launch_bounds__(256) k_pressure(__grid_constant__ const Dev<R> d, int first_pass) {
-    const int step = first_pass ? d.counters[0] : d.counters[1] - 1;
+// pass_code: bit 0 = first pass of the step, bit 1 = parity of the step.
+// Step counters: the first pass reads counters[par] and publishes the step to
+// the second pass through counters[par ^ 1]; the second pass sets
+// counters[par] too. A launch never writes a word its own blocks read, and
+// after every step counters[next parity] holds the next step index (the
+// fused kernel keeps the same invariant).
+__global__ void __launch_bounds__(256) k_pressure(__grid_constant__ const Dev<R> d, int pass_code) {
+    const int first_pass = pass_code & 1, par = (pass_code >> 1) & 1;
+    const int step = first_pass ? d.counters[par] : d.counters[par ^ 1] - 1;
     const bool y1_on = step + 1 >= d.pml_y_time;
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = blockIdx.y * blockDim.y + threadIdx.y;
@@ -372,12 +402,9 @@ __global__ void __launch_bounds__(256) k_pressure(__grid_constant__ const Dev<R>
             if (fabs(val) < 1.0e-100) val = 0.0;
             d.rec_out[static_cast<size_t>(step) * d.nrec + t] = val;
         }
-        // pass 1 publishes the step to pass 2 through counters[1]; pass 2
-        // advances counters[0] for the next step (no block reads the word
-        // that this pass writes)
         if (t == 0) {
-            if (first_pass) d.counters[1] = step + 1;
-            else d.counters[0] = step + 1;
+            if (first_pass) d.counters[par ^ 1] = step + 1;
+            else d.counters[par] = step + 1;
         }
     }
     if (j >= d.NJ || i >= d.NI) return;
@@ -403,15 +430,16 @@ __global__ void __launch_bounds__(256) k_pressure(__grid_constant__ const Dev<R>
 // calculation_2D.cpp:777-864), the east TDBC (calculation_2D.cpp:986-1017)
 // and advances Qu/Qv/Qw (air::Update_PML_Qvw, air.cpp:2323-2386).
 template <typename R, bool WIND>
-__global__ void __launch_bounds__(256) k_velocity(__grid_constant__ const Dev<R> d, int first_pass) {
-    const int step = first_pass ? d.counters[0] : d.counters[1] - 1;
+__global__ void __launch_bounds__(256) k_velocity(__grid_constant__ const Dev<R> d, int pass_code) {
+    const int first_pass = pass_code & 1, par = (pass_code >> 1) & 1;
+    const int step = first_pass ? d.counters[par] : d.counters[par ^ 1] - 1;
     const bool y1_on = step + 1 >= d.pml_y_time;
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = blockIdx.y * blockDim.y + threadIdx.y;
     const int g = blockIdx.z;
     if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0 && threadIdx.y == 0) {
-        if (first_pass) d.counters[1] = step + 1;
-        else d.counters[0] = step + 1;
+        if (first_pass) d.counters[par ^ 1] = step + 1;
+        else d.counters[par] = step + 1;
     }
     if (j >= d.NJ || i >= d.NI) return;
     const bool pore = g < d.gAir0;

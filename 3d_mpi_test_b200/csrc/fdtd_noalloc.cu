@@ -112,7 +112,7 @@ int step(int NI, int NJ, int NK, const double* X, const double* Y, const double*
     if (e != cudaSuccess) return fail(FDTD_ERR_CUDA, cudaGetErrorString(e));
 
     fdtd::Dev<R> d{};
-    d.NI = NI; d.NJ = NJ; d.NG = NK;
+    d.NI = NI; d.NJ = NJ; d.NG = NK; d.NJP = NJ;  // caller rows are unpadded
     d.porous = 0; d.gAir0 = 0; d.gOff = 0; d.Kair = NK;
     d.rigid_south = 1; d.tdbc = 0; d.fbvp = 0;
     d.axA = dfac; d.ayA = dfac + kNoAllocMaxAxis; d.azG = dfac + 2 * kNoAllocMaxAxis;

@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include "fdtd_device.cuh"
+#include "fdtd_fused.cuh"
 
 namespace fdtd {
 
@@ -123,6 +124,8 @@ class SolverImplBase {
     virtual void copy_state(int dir, void* host) = 0;
     virtual long long launch_count() const = 0;
     virtual double last_device_ms() const = 0;
+    virtual void set_tiling_api(int TI, int GC, int nt, int variant) = 0;
+    virtual std::array<int, 4> autotune(int nsteps) = 0;
 };
 
 template <typename R>
@@ -146,6 +149,9 @@ class SolverImpl final : public SolverImplBase {
         FDTD_CK(cudaEventCreate(&ev1_));
         allocate();
         FDTD_CK(cudaDeviceSynchronize());
+        // FB_p_v runs as one fused pass per step; FB_v_p keeps the two passes
+        fused_ = (in.scheme == FB_P_V);
+        if (fused_) set_tiling(4, 16, std::min(NJ_, 256), 0);
         reset(in.time_domain);
     }
 
@@ -211,6 +217,8 @@ class SolverImpl final : public SolverImplBase {
         }
         NI_ = air_.I;
         NJ_ = air_.J;
+        // field rows padded to 16 bytes so whole rows can move as bulk copies
+        NJP_ = (NJ_ * static_cast<int>(sizeof(R)) + 15) / 16 * 16 / static_cast<int>(sizeof(R));
         Kair_ = air_.K;
         if (porous_) {
             gAir0_ = pore_.K - 1;
@@ -417,7 +425,7 @@ class SolverImpl final : public SolverImplBase {
     }
 
     void allocate() {
-        const size_t N = static_cast<size_t>(NI_) * NJ_ * NG_;
+        const size_t N = static_cast<size_t>(NI_) * NJP_ * NG_;
         nodes_ = N;
         for (int b = 0; b < 2; ++b)
             for (int c = 0; c < 4; ++c) F_[b][c] = track(dalloc<R>(N));
@@ -521,7 +529,7 @@ class SolverImpl final : public SolverImplBase {
             if (jj >= sh && jj < NJ_ + sh) {
                 const int jl = jj - sh;
                 if (jl > 0 && jl < NJ_ - 1 && ii > 0 && ii < NI_ - 1 && kk > 0 && kk < Kair_ - 1)
-                    node[r] = static_cast<long long>((static_cast<size_t>(kk + gOff_) * NI_ + ii) * NJ_ + jl);
+                    node[r] = static_cast<long long>((static_cast<size_t>(kk + gOff_) * NI_ + ii) * NJP_ + jl);
             }
         }
         h2d(d_rec_node_, node.data(), sizeof(long long) * kMaxRec);
@@ -590,7 +598,7 @@ class SolverImpl final : public SolverImplBase {
                 for (int j = 0; j < NJ_; ++j) {
                     const double x = m.X[i] - in.source[0], y = m.axY[j] - in.source[1], zz = m.Z[k] - in.source[2];
                     const double rr = std::sqrt(std::pow(x, 2) + std::pow(y, 2) + std::pow(zz, 2));
-                    p[(static_cast<size_t>(g) * NI_ + i) * NJ_ + j] = static_cast<R>(1.0 * std::exp(-gc * rr * rr));
+                    p[(static_cast<size_t>(g) * NI_ + i) * NJP_ + j] = static_cast<R>(1.0 * std::exp(-gc * rr * rr));
                 }
         }
         h2d(F_[0][3], p.data(), N * sizeof(R));
@@ -618,7 +626,7 @@ class SolverImpl final : public SolverImplBase {
     // params of one pass at parity par
     Dev<R> params(bool pressure, int par) const {
         Dev<R> d{};
-        d.NI = NI_; d.NJ = NJ_; d.NG = NG_;
+        d.NI = NI_; d.NJ = NJ_; d.NG = NG_; d.NJP = NJP_;
         d.porous = porous_; d.gAir0 = gAir0_; d.gOff = gOff_; d.Kair = Kair_;
         d.rigid_south = !porous_;
         d.tdbc = tdbc_;
@@ -689,20 +697,98 @@ class SolverImpl final : public SolverImplBase {
         const dim3 blk(32, 8, 1);
         const dim3 grd((NJ_ + 31) / 32, (NI_ + 7) / 8, NG_);
         const Dev<R> d = params(pressure, par);
-        const int fp = first ? 1 : 0;
+        const int code = (first ? 1 : 0) | (par << 1);
         if (pressure) {
-            if (wind_on_) k_pressure<R, true><<<grd, blk, 0, stream_>>>(d, fp);
-            else k_pressure<R, false><<<grd, blk, 0, stream_>>>(d, fp);
+            if (wind_on_) k_pressure<R, true><<<grd, blk, 0, stream_>>>(d, code);
+            else k_pressure<R, false><<<grd, blk, 0, stream_>>>(d, code);
         } else {
-            if (wind_on_) k_velocity<R, true><<<grd, blk, 0, stream_>>>(d, fp);
-            else k_velocity<R, false><<<grd, blk, 0, stream_>>>(d, fp);
+            if (wind_on_) k_velocity<R, true><<<grd, blk, 0, stream_>>>(d, code);
+            else k_velocity<R, false><<<grd, blk, 0, stream_>>>(d, code);
+        }
+        FDTD_CK(cudaGetLastError());
+        ++launches_;
+    }
+
+    // params of the fused pass at parity par: every read from the time level /
+    // slab buffer of this step, every write to the other one
+    Dev<R> params_fused(int par) const {
+        Dev<R> d = params(true, par);
+        const int o = par, nw = 1 - par;
+        d.u_in = F_[o][0]; d.v_in = F_[o][1]; d.w_in = F_[o][2];
+        d.pold = F_[o][3]; d.p_in = F_[o][3];
+        d.u_out = F_[nw][0]; d.v_out = F_[nw][1]; d.w_out = F_[nw][2]; d.p_out = F_[nw][3];
+        for (int s = 0; s < 6; ++s) {
+            if (!slab_n_[s]) continue;
+            for (int c = 0; c < 4; ++c) { d.sl[s].rd[c] = Q_[s][o][c]; d.sl[s].wr[c] = Q_[s][nw][c]; }
+        }
+        return d;
+    }
+
+    // Tile choice for the fused pass: TI rows x all NJ columns x GC planes per
+    // block; nt threads stride the columns.
+    // shared memory of a fused tile (variant 0: two new-pressure slots;
+    // variant 1: plus the mbarriers and the bulk-copy ring)
+    size_t fused_smem_bytes(const FusedTiling& t, int variant) const {
+        const size_t srows = t.rows_max + 1, sr = t.rows_max + 3;
+        const size_t pslots = 2 * srows * NJ_ * sizeof(R);
+        if (variant == 0) return pslots;
+        return 128 + pslots + 16 + static_cast<size_t>(t.nstage) * 4 * sr * NJP_ * sizeof(R);
+    }
+
+    FusedTiling make_tiling(int TI, int GC) const {
+        FusedTiling t{};
+        t.TI = std::max(2, TI);
+        t.nrb = std::max(1, NI_ / t.TI);
+        t.rows_max = (t.nrb == 1) ? NI_ : t.TI + NI_ % t.TI;
+        t.GC = std::max(1, GC);
+        t.nchunk = (NG_ - 2 + t.GC - 1) / t.GC;
+        t.nstage = 3 + (wind_on_ ? 1 : 0);  // planes g-1 (wind), g, g+1 resident, g+2 in flight
+        return t;
+    }
+
+    // Tile choice for the fused pass: TI rows x all NJ columns x GC planes per
+    // block; nt threads stride the columns; variant 0 plain, 1 bulk-staged.
+    void set_tiling(int TI, int GC, int nt, int variant) {
+        const FusedTiling t = make_tiling(TI, GC);
+        if (variant != 0 && variant != 1) fail(-5, "variant must be 0 (plain) or 1 (bulk-staged)");
+        const size_t smem = fused_smem_bytes(t, variant);
+        if (smem > 227 * 1024) fail(-2, "fused tile does not fit shared memory");
+        nt = std::min(std::max(32, (nt + 31) / 32 * 32), 256);
+        if (smem > 48 * 1024) {
+            const int b = static_cast<int>(smem);
+            if (variant == 0) {
+                FDTD_CK(cudaFuncSetAttribute(k_fused<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+                FDTD_CK(cudaFuncSetAttribute(k_fused<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+            } else {
+                FDTD_CK(cudaFuncSetAttribute(k_fused_tma<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+                FDTD_CK(cudaFuncSetAttribute(k_fused_tma<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+            }
+        }
+        tiling_ = t;
+        fused_threads_ = nt;
+        fused_smem_ = smem;
+        fused_variant_ = variant;
+        graph_dirty_ = true;
+    }
+
+    void launch_fused(int par) {
+        const dim3 grd(tiling_.nrb, tiling_.nchunk, 1), blk(fused_threads_, 1, 1);
+        const Dev<R> d = params_fused(par);
+        if (fused_variant_ == 1) {
+            if (wind_on_) k_fused_tma<R, true><<<grd, blk, fused_smem_, stream_>>>(d, tiling_, par);
+            else k_fused_tma<R, false><<<grd, blk, fused_smem_, stream_>>>(d, tiling_, par);
+        } else {
+            if (wind_on_) k_fused<R, true><<<grd, blk, fused_smem_, stream_>>>(d, tiling_, par);
+            else k_fused<R, false><<<grd, blk, fused_smem_, stream_>>>(d, tiling_, par);
         }
         FDTD_CK(cudaGetLastError());
         ++launches_;
     }
 
     void enqueue_step(int par) {
-        if (in.scheme == FB_P_V) {
+        if (in.scheme == FB_P_V && fused_) {
+            launch_fused(par);
+        } else if (in.scheme == FB_P_V) {
             launch_pass(true, par, true);
             launch_pass(false, par, false);
         } else {
@@ -748,7 +834,7 @@ class SolverImpl final : public SolverImplBase {
         // fields (all media) and p's west copy: calculation_2D.cpp:458-481
         const int rows = NI_ * NG_;
         for (int c = 0; c < 4; ++c) {
-            k_shift_rows<R><<<(rows + 127) / 128, 128, 0, stream_>>>(F_[par_][c], rows, NJ_, sh, lead, tempJ, NJ_,
+            k_shift_rows<R><<<(rows + 127) / 128, 128, 0, stream_>>>(F_[par_][c], rows, NJP_, sh, lead, tempJ, NJ_,
                                                                      c == 3 ? 1 : 0);
             FDTD_CK(cudaGetLastError());
             ++launches_;
@@ -885,7 +971,7 @@ class SolverImpl final : public SolverImplBase {
             for (int j = 0; j < J; ++j)
                 for (int k = 0; k < K; ++k)
                     out[(static_cast<size_t>(i) * J + j) * K + k] =
-                        static_cast<double>(h[(static_cast<size_t>(k + g0) * NI_ + i) * NJ_ + j]);
+                        static_cast<double>(h[(static_cast<size_t>(k + g0) * NI_ + i) * NJP_ + j]);
     }
 
     void set_field(int medium, int comp, const double* src) override {
@@ -897,7 +983,7 @@ class SolverImpl final : public SolverImplBase {
         for (int i = 0; i < I; ++i)
             for (int j = 0; j < J; ++j)
                 for (int k = 0; k < K; ++k)
-                    h[(static_cast<size_t>(k + g0) * NI_ + i) * NJ_ + j] =
+                    h[(static_cast<size_t>(k + g0) * NI_ + i) * NJP_ + j] =
                         static_cast<R>(src[(static_cast<size_t>(i) * J + j) * K + k]);
         h2d(dptr, h.data(), nodes_ * sizeof(R));
         FDTD_CK(cudaStreamSynchronize(stream_));
@@ -945,6 +1031,52 @@ class SolverImpl final : public SolverImplBase {
                 in.scheme == FB_V_P ? 1 : 0, steps_};
     }
     long long launch_count() const override { return launches_; }
+
+    void set_tiling_api(int TI, int GC, int nt, int variant) override {
+        FDTD_CK(cudaSetDevice(device_));
+        if (!fused_) fail(-2, "tiling applies to the fused FB_p_v pass only");
+        set_tiling(TI, GC, nt, variant);
+    }
+
+    // Project autotuner: time every candidate tile on this domain and keep the
+    // fastest. Candidates: variant {plain, bulk-staged} x rows per block
+    // {2, 4, 8} x planes per block chosen so the grid fills the SMs 1, 2 or 4
+    // times x threads {64, 128, 256}; tiles that do not fit are skipped.
+    std::array<int, 4> autotune(int nsteps) override {
+        FDTD_CK(cudaSetDevice(device_));
+        if (!fused_) fail(-2, "autotune applies to the fused FB_p_v pass only");
+        cudaDeviceProp prop{};
+        FDTD_CK(cudaGetDeviceProperties(&prop, device_));
+        const int sms = prop.multiProcessorCount;
+        std::vector<std::array<int, 4>> cands;
+        for (int variant : {0, 1})
+            for (int TI : {2, 4, 8}) {
+                const int nrb = std::max(1, NI_ / TI);
+                for (int waves : {1, 2, 4}) {
+                    const int chunks = std::max(1, (waves * sms + nrb - 1) / nrb);
+                    const int GC = std::max(1, (NG_ - 2 + chunks - 1) / chunks);
+                    for (int nt : {64, 128, 256}) {
+                        if (nt > ((NJ_ + 31) / 32) * 32 && nt != 64) continue;
+                        if (fused_smem_bytes(make_tiling(TI, GC), variant) > 227 * 1024) continue;
+                        cands.push_back({TI, GC, nt, variant});
+                    }
+                }
+            }
+        const int saved_horizon = horizon_;
+        const int h = std::max(horizon_, (nsteps + 2) * static_cast<int>(cands.size()) + 4);
+        std::array<int, 4> best{tiling_.TI, tiling_.GC, fused_threads_, fused_variant_};
+        double best_ms = 1e300;
+        reset(h);
+        for (const auto& c : cands) {
+            set_tiling(c[0], c[1], c[2], c[3]);
+            advance(2, nullptr);  // graph build and first-touch outside the timing
+            advance(nsteps, nullptr);
+            if (last_ms_ < best_ms) { best_ms = last_ms_; best = c; }
+        }
+        set_tiling(best[0], best[1], best[2], best[3]);
+        reset(saved_horizon);
+        return best;
+    }
     double last_device_ms() const override { return last_ms_; }
 
    private:
@@ -957,7 +1089,7 @@ class SolverImpl final : public SolverImplBase {
     int ijkmax_ = 0;
     Medium air_, pore_;
     bool porous_ = false;
-    int NI_ = 0, NJ_ = 0, NG_ = 0, Kair_ = 0, gAir0_ = 0, gOff_ = 0;
+    int NI_ = 0, NJ_ = 0, NJP_ = 0, NG_ = 0, Kair_ = 0, gAir0_ = 0, gOff_ = 0;
     size_t nodes_ = 0;
     // PML
     int jx_ = 0, jy_ = 0, jz_ = 0, I1_ = 0, I2_ = 0, Y1_ = 0, Y2_ = 0, K1_ = 0, K2_ = 0, pml_y_time_ = 0;
@@ -993,6 +1125,11 @@ class SolverImpl final : public SolverImplBase {
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
     cudaGraphExec_t graph_exec_ = nullptr;
     bool graph_dirty_ = true;
+    bool fused_ = false;
+    FusedTiling tiling_{};
+    int fused_threads_ = 0;
+    int fused_variant_ = 0;
+    size_t fused_smem_ = 0;
     // receivers
     std::vector<std::array<int, 3>> rec_idx_;
     // time loop
@@ -1029,6 +1166,8 @@ int Solver::get_slab(int s, int c, double* out, int* dims) { return impl_->get_s
 size_t Solver::state_elems() const { return impl_->state_elems(); }
 void Solver::copy_state(int dir, void* host) { impl_->copy_state(dir, host); }
 long long Solver::launch_count() const { return impl_->launch_count(); }
+void Solver::set_tiling(int TI, int GC, int nt, int variant) { impl_->set_tiling_api(TI, GC, nt, variant); }
+std::array<int, 4> Solver::autotune(int nsteps) { return impl_->autotune(nsteps); }
 double Solver::last_device_ms() const { return impl_->last_device_ms(); }
 
 }  // namespace fdtd

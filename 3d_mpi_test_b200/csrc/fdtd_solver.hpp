@@ -50,6 +50,8 @@ class Solver {
     size_t state_elems() const;
     void copy_state(int dir, void* host);
     long long launch_count() const;
+    void set_tiling(int rows_per_block, int planes_per_block, int threads_per_block, int variant);
+    std::array<int, 4> autotune(int nsteps);
     double last_device_ms() const;
 
    private:

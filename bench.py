@@ -86,7 +86,7 @@ class ClockSampler:
         if shutil.which("nvidia-smi"):
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
         return self
@@ -226,6 +226,11 @@ def run_gpu(args, rank, world, local_rank):
     for prec in ("f32", "f64"):
         word = 4 if prec == "f32" else 8
         a = pkg.Airpore(case_dir, prec, device=local_rank)
+        if args.tile:
+            tile = tuple(int(x) for x in args.tile.split(","))
+            a.set_tiling(*tile)
+        else:
+            tile = a.autotune(10)  # the project's tile autotuner, on this domain
         a.set_receivers(rec)
         a.reset(horizon)
         for _ in range(args.warmup):
@@ -256,7 +261,7 @@ def run_gpu(args, rank, world, local_rank):
         gcell = world * cells * steps_total / (dev_ms * 1e-3) / 1e9
         ab = algorithmic_bytes(case, word)
         achieved = ab["bytes_per_step"] / (dev_ms * 1e-3 / steps_total) / 1e9
-        results[prec] = {"gcell": gcell, "ms_per_bench_step": dev_ms / args.steps, "wall_s": wall,
+        results[prec] = {"gcell": gcell, "ms_per_bench_step": dev_ms / args.steps, "wall_s": wall, "tile": tile,
                          "launches": launches, "achieved_gbs": achieved, "bytes_per_step": ab["bytes_per_step"],
                          "clocks": sampler.summary() if sampler else None}
         # end to end through the public API with host buffers (FP32 headline only)
@@ -284,7 +289,8 @@ def run_gpu(args, rank, world, local_rank):
     roof = {"bound": "hbm", "achieved": round(f32["achieved_gbs"], 1), "peak": hbm_peak, "unit": "GB/s",
             "frac": round(f32["achieved_gbs"] / hbm_peak, 4), "traffic": None,
             "peak_kind": peak_kind,
-            "kernel": "one FB step (pressure pass + velocity pass), FP32",
+            "kernel": "k_fused (one launch = one FB step of the whole domain), FP32",
+            "tile_rows_planes_threads_variant": list(f32["tile"]),
             "algorithmic_bytes_per_step": f32["bytes_per_step"]}
     prof = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(prof):
@@ -298,6 +304,7 @@ def run_gpu(args, rank, world, local_rank):
                    "cells_per_fb_step": cells, "l2": "flushed (512 MB write) between bench steps",
                    "parallelism": f"replicas x{world}" if world > 1 else "single device-resident domain"},
         "fp64": {"value": round(f64["gcell"], 3), "ms_per_step": round(f64["ms_per_bench_step"], 4),
+                 "tile_rows_planes_threads_variant": list(f64["tile"]),
                  "achieved_gbs": round(f64["achieved_gbs"], 1),
                  "frac": round(f64["achieved_gbs"] / hbm_peak, 4),
                  "fp32_speedup": round(f32["gcell"] / f64["gcell"], 3)},
@@ -347,11 +354,12 @@ def run_reference_arm(args, world, rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--inner", type=int, default=50)
+    ap.add_argument("--inner", type=int, default=200)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tile", default="", help="rows,planes,threads,variant of the fused pass (default: autotune)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

@@ -96,12 +96,26 @@ int fdtd_get_psi(fdtd_solver *h, double *out);
  * returns 1 if the slab exists, 0 if not. out may be NULL. */
 int fdtd_get_slab(fdtd_solver *h, int s, int comp, double *out, int *dims);
 
-/* Whole device state in the native layout ([g][i][j], precision of the
- * handle): 4 fields u v w p, each fdtd_state_elems() elements. dir 0:
+/* Whole device state in the native layout ([g][i][j] with each j row padded
+ * to a multiple of 16 bytes, precision of the handle): 4 fields u v w p,
+ * each fdtd_state_elems() elements. dir 0:
  * device -> host, 1: host -> device. Used for end-to-end timing with host
  * buffers. */
 size_t fdtd_state_elems(const fdtd_solver *h);
 int fdtd_copy_state(fdtd_solver *h, int dir, void *host);
+
+/* Tile shape of the fused FB_p_v pass: rows_per_block i-rows x all j
+ * columns x planes_per_block g-planes per thread block, threads_per_block
+ * threads striding the columns (multiple of 32, <= 256); variant 0 reads
+ * the stencil inputs from global memory, 1 streams them into shared memory
+ * with bulk asynchronous copies. Takes effect for the next step. Returns
+ * FDTD_ERR_UNSUPPORTED when the tile does not fit shared memory. */
+int fdtd_set_tiling(fdtd_solver *h, int rows_per_block, int planes_per_block, int threads_per_block, int variant);
+
+/* Times each candidate tile on this handle's domain (nsteps FB steps each,
+ * CUDA events), keeps the fastest and returns it in best[4] (rows, planes,
+ * threads, variant); the state is reset to t = 0 afterwards. */
+int fdtd_autotune(fdtd_solver *h, int nsteps, int *best);
 
 /* Kernel launches issued since creation (both passes, graphs included). */
 long long fdtd_launch_count(const fdtd_solver *h);

@@ -1526,7 +1526,10 @@ int orc_run(orc *o, int nsteps, double *rec_out)
             if ((temp_time + MF_limit) > time_domain) MF_limit = time_domain - temp_time;
         }
         airpore_set_moving_frame(o, MF_count);
-        for (int n = 0; n < MF_limit; n++) {
+        /* The reference runs frame 0 for its full MF_limit even when
+         * time_domain is shorter, writing receiver samples past its buffer
+         * (airpore.cpp:545,566-578); the restatement stops at time_domain. */
+        for (int n = 0; n < MF_limit && index < time_domain; n++) {
             index = index + 1;
             for (int r = 0; r < o->nrec; ++r) {
                 double t = get_pressure(&o->air.g, o->ri[r], o->rj[r], o->rk[r], MF_count);

@@ -186,7 +186,8 @@ int main(int argc, char **argv)
             for (size_t r = 0; r < recs.size(); ++r) {
                 double temp = A->get_pressure(recs[r].i, recs[r].j, recs[r].k, MF_count);
                 if (std::fabs(temp) < 1.0e-100) temp = 0.0;
-                rec_out[(size_t)(index_pressure - 1) * recs.size() + r] = temp;
+                /* frame 0 may run past time_domain (airpore.cpp:545); keep the buffer in bounds */
+                if (index_pressure <= time_domain) rec_out[(size_t)(index_pressure - 1) * recs.size() + r] = temp;
             }
             one_step(ap, MF_count);
         }

@@ -70,7 +70,7 @@ def test_fp64_matches_oracle(name, case_dirs):
         for c in "uvwp":
             errs[f"Q{c}_{s}"] = rel_l2(got["slabs"][s][c], q[c])
     assert max(errs.values()) <= TOL_F64, errs
-    assert got["launches"] >= 2 * n  # two passes per step ran on the device
+    assert got["launches"] >= n  # at least one kernel per step ran on the device
 
 
 @pytest.mark.parametrize("name", ["pml_rigid", "porous_ground", "tdbc_east", "moving_frame", "wind_log", "hill1"])
@@ -94,7 +94,8 @@ def test_half_steps_match_full_step(case_dirs):
     with pkg.Airpore(d, "f64") as b:
         b.get_output(5)
         p_full = b.field("p")
-    assert np.array_equal(p_half, p_full)
+    # half steps run the two-pass kernels, the time loop the fused pass
+    assert rel_l2(p_half, p_full) <= 1e-13
 
 
 def test_pressure_half_step_matches_oracle(case_dirs):
@@ -165,3 +166,57 @@ def test_nonfinite_watchdog(case_dirs):
         assert e.value.code == pkg.FDTD_ERR_NONFINITE
         a.reset(5)
         a.advance(2)  # usable after the error
+
+
+TILINGS = [(2, 1, 32, 0), (3, 5, 64, 0), (8, 7, 256, 0), (4, 16, 128, 0),
+           (2, 1, 32, 1), (3, 5, 64, 1), (8, 7, 256, 1), (4, 16, 128, 1)]
+
+
+@pytest.mark.parametrize("tiling", TILINGS)
+@pytest.mark.parametrize("name", ["porous_tdbc_fine_pore", "south_pml_all_faces", "wind_log", "moving_frame"])
+def test_fused_tilings_match_oracle(name, tiling, case_dirs):
+    """The fused FB_p_v pass is exact for any tile shape: halo rows,
+    warm-up planes, odd row splits, single-plane chunks."""
+    d, rec, n = case_dirs[name]
+    ref = oracle.run_case(d, rec, n)
+    with pkg.Airpore(d, "f64") as a:
+        a.set_tiling(*tiling)
+        a.set_receivers(rec)
+        r = a.get_output(n)
+        errs = {"receivers": rel_l2(r, ref["receivers"])}
+        for f in "puvw":
+            errs[f] = rel_l2(a.field(f), ref[f])
+        errs["psi"] = rel_l2(a.psi(), ref["psi"])
+        sl = a.slabs()
+        for s, q in ref["slabs"].items():
+            for c in "uvwp":
+                errs[f"Q{c}_{s}"] = rel_l2(sl[s][c], q[c])
+    assert max(errs.values()) <= TOL_F64, errs
+
+
+def test_autotune_keeps_results_exact(case_dirs):
+    d, rec, n = case_dirs["porous_ground"]
+    ref = oracle.run_case(d, rec, n)
+    with pkg.Airpore(d, "f32") as a:
+        best = a.autotune(4)
+        assert best[0] >= 2 and best[1] >= 1 and best[2] % 32 == 0 and best[3] in (0, 1)
+        a.set_receivers(rec)
+        r = a.get_output(n)
+    assert rel_l2(r, ref["receivers"]) <= TOL_F32
+
+
+def test_fused_and_two_pass_agree(case_dirs):
+    """FB_v_p still runs the two-pass kernels; FB_p_v the fused pass. Both
+    are pinned to the oracle above; here the FB_p_v half-step API (two-pass
+    kernels) is checked against the fused time loop for the same state."""
+    d, rec, _ = case_dirs["hill2"]
+    with pkg.Airpore(d, "f64") as a:
+        a.reset(8)
+        for _ in range(4):
+            a.Cal_pressure()
+            a.Cal_velocity()
+        p2 = a.field("p")
+    with pkg.Airpore(d, "f64") as b:
+        b.get_output(4)
+        p1 = b.field("p")
+    assert rel_l2(p1, p2) <= 1e-13
