@@ -212,8 +212,9 @@ class Airpore:
         self._check(self._L.fdtd_copy_state(self._h, 1 if to_device else 0, host.ctypes.data_as(ctypes.c_void_p)))
 
     def set_tiling(self, rows_per_block: int, planes_per_block: int, threads_per_block: int,
-                   variant: int = 1) -> None:
-        """Tile of the fused pass; variant 0 plain loads, 1 bulk-copy staging."""
+                   variant: int = 0) -> None:
+        """Tile of the single-pass marching kernel (rows, planes, threads per
+        block; threads round down to whole rows of column-vector threads)."""
         self._check(self._L.fdtd_set_tiling(self._h, rows_per_block, planes_per_block, threads_per_block, variant))
 
     def autotune(self, nsteps: int = 20) -> Tuple[int, int, int, int]:

@@ -6,18 +6,23 @@
 // air k=0 := pore K-2, pore K-1 := air k=1), which is exactly a shared
 // node, so each overlap node is stored once.
 //
-// Layout: SoA, index ((g * NI) + i) * NJ + j, j (range / propagation axis,
-// the reference's Y) contiguous.
+// Layout: SoA, index ((g * NI) + i) * NJP + j, j (range / propagation axis,
+// the reference's Y) contiguous, rows padded to NJP >= NJ (16-byte rows).
 //
-// A forward-backward step (FB_p_v, airpore.cpp:589-614) is two passes:
+// A forward-backward step (FB_p_v, airpore.cpp:589-614) is, in the two-pass
+// form of this file, two passes:
 //   pressure pass  p_nn for every node, Qp slabs, receiver sampling
 //   velocity pass  u,v,w_nn for every node, Qu/Qv/Qw slabs, TDBC state
-// Boundary nodes are not swept afterwards as in the reference
-// (UpdateBC_*, calculation_2D.cpp:646-864); their final value is resolved
-// in closed form: the BC sequence only ever copies from the inward
-// neighbour, zeroes a normal component, extrapolates (east p) or applies the
-// TDBC (east v), so the last face in sequence decides and the chain ends at
-// an interior node whose fresh value the owning thread recomputes.
+// (fdtd_march.cuh holds the single-pass form.) Boundary nodes are not swept
+// afterwards as in the reference (UpdateBC_*, calculation_2D.cpp:646-864);
+// their final value is resolved in closed form: the BC sequence only ever
+// copies from the inward neighbour, zeroes a normal component, extrapolates
+// (east p) or applies the TDBC (east v), so the last face in sequence
+// decides and the chain ends at an interior node whose fresh value the
+// owning thread recomputes.
+//
+// The per-node physics (p_node, vel_node and the PML / wind / inclusion
+// helpers below) is written once and shared by both forms.
 #pragma once
 
 #include <cstdint>
@@ -31,17 +36,20 @@ template <typename R>
 struct Slab {
     // storage range of one PML integral slab, in air node indices (k = air k)
     int i0, j0, k0, ni, nj, nk;
+    int ja, jp;      // storage rows: 16-byte-aligned column origin ja <= j0, padded pitch jp
     const R* rd[4];  // u v w p  (values read this pass)
-    R* wr[4];        // u v w p  (values written this pass; only one kind per pass)
-    __device__ __forceinline__ size_t at(int i, int j, int k) const {
-        return (static_cast<size_t>(k - k0) * ni + (i - i0)) * nj + (j - j0);
-    }
+    R* wr[4];        // u v w p  (values written this pass)
+    // 32-bit element index; the host rejects slabs of 2^31 elements or more
+    __device__ __forceinline__ int q(int i, int j, int k) const { return ((k - k0) * ni + (i - i0)) * jp + (j - ja); }
+    __device__ __forceinline__ bool holds_i(int i) const { return i >= i0 && i < i0 + ni; }
+    __device__ __forceinline__ bool holds_j(int j) const { return j >= j0 && j < j0 + nj; }
+    __device__ __forceinline__ bool holds_k(int k) const { return k >= k0 && k < k0 + nk; }
 };
 
 template <typename R>
 struct Dev {
     int NI, NJ, NG;
-    int NJP;     // row pitch of the field arrays (>= NJ; 16-byte rows for bulk copies)
+    int NJP;     // row pitch of the field arrays (>= NJ; 16-byte rows)
     int porous;  // porous ground stacked below the air
     int gAir0;   // first g owned by the air medium
     int gOff;    // air k = g - gOff
@@ -55,7 +63,8 @@ struct Dev {
     const R* pold;                       // p_n (pressure pass)
     R *u_out, *v_out, *w_out, *p_out;
 
-    // derivative factors x_over_X*rdx etc. (reference metric x scale)
+    // derivative factors x_over_X*rdx etc. (reference metric x scale);
+    // the per-column arrays ayA / ayP are padded to NJP with zeros
     const R *axA, *ayA, *axP, *ayP, *azG;
 
     // air constants
@@ -87,23 +96,12 @@ struct Dev {
     int nrec;
     const long long* rec_node;  // unified index or -1 (outside window / not strictly interior)
     double* rec_out;            // [step][nrec]
-    int* counters;              // [0] step index seen by pass 1, [1] by pass 2
-    int* status;                // bit 0: non-finite pressure seen
+    int* counters;              // step counters (see k_pressure)
+    int* status;                // bit 0: non-finite pressure seen; bit 1: staged-copy timeout
 
     __device__ __forceinline__ size_t ix(int g, int i, int j) const {
         return (static_cast<size_t>(g) * NI + i) * NJP + j;
     }
-};
-
-// Reads of the step's input fields (u, v, w and the old pressure) at
-// (i, j, g) straight from global memory.
-template <typename R>
-struct GlobalFields {
-    const Dev<R>& d;
-    __device__ __forceinline__ R u(int i, int j, int g) const { return d.u_in[d.ix(g, i, j)]; }
-    __device__ __forceinline__ R v(int i, int j, int g) const { return d.v_in[d.ix(g, i, j)]; }
-    __device__ __forceinline__ R w(int i, int j, int g) const { return d.w_in[d.ix(g, i, j)]; }
-    __device__ __forceinline__ R p(int i, int j, int g) const { return d.pold[d.ix(g, i, j)]; }
 };
 
 // ---------------------------------------------------------------- helpers
@@ -117,224 +115,543 @@ __device__ __forceinline__ int y_side(const Dev<R>& d, int j, bool y1_on) {
     return s;
 }
 
-// -------------------------------------------------- fresh interior values
-// Pressure at an interior node of either medium: p_n + increment.
-// Air: air::cal_fp (air.cpp:1953-2322); pore: porous::cal_fp (porous.cpp:107-143);
-// accumulation: calculation_2D::Cal_pressure (calculation_2D.cpp:581-613).
-template <typename R, bool WIND, typename F>
-__device__ R fresh_p(const Dev<R>& d, const F& f, int i, int j, int g, bool y1_on) {
-    const R u0 = f.u(i, j, g), v0 = f.v(i, j, g), w0 = f.w(i, j, g);
-    const R az = ldg(d.azG + g);
-    const R pn = f.p(i, j, g);
-    if (g < d.gAir0) {  // porous ground
-        const R ax = ldg(d.axP + i), ay = ldg(d.ayP + j);
-        const R div = ax * (f.u(i + 1, j, g) - u0) + ay * (f.v(i, j + 1, g) - v0) + az * (f.w(i, j, g + 1) - w0);
-        return pn - d.pGama * div;
-    }
-    const R ax = ldg(d.axA + i), ay = ldg(d.ayA + j);
-    const R gu = ax * (f.u(i + 1, j, g) - u0), gv = ay * (f.v(i, j + 1, g) - v0), gw = az * (f.w(i, j, g + 1) - w0);
-    const int k = g - d.gOff;
-    const int8_t* m = d.mask;
-    if (m && i >= d.mi0 && i <= d.mi1 && j >= d.mj0 && j <= d.mj1 && k >= d.mk0 && k <= d.mk1) {
-        const int mv = m[(static_cast<size_t>(k - d.mk0) * (d.mi1 - d.mi0 + 1) + (i - d.mi0)) * (d.mj1 - d.mj0 + 1) +
-                         (j - d.mj0)];
-        if (mv == 1) return pn - d.m1_gama * (gu + gv + gw);
-        if (mv == 2) return pn - d.m2_gama * (gu + gv + gw);
-    }
-    R dp = -d.gP0dt * (gu + gv + gw);
-    if (WIND) {
-        const size_t wk = static_cast<size_t>(k) * d.NJ + j, wS = d.NJ;
-        const R U = ldg(d.Uw + wk), V = ldg(d.Vw + wk), W = ldg(d.Ww + wk);
-        const R pim = f.p(i - 1, j, g), pjm = f.p(i, j - 1, g), pkm = f.p(i, j, g - 1);
-        dp += -(U * ax * d.dt) * (pn - pim) - (V * ay * d.dt) * (pn - pjm) - (W * az * d.dt) * (pn - pkm);
-        const R dVdY = ay * (ldg(d.Vw + wk + 1) - ldg(d.Vw + wk - 1)) * R(0.5);
-        const R dWdZ = az * (ldg(d.Ww + wk + wS) - ldg(d.Ww + wk - wS)) * R(0.5);
-        dp += -d.gdt * pn * (dVdY + dWdZ);
-    }
-    const int xs = d.sdI[i], ys = y_side(d, j, y1_on), zs = d.sdK[k];
-    if (xs | ys | zs) {
-        const R sx = xs ? ldg(d.sxI + i) : R(0), sy = ys ? ldg(d.syJ + j) : R(0), sz = zs ? ldg(d.szK + k) : R(0);
-        const Slab<R>* SX = xs ? &d.sl[xs - 1] : nullptr;
-        const Slab<R>* SY = ys ? &d.sl[ys + 1] : nullptr;
-        const Slab<R>* SZ = zs ? &d.sl[zs + 3] : nullptr;
-        const R gP0 = d.gP0, dt = d.dt;
-        size_t qx = 0, qy = 0, qz = 0;
-        R dQux = 0, dQvx = 0, dQwx = 0, dQuy = 0, dQvy = 0, dQwy = 0, dQuz = 0, dQvz = 0;
-        if (SX) {
-            qx = SX->at(i, j, k);
-            const int sj = 1, sk = SX->ni * SX->nj, si = SX->nj;
-            dQux = ax * (SX->rd[0][qx + si] - SX->rd[0][qx]);
-            dQvx = ay * (SX->rd[1][qx + sj] - SX->rd[1][qx]);
-            dQwx = az * (SX->rd[2][qx + sk] - SX->rd[2][qx]);
-            dp += ldg(d.fxI + i) * gP0 * gu * dt - sx * (pn + gP0 * (dQvx + dQwx)) * dt;
-        }
-        if (SY) {
-            qy = SY->at(i, j, k);
-            const int sj = 1, sk = SY->ni * SY->nj, si = SY->nj;
-            dQuy = ax * (SY->rd[0][qy + si] - SY->rd[0][qy]);
-            dQvy = ay * (SY->rd[1][qy + sj] - SY->rd[1][qy]);
-            dQwy = az * (SY->rd[2][qy + sk] - SY->rd[2][qy]);
-            dp += ldg(d.fyJ + j) * gP0 * gv * dt - sy * (pn + gP0 * (dQuy + dQwy)) * dt;
-            if (SX) {
-                dp += -(SX->rd[3][qx] * sx * sy + gP0 * (ldg(d.gxI + i) * sy * dQux + ldg(d.gyJ + j) * sx * dQvx)) * dt;
-            }
-        }
-        if (SZ) {
-            qz = SZ->at(i, j, k);
-            const int sk = SZ->ni * SZ->nj, si = SZ->nj;
-            dQuz = ax * (SZ->rd[0][qz + si] - SZ->rd[0][qz]);
-            dQvz = ay * (SZ->rd[1][qz + 1] - SZ->rd[1][qz]);
-            (void)sk;
-            dp += ldg(d.fzK + k) * gP0 * gw * dt - sz * (pn + gP0 * (dQuz + dQvz)) * dt;
-            if (SX) {
-                dp += -(SX->rd[3][qx] * sx * sz + gP0 * (ldg(d.gxI + i) * sz * dQux + ldg(d.gzK + k) * sx * dQwx)) * dt;
-            }
-            if (SY) {
-                dp += -(SY->rd[3][qy] * sy * sz + gP0 * (ldg(d.gyJ + j) * sz * dQvy + ldg(d.gzK + k) * sy * dQwy)) * dt;
-            }
-        }
-    }
-    return pn + dp;
-}
-
+// PML coefficients of one axis at one node: sigma, 1 - 1/beta, 1/beta - 1
+// (air.cpp:509-937 profile, beta = 1 + 25 (d/W)^alpha)
 template <typename R>
-struct Vel3 {
-    R u, v, w;
+struct PmlC {
+    R s, f, g;
 };
 
-// Velocity at an interior node: u_n + increment, with p = the pressure the
-// scheme prescribes (p_nn for FB_p_v). Air: air::cal_fuvw (air.cpp:1476-1949);
-// pore: porous::cal_fuvw (porous.cpp:58-104); accumulation:
-// calculation_2D::Cal_velocity (calculation_2D.cpp:548-579).
-//
-// p0, pim, pjm, pkm: the scheme's pressure at the node and its i-1, j-1,
-// g-1 neighbours. qp_old: the slabs' Qp buffers still hold the values from
-// before this step's pressure update (fused pass), so the advanced Qp is
-// formed here as Qp + dt * p, the expression of air::Update_PML_Qp.
-template <typename R, bool WIND, typename F>
-__device__ Vel3<R> fresh_vel_core(const Dev<R>& d, const F& f, int i, int j, int g, bool y1_on, R p0, R pim, R pjm,
-                                  R pkm, bool qp_old) {
-    const R u0 = f.u(i, j, g), v0 = f.v(i, j, g), w0 = f.w(i, j, g);
-    const R bpi = p0 - pim, bpj = p0 - pjm, bpk = p0 - pkm;
-    const R az = ldg(d.azG + g);
-    Vel3<R> r;
-    if (g < d.gAir0) {
-        const R ax = ldg(d.axP + i), ay = ldg(d.ayP + j);
-        r.u = u0 + (-d.pIBdtEff * (ax * bpi) + u0 * d.pInvB - u0);
-        r.v = v0 + (-d.pIBdtEff * (ay * bpj) + v0 * d.pInvB - v0);
-        r.w = w0 + (-d.pIBdtEff * (az * bpk) + w0 * d.pInvB - w0);
-        return r;
+// N consecutive column values (N * sizeof(R) <= 16) moved as one access;
+// Vec is the 16-byte column vector of the marching kernel. N = 1 is the
+// node-wise form of the two-pass kernels.
+template <typename R, int N>
+struct alignas(sizeof(R) * N) Arr {
+    R e[N];
+};
+template <typename R>
+using Vec = Arr<R, 16 / static_cast<int>(sizeof(R))>;
+
+template <typename R, int N>
+__device__ __forceinline__ Arr<R, N> ldn(const R* p) {
+    return *reinterpret_cast<const Arr<R, N>*>(p);
+}
+template <typename R, int N>
+__device__ __forceinline__ void stn(R* p, const Arr<R, N>& v) {
+    *reinterpret_cast<Arr<R, N>*>(p) = v;
+}
+
+// Compiler scheduling fence: memory accesses are not moved across it. Used
+// between the x, y and z PML sections, which are mostly exclusive (a node
+// lies in one layer except along edges), so hoisting every section's loads
+// ahead would only raise register pressure.
+__device__ __forceinline__ void sched_fence() { asm volatile("" ::: "memory"); }
+
+// Active y PML sides of N columns are packed 2 bits per column (0 none, 1
+// low, 2 high). y_common: 0 when no column is in the layer, the side when
+// every active column shares it, 3 when both sides occur.
+template <int N>
+__device__ __forceinline__ int y_common(int ysp) {
+    int c = 0;
+#pragma unroll
+    for (int e = 0; e < N; ++e) {
+        const int s = (ysp >> (2 * e)) & 3;
+        if (s) c = (c == 0 || c == s) ? s : 3;
     }
-    const R ax = ldg(d.axA + i), ay = ldg(d.ayA + j);
-    const R gpX = ax * bpi, gpY = ay * bpj, gpZ = az * bpk;
-    const int k = g - d.gOff;
-    const int8_t* m = d.mask;
-    if (m && i >= d.mi0 && i <= d.mi1 && j >= d.mj0 && j <= d.mj1 && k >= d.mk0 && k <= d.mk1) {
-        const int mv = m[(static_cast<size_t>(k - d.mk0) * (d.mi1 - d.mi0 + 1) + (i - d.mi0)) * (d.mj1 - d.mj0 + 1) +
-                         (j - d.mj0)];
-        if (mv == 1 || mv == 2) {
-            const R a = mv == 1 ? d.m1_ibdteff : d.m2_ibdteff, b = mv == 1 ? d.m1_ib : d.m2_ib;
-            r.u = u0 + (-a * gpX + u0 * b - u0);
-            r.v = v0 + (-a * gpY + v0 * b - v0);
-            r.w = w0 + (-a * gpZ + w0 * b - w0);
-            return r;
-        }
+    return c;
+}
+
+// Coefficients constant over one plane g (air k = g - gOff).
+template <typename R>
+struct PlaneC {
+    R az;
+    int pore;    // porous-ground plane
+    int k;       // air k
+    int zs;      // active z PML side of an air plane (0 none, 1 low, 2 high)
+    PmlC<R> Z;
+    int inmask;  // plane crosses the inclusion box
+};
+
+template <typename R>
+__device__ __forceinline__ PlaneC<R> plane_c(const Dev<R>& d, int g) {
+    PlaneC<R> c;
+    c.az = ldg(d.azG + g);
+    c.pore = g < d.gAir0;
+    c.k = g - d.gOff;
+    c.zs = 0;
+    c.Z = {R(0), R(0), R(0)};
+    c.inmask = 0;
+    if (!c.pore) {
+        c.zs = d.sdK[c.k];
+        if (c.zs) c.Z = {ldg(d.szK + c.k), ldg(d.fzK + c.k), ldg(d.gzK + c.k)};
+        c.inmask = d.mask != nullptr && c.k >= d.mk0 && c.k <= d.mk1;
     }
-    R du = -d.Aavdt * gpX, dv = -d.Aavdt * gpY, dw = -d.Aavdt * gpZ;
-    if (WIND) {
-        const size_t wk = static_cast<size_t>(k) * d.NJ + j, wS = d.NJ;
-        const R U = ldg(d.Uw + wk), V = ldg(d.Vw + wk), W = ldg(d.Ww + wk);
-        const R c1 = U * ax * d.dt, c2 = V * ay * d.dt, c3 = W * az * d.dt;
-        du += -c1 * (f.u(i + 1, j, g) - u0) - c2 * (f.u(i, j + 1, g) - u0) - c3 * (f.u(i, j, g + 1) - u0);
-        dv += -c1 * (f.v(i + 1, j, g) - v0) - c2 * (f.v(i, j + 1, g) - v0) - c3 * (f.v(i, j, g + 1) - v0);
-        dw += -c1 * (f.w(i + 1, j, g) - w0) - c2 * (f.w(i, j + 1, g) - w0) - c3 * (f.w(i, j, g + 1) - w0);
-        const R h = R(0.5);
-        const R dUdY = ay * (ldg(d.Uw + wk + 1) - ldg(d.Uw + wk - 1)) * h;
-        const R dUdZ = az * (ldg(d.Uw + wk + wS) - ldg(d.Uw + wk - wS)) * h;
-        const R dVdY = ay * (ldg(d.Vw + wk + 1) - ldg(d.Vw + wk - 1)) * h;
-        const R dVdZ = az * (ldg(d.Vw + wk + wS) - ldg(d.Vw + wk - wS)) * h;
-        const R dWdY = ay * (ldg(d.Ww + wk + 1) - ldg(d.Ww + wk - 1)) * h;
-        const R dWdZ = az * (ldg(d.Ww + wk + wS) - ldg(d.Ww + wk - wS)) * h;
-        du += -(v0 * dUdY + w0 * dUdZ) * d.dt;
-        dv += -(v0 * dVdY + w0 * dVdZ) * d.dt;
-        dw += -(v0 * dWdY + w0 * dWdZ) * d.dt;
+    return c;
+}
+
+// Coefficients constant along one row i of a plane.
+template <typename R>
+struct RowC {
+    R ax;
+    int xs;  // active x PML side
+    PmlC<R> X;
+    int inmask;
+};
+
+template <typename R>
+__device__ __forceinline__ RowC<R> row_c(const Dev<R>& d, const PlaneC<R>& pc, int i) {
+    RowC<R> r;
+    r.ax = ldg((pc.pore ? d.axP : d.axA) + i);
+    r.xs = 0;
+    r.X = {R(0), R(0), R(0)};
+    r.inmask = pc.inmask && i >= d.mi0 && i <= d.mi1;
+    if (!pc.pore) {
+        r.xs = d.sdI[i];
+        if (r.xs) r.X = {ldg(d.sxI + i), ldg(d.fxI + i), ldg(d.gxI + i)};
     }
-    const int xs = d.sdI[i], ys = y_side(d, j, y1_on), zs = d.sdK[k];
-    if (xs | ys | zs) {
-        const R sx = xs ? ldg(d.sxI + i) : R(0), sy = ys ? ldg(d.syJ + j) : R(0), sz = zs ? ldg(d.szK + k) : R(0);
-        const Slab<R>* SX = xs ? &d.sl[xs - 1] : nullptr;
-        const Slab<R>* SY = ys ? &d.sl[ys + 1] : nullptr;
-        const Slab<R>* SZ = zs ? &d.sl[zs + 3] : nullptr;
-        const R A = d.Aav, dt = d.dt;
-        // backward differences of the slab's Qp advanced to this step
-        auto bq = [&](const Slab<R>* S, size_t q, R& bx, R& by, R& bz) {
-            const R* Q = S->rd[3];
-            const size_t sk = static_cast<size_t>(S->ni) * S->nj;
-            R q0 = Q[q], qi = Q[q - S->nj], qj = Q[q - 1], qk = Q[q - sk];
-            if (qp_old) {
-                q0 = q0 + dt * p0;
-                qi = qi + dt * pim;
-                qj = qj + dt * pjm;
-                qk = qk + dt * pkm;
-            }
-            bx = ax * (q0 - qi);
-            by = ay * (q0 - qj);
-            bz = az * (q0 - qk);
-        };
-        R bxX = 0, byX = 0, bzX = 0, bxY = 0, byY = 0, bzY = 0, bxZ = 0, byZ = 0, bzZ = 0;
-        size_t qx = 0, qy = 0;
-        if (SX) {
-            qx = SX->at(i, j, k);
-            bq(SX, qx, bxX, byX, bzX);
-            du += -sx * u0 * dt + ldg(d.fxI + i) * (A * gpX) * dt;
-            dv += -sx * (v0 + A * byX) * dt;
-            dw += -sx * (w0 + A * bzX) * dt;
-        }
-        if (SY) {
-            qy = SY->at(i, j, k);
-            bq(SY, qy, bxY, byY, bzY);
-            du += -sy * (u0 + A * bxY) * dt;
-            dv += ldg(d.fyJ + j) * A * gpY * dt - sy * v0 * dt;
-            dw += -sy * (w0 + A * bzY) * dt;
-            if (SX) {
-                du += -(SX->rd[0][qx] * sx * sy + ldg(d.gxI + i) * sy * A * bxX) * dt;
-                dv += -(SX->rd[1][qx] * sx * sy + ldg(d.gyJ + j) * sx * A * byX) * dt;
-                dw += -SX->rd[2][qx] * sx * sy * dt;
-            }
-        }
-        if (SZ) {
-            const size_t qz = SZ->at(i, j, k);
-            R bxZ_, byZ_, bzZ_;
-            bq(SZ, qz, bxZ_, byZ_, bzZ_);
-            bxZ = bxZ_; byZ = byZ_; bzZ = bzZ_;
-            du += -sz * (u0 + A * bxZ) * dt;
-            dv += -sz * (v0 + A * byZ) * dt;
-            dw += ldg(d.fzK + k) * A * gpZ * dt - sz * w0 * dt;
-            if (SX) {
-                du += -(SX->rd[0][qx] * sx * sz + ldg(d.gxI + i) * sz * A * bxX) * dt;
-                dv += -SX->rd[1][qx] * sx * sz * dt;
-                dw += -(SX->rd[2][qx] * sx * sz + ldg(d.gzK + k) * sx * A * bzX) * dt;
-            }
-            if (SY) {
-                du += -SY->rd[0][qy] * sy * sz * dt;
-                dv += -(SY->rd[1][qy] * sy * sz + ldg(d.gyJ + j) * sz * A * byY) * dt;
-                dw += -(SY->rd[2][qy] * sy * sz + ldg(d.gzK + k) * sy * A * bzY) * dt;
-            }
-        }
-    }
-    r.u = u0 + du;
-    r.v = v0 + dv;
-    r.w = w0 + dw;
     return r;
 }
 
-// Velocity with the scheme's pressure read from global memory and the Qp
-// slabs already advanced (two-pass path).
+template <typename R>
+__device__ __forceinline__ PmlC<R> pml_y(const Dev<R>& d, int ys, int j) {
+    if (!ys) return {R(0), R(0), R(0)};
+    return {ldg(d.syJ + j), ldg(d.fyJ + j), ldg(d.gyJ + j)};
+}
+
+// inclusion mask value at air node (i, j, k) of a row inside the box's i
+// and k range: 0 air, 1 canopy, 2 trunk (air::cal_hill_var, air.cpp:938-1122)
+template <typename R>
+__device__ __forceinline__ int mask_at(const Dev<R>& d, int i, int j, int k) {
+    if (j < d.mj0 || j > d.mj1) return 0;
+    return d.mask[((k - d.mk0) * (d.mi1 - d.mi0 + 1) + (i - d.mi0)) * (d.mj1 - d.mj0 + 1) + (j - d.mj0)];
+}
+
+// element e of an N-vector as a 1-vector
+template <typename R, int N>
+__device__ __forceinline__ Arr<R, 1> el(const Arr<R, N>& a, int e) {
+    return Arr<R, 1>{{a.e[e]}};
+}
+
+// -------------------------------------------------- pressure increment parts
+// PML part of the air pressure increment of N columns [jb, jb+N) of row i
+// (air::cal_fp, air.cpp:1953-2322): per active layer its sigma / beta terms
+// with the Q-slab forward differences, then the pairwise corner products,
+// added to dp in the reference's order. x and z layers are uniform over the
+// columns; the y layer is per column (ysp), all active columns on side ysv
+// (1 or 2). Columns outside the y layer take zero y coefficients, which
+// adds exact zeros; their slab reads stay inside the padded slab row.
+template <typename R, int N>
+__device__ __forceinline__ void pml_dp_v(const Dev<R>& d, int i, int jb, int k, int xs, int ysp, int ysv, int zs,
+                                         R ax, const Arr<R, N>& ay, R az, const Arr<R, N>& gu, const Arr<R, N>& gv,
+                                         const Arr<R, N>& gw, const Arr<R, N>& pn, const PmlC<R>& X,
+                                         const PmlC<R>& Z, Arr<R, N>& dp) {
+    const R gP0 = d.gP0, dt = d.dt;
+    const int NJ = d.NJ;
+    Arr<R, N> dQux{}, dQvx{}, dQwx{}, QpX{}, dQvy{}, dQwy{}, QpY{};
+    PmlC<R> Y[N];
+    if (xs) {
+        const Slab<R>& S = d.sl[xs - 1];
+        const int q = S.q(i, jb, k);
+        const Arr<R, N> u0 = ldn<R, N>(S.rd[0] + q), u1 = ldn<R, N>(S.rd[0] + q + S.jp);
+        const Arr<R, N> v0 = ldn<R, N>(S.rd[1] + q);
+        const R vn = (jb + N <= NJ - 1) ? S.rd[1][q + N] : R(0);
+        const Arr<R, N> w0 = ldn<R, N>(S.rd[2] + q), w1 = ldn<R, N>(S.rd[2] + q + S.ni * S.jp);
+        if (ysv | zs) QpX = ldn<R, N>(S.rd[3] + q);
+#pragma unroll
+        for (int e = 0; e < N; ++e) {
+            const R v1 = e + 1 < N ? v0.e[e + 1 < N ? e + 1 : 0] : vn;
+            dQux.e[e] = ax * (u1.e[e] - u0.e[e]);
+            dQvx.e[e] = ay.e[e] * (v1 - v0.e[e]);
+            dQwx.e[e] = az * (w1.e[e] - w0.e[e]);
+            dp.e[e] += X.f * gP0 * gu.e[e] * dt - X.s * (pn.e[e] + gP0 * (dQvx.e[e] + dQwx.e[e])) * dt;
+        }
+    }
+    sched_fence();
+    if (ysv) {
+        const Slab<R>& S = d.sl[ysv + 1];
+        const int q = S.q(i, jb, k);
+        const Arr<R, N> u0 = ldn<R, N>(S.rd[0] + q), u1 = ldn<R, N>(S.rd[0] + q + S.jp);
+        const Arr<R, N> v0 = ldn<R, N>(S.rd[1] + q);
+        const R vn = ((ysp >> (2 * (N - 1))) & 3) ? S.rd[1][q + N] : R(0);
+        const Arr<R, N> w0 = ldn<R, N>(S.rd[2] + q), w1 = ldn<R, N>(S.rd[2] + q + S.ni * S.jp);
+        if (xs | zs) QpY = ldn<R, N>(S.rd[3] + q);
+#pragma unroll
+        for (int e = 0; e < N; ++e) {
+            Y[e] = pml_y(d, (ysp >> (2 * e)) & 3, jb + e);
+            const R v1 = e + 1 < N ? v0.e[e + 1 < N ? e + 1 : 0] : vn;
+            const R dQuy = ax * (u1.e[e] - u0.e[e]);
+            dQvy.e[e] = ay.e[e] * (v1 - v0.e[e]);
+            dQwy.e[e] = az * (w1.e[e] - w0.e[e]);
+            dp.e[e] += Y[e].f * gP0 * gv.e[e] * dt - Y[e].s * (pn.e[e] + gP0 * (dQuy + dQwy.e[e])) * dt;
+            if (xs)
+                dp.e[e] += -(QpX.e[e] * X.s * Y[e].s + gP0 * (X.g * Y[e].s * dQux.e[e] + Y[e].g * X.s * dQvx.e[e])) * dt;
+        }
+    }
+    sched_fence();
+    if (zs) {
+        const Slab<R>& S = d.sl[zs + 3];
+        const int q = S.q(i, jb, k);
+        const Arr<R, N> u0 = ldn<R, N>(S.rd[0] + q), u1 = ldn<R, N>(S.rd[0] + q + S.jp);
+        const Arr<R, N> v0 = ldn<R, N>(S.rd[1] + q);
+        const R vn = (jb + N <= NJ - 1) ? S.rd[1][q + N] : R(0);
+#pragma unroll
+        for (int e = 0; e < N; ++e) {
+            const R v1 = e + 1 < N ? v0.e[e + 1 < N ? e + 1 : 0] : vn;
+            const R dQuz = ax * (u1.e[e] - u0.e[e]);
+            const R dQvz = ay.e[e] * (v1 - v0.e[e]);
+            dp.e[e] += Z.f * gP0 * gw.e[e] * dt - Z.s * (pn.e[e] + gP0 * (dQuz + dQvz)) * dt;
+            if (xs)
+                dp.e[e] += -(QpX.e[e] * X.s * Z.s + gP0 * (X.g * Z.s * dQux.e[e] + Z.g * X.s * dQwx.e[e])) * dt;
+            if (ysv)
+                dp.e[e] +=
+                    -(QpY.e[e] * Y[e].s * Z.s + gP0 * (Y[e].g * Z.s * dQvy.e[e] + Z.g * Y[e].s * dQwy.e[e])) * dt;
+        }
+    }
+}
+
+// Mean-wind part of the air pressure increment at one node: one-sided
+// upwind advection of p and gamma p div U0 (air.cpp:1953-2322, wind branch).
+template <typename R>
+__device__ __forceinline__ void wind_dp(const Dev<R>& d, int j, int k, R ax, R ay, R az, R pn, R pim, R pjm, R pkm,
+                                        R& dp) {
+    const int wk = k * d.NJ + j, wS = d.NJ;
+    const R U = ldg(d.Uw + wk), V = ldg(d.Vw + wk), W = ldg(d.Ww + wk);
+    dp += -(U * ax * d.dt) * (pn - pim) - (V * ay * d.dt) * (pn - pjm) - (W * az * d.dt) * (pn - pkm);
+    const R dVdY = ay * (ldg(d.Vw + wk + 1) - ldg(d.Vw + wk - 1)) * R(0.5);
+    const R dWdZ = az * (ldg(d.Ww + wk + wS) - ldg(d.Ww + wk - wS)) * R(0.5);
+    dp += -d.gdt * pn * (dVdY + dWdZ);
+}
+
+// New pressure at N interior columns [jb, jb+N) of row i from their stencil
+// values: p_n + increment. Air: air::cal_fp (air.cpp:1953-2322); pore:
+// porous::cal_fp (porous.cpp:107-143); accumulation:
+// calculation_2D::Cal_pressure (calculation_2D.cpp:581-613).
+//   u0 v0 w0 pn  the nodes' u, v, w, p_n
+//   ui vj wk     u(i+1), v(j+1), w(g+1)
+//   pim pjm pkm  p_n(i-1), p_n(j-1), p_n(g-1) (read with wind only)
+// Columns outside 1..NJ-2 (faces, row padding) get values the caller
+// discards; every read for them stays in bounds.
+template <typename R, bool WIND, int N>
+__device__ __forceinline__ Arr<R, N> p_vec(const Dev<R>& d, const PlaneC<R>& pc, const RowC<R>& rc, int i, int jb,
+                                           const Arr<R, N>& ay, int ysp, const Arr<R, N>& u0, const Arr<R, N>& v0,
+                                           const Arr<R, N>& w0, const Arr<R, N>& pn, const Arr<R, N>& ui,
+                                           const Arr<R, N>& vj, const Arr<R, N>& wk, const Arr<R, N>& pim,
+                                           const Arr<R, N>& pjm, const Arr<R, N>& pkm) {
+    Arr<R, N> gu, gv, gw, out;
+#pragma unroll
+    for (int e = 0; e < N; ++e) {
+        gu.e[e] = rc.ax * (ui.e[e] - u0.e[e]);
+        gv.e[e] = ay.e[e] * (vj.e[e] - v0.e[e]);
+        gw.e[e] = pc.az * (wk.e[e] - w0.e[e]);
+    }
+    if (pc.pore) {
+#pragma unroll
+        for (int e = 0; e < N; ++e) out.e[e] = pn.e[e] - d.pGama * (gu.e[e] + gv.e[e] + gw.e[e]);
+        return out;
+    }
+    Arr<R, N> dp;
+#pragma unroll
+    for (int e = 0; e < N; ++e) dp.e[e] = -d.gP0dt * (gu.e[e] + gv.e[e] + gw.e[e]);
+    if (WIND) {
+#pragma unroll
+        for (int e = 0; e < N; ++e)
+            if (jb + e >= 1 && jb + e <= d.NJ - 2)
+                wind_dp(d, jb + e, pc.k, rc.ax, ay.e[e], pc.az, pn.e[e], pim.e[e], pjm.e[e], pkm.e[e], dp.e[e]);
+    }
+    const int ysv = y_common<N>(ysp);
+    if (rc.xs | ysv | pc.zs) {
+        if (ysv != 3) {
+            pml_dp_v<R, N>(d, i, jb, pc.k, rc.xs, ysp, ysv, pc.zs, rc.ax, ay, pc.az, gu, gv, gw, pn, rc.X, pc.Z, dp);
+        } else {  // both y layers within N columns (very narrow grids): column by column
+#pragma unroll
+            for (int e = 0; e < N; ++e) {
+                const int s = (ysp >> (2 * e)) & 3;
+                Arr<R, 1> dpe = el(dp, e);
+                pml_dp_v<R, 1>(d, i, jb + e, pc.k, rc.xs, s, s, pc.zs, rc.ax, el(ay, e), pc.az, el(gu, e), el(gv, e),
+                               el(gw, e), el(pn, e), rc.X, pc.Z, dpe);
+                dp.e[e] = dpe.e[0];
+            }
+        }
+    }
+#pragma unroll
+    for (int e = 0; e < N; ++e) out.e[e] = pn.e[e] + dp.e[e];
+    if (rc.inmask) {
+#pragma unroll
+        for (int e = 0; e < N; ++e) {
+            const int mv = mask_at(d, i, jb + e, pc.k);
+            if (mv == 1) out.e[e] = pn.e[e] - d.m1_gama * (gu.e[e] + gv.e[e] + gw.e[e]);
+            if (mv == 2) out.e[e] = pn.e[e] - d.m2_gama * (gu.e[e] + gv.e[e] + gw.e[e]);
+        }
+    }
+    return out;
+}
+
+// -------------------------------------------------- velocity increment parts
+// PML part of the air velocity increment of N columns (air::cal_fuvw,
+// air.cpp:1476-1949); same column conventions as pml_dp_v. p0, pim, pjm,
+// pkm: the scheme's pressure at the nodes and at i-1, j-1, g-1. qp_old: the
+// slabs' Qp buffers still hold the values from before this step's pressure
+// update (single-pass form), so the advanced Qp is formed here as
+// Qp + dt * p, the expression of air::Update_PML_Qp.
+template <typename R, int N>
+__device__ __forceinline__ void pml_dvel_v(const Dev<R>& d, int i, int jb, int k, int xs, int ysp, int ysv, int zs,
+                                           R ax, const Arr<R, N>& ay, R az, const Arr<R, N>& u0, const Arr<R, N>& v0,
+                                           const Arr<R, N>& w0, const Arr<R, N>& gpX, const Arr<R, N>& gpY,
+                                           const Arr<R, N>& gpZ, const Arr<R, N>& p0, const Arr<R, N>& pim,
+                                           const Arr<R, N>& pjm, const Arr<R, N>& pkm, bool qp_old,
+                                           const PmlC<R>& X, const PmlC<R>& Z, Arr<R, N>& du, Arr<R, N>& dv,
+                                           Arr<R, N>& dw) {
+    const R A = d.Aav, dt = d.dt;
+    // backward differences of the slab's Qp advanced to this step
+    auto bq = [&](const Slab<R>& S, int q, Arr<R, N>& bx, Arr<R, N>& by, Arr<R, N>& bz) {
+        const R* Q = S.rd[3];
+        const Arr<R, N> q0 = ldn<R, N>(Q + q), qi = ldn<R, N>(Q + q - S.jp), qk = ldn<R, N>(Q + q - S.ni * S.jp);
+        const R qjm = jb > S.ja ? Q[q - 1] : R(0);  // column jb-1
+#pragma unroll
+        for (int e = 0; e < N; ++e) {
+            R a = q0.e[e], b = qi.e[e], c = e > 0 ? q0.e[e > 0 ? e - 1 : 0] : qjm, f = qk.e[e];
+            if (qp_old) {
+                a = a + dt * p0.e[e];
+                b = b + dt * pim.e[e];
+                c = c + dt * pjm.e[e];
+                f = f + dt * pkm.e[e];
+            }
+            bx.e[e] = ax * (a - b);
+            by.e[e] = ay.e[e] * (a - c);
+            bz.e[e] = az * (a - f);
+        }
+    };
+    Arr<R, N> bxX{}, byX{}, bzX{}, bxY{}, byY{}, bzY{};
+    Arr<R, N> QuX{}, QvX{}, QwX{}, QuY{}, QvY{}, QwY{};
+    PmlC<R> Y[N];
+    if (xs) {
+        const Slab<R>& S = d.sl[xs - 1];
+        const int q = S.q(i, jb, k);
+        bq(S, q, bxX, byX, bzX);
+        if (ysv | zs) {
+            QuX = ldn<R, N>(S.rd[0] + q);
+            QvX = ldn<R, N>(S.rd[1] + q);
+            QwX = ldn<R, N>(S.rd[2] + q);
+        }
+#pragma unroll
+        for (int e = 0; e < N; ++e) {
+            du.e[e] += -X.s * u0.e[e] * dt + X.f * (A * gpX.e[e]) * dt;
+            dv.e[e] += -X.s * (v0.e[e] + A * byX.e[e]) * dt;
+            dw.e[e] += -X.s * (w0.e[e] + A * bzX.e[e]) * dt;
+        }
+    }
+    sched_fence();
+    if (ysv) {
+        const Slab<R>& S = d.sl[ysv + 1];
+        const int q = S.q(i, jb, k);
+        bq(S, q, bxY, byY, bzY);
+        if (zs) {
+            QuY = ldn<R, N>(S.rd[0] + q);
+            QvY = ldn<R, N>(S.rd[1] + q);
+            QwY = ldn<R, N>(S.rd[2] + q);
+        }
+#pragma unroll
+        for (int e = 0; e < N; ++e) {
+            Y[e] = pml_y(d, (ysp >> (2 * e)) & 3, jb + e);
+            du.e[e] += -Y[e].s * (u0.e[e] + A * bxY.e[e]) * dt;
+            dv.e[e] += Y[e].f * A * gpY.e[e] * dt - Y[e].s * v0.e[e] * dt;
+            dw.e[e] += -Y[e].s * (w0.e[e] + A * bzY.e[e]) * dt;
+            if (xs) {
+                du.e[e] += -(QuX.e[e] * X.s * Y[e].s + X.g * Y[e].s * A * bxX.e[e]) * dt;
+                dv.e[e] += -(QvX.e[e] * X.s * Y[e].s + Y[e].g * X.s * A * byX.e[e]) * dt;
+                dw.e[e] += -QwX.e[e] * X.s * Y[e].s * dt;
+            }
+        }
+    }
+    sched_fence();
+    if (zs) {
+        const Slab<R>& S = d.sl[zs + 3];
+        const int q = S.q(i, jb, k);
+        Arr<R, N> bxZ, byZ, bzZ;
+        bq(S, q, bxZ, byZ, bzZ);
+#pragma unroll
+        for (int e = 0; e < N; ++e) {
+            du.e[e] += -Z.s * (u0.e[e] + A * bxZ.e[e]) * dt;
+            dv.e[e] += -Z.s * (v0.e[e] + A * byZ.e[e]) * dt;
+            dw.e[e] += Z.f * A * gpZ.e[e] * dt - Z.s * w0.e[e] * dt;
+            if (xs) {
+                du.e[e] += -(QuX.e[e] * X.s * Z.s + X.g * Z.s * A * bxX.e[e]) * dt;
+                dv.e[e] += -QvX.e[e] * X.s * Z.s * dt;
+                dw.e[e] += -(QwX.e[e] * X.s * Z.s + Z.g * X.s * A * bzX.e[e]) * dt;
+            }
+            if (ysv) {
+                du.e[e] += -QuY.e[e] * Y[e].s * Z.s * dt;
+                dv.e[e] += -(QvY.e[e] * Y[e].s * Z.s + Y[e].g * Z.s * A * byY.e[e]) * dt;
+                dw.e[e] += -(QwY.e[e] * Y[e].s * Z.s + Z.g * Y[e].s * A * bzY.e[e]) * dt;
+            }
+        }
+    }
+}
+
+// forward neighbours of u, v, w for the wind advection terms
+template <typename R, int N>
+struct WindNb {
+    Arr<R, N> ui, uj, uk, vi, vj, vk, wi, wj, wk;  // f(i+1), f(j+1), f(g+1)
+};
+
+// Mean-wind part of the air velocity increment at one node: forward-
+// difference advection (U0 . grad) u and the central-difference shear
+// u . grad U0 (air.cpp:1476-1949).
+template <typename R>
+__device__ __forceinline__ void wind_dvel(const Dev<R>& d, int j, int k, R ax, R ay, R az, R u0, R v0, R w0, R ui,
+                                          R uj, R uk, R vi, R vj, R vk, R wi, R wj, R wk, R& du, R& dv, R& dw) {
+    const int q = k * d.NJ + j, wS = d.NJ;
+    const R U = ldg(d.Uw + q), V = ldg(d.Vw + q), W = ldg(d.Ww + q);
+    const R c1 = U * ax * d.dt, c2 = V * ay * d.dt, c3 = W * az * d.dt;
+    du += -c1 * (ui - u0) - c2 * (uj - u0) - c3 * (uk - u0);
+    dv += -c1 * (vi - v0) - c2 * (vj - v0) - c3 * (vk - v0);
+    dw += -c1 * (wi - w0) - c2 * (wj - w0) - c3 * (wk - w0);
+    const R h = R(0.5);
+    const R dUdY = ay * (ldg(d.Uw + q + 1) - ldg(d.Uw + q - 1)) * h;
+    const R dUdZ = az * (ldg(d.Uw + q + wS) - ldg(d.Uw + q - wS)) * h;
+    const R dVdY = ay * (ldg(d.Vw + q + 1) - ldg(d.Vw + q - 1)) * h;
+    const R dVdZ = az * (ldg(d.Vw + q + wS) - ldg(d.Vw + q - wS)) * h;
+    const R dWdY = ay * (ldg(d.Ww + q + 1) - ldg(d.Ww + q - 1)) * h;
+    const R dWdZ = az * (ldg(d.Ww + q + wS) - ldg(d.Ww + q - wS)) * h;
+    du += -(v0 * dUdY + w0 * dUdZ) * d.dt;
+    dv += -(v0 * dVdY + w0 * dVdZ) * d.dt;
+    dw += -(v0 * dWdY + w0 * dWdZ) * d.dt;
+}
+
+template <typename R, int N>
+struct Vel {
+    Arr<R, N> u, v, w;
+};
+
+// New velocity at N interior columns: u_n + increment, with p the pressure
+// the scheme prescribes (p_nn for FB_p_v). Air: air::cal_fuvw
+// (air.cpp:1476-1949); pore: porous::cal_fuvw (porous.cpp:58-104);
+// accumulation: calculation_2D::Cal_velocity (calculation_2D.cpp:548-579).
+// Column conventions as p_vec.
+template <typename R, bool WIND, int N>
+__device__ __forceinline__ Vel<R, N> vel_vec(const Dev<R>& d, const PlaneC<R>& pc, const RowC<R>& rc, int i, int jb,
+                                             const Arr<R, N>& ay, int ysp, const Arr<R, N>& u0, const Arr<R, N>& v0,
+                                             const Arr<R, N>& w0, const Arr<R, N>& p0, const Arr<R, N>& pim,
+                                             const Arr<R, N>& pjm, const Arr<R, N>& pkm, const WindNb<R, N>& nb,
+                                             bool qp_old) {
+    const R ax = rc.ax, az = pc.az;
+    Arr<R, N> bpi, bpj, bpk;
+#pragma unroll
+    for (int e = 0; e < N; ++e) {
+        bpi.e[e] = p0.e[e] - pim.e[e];
+        bpj.e[e] = p0.e[e] - pjm.e[e];
+        bpk.e[e] = p0.e[e] - pkm.e[e];
+    }
+    Vel<R, N> r;
+    if (pc.pore) {
+#pragma unroll
+        for (int e = 0; e < N; ++e) {
+            r.u.e[e] = u0.e[e] + (-d.pIBdtEff * (ax * bpi.e[e]) + u0.e[e] * d.pInvB - u0.e[e]);
+            r.v.e[e] = v0.e[e] + (-d.pIBdtEff * (ay.e[e] * bpj.e[e]) + v0.e[e] * d.pInvB - v0.e[e]);
+            r.w.e[e] = w0.e[e] + (-d.pIBdtEff * (az * bpk.e[e]) + w0.e[e] * d.pInvB - w0.e[e]);
+        }
+        return r;
+    }
+    Arr<R, N> gpX, gpY, gpZ, du, dv, dw;
+#pragma unroll
+    for (int e = 0; e < N; ++e) {
+        gpX.e[e] = ax * bpi.e[e];
+        gpY.e[e] = ay.e[e] * bpj.e[e];
+        gpZ.e[e] = az * bpk.e[e];
+        du.e[e] = -d.Aavdt * gpX.e[e];
+        dv.e[e] = -d.Aavdt * gpY.e[e];
+        dw.e[e] = -d.Aavdt * gpZ.e[e];
+    }
+    if (WIND) {
+#pragma unroll
+        for (int e = 0; e < N; ++e)
+            if (jb + e >= 1 && jb + e <= d.NJ - 2)
+                wind_dvel(d, jb + e, pc.k, ax, ay.e[e], az, u0.e[e], v0.e[e], w0.e[e], nb.ui.e[e], nb.uj.e[e],
+                          nb.uk.e[e], nb.vi.e[e], nb.vj.e[e], nb.vk.e[e], nb.wi.e[e], nb.wj.e[e], nb.wk.e[e],
+                          du.e[e], dv.e[e], dw.e[e]);
+    }
+    const int ysv = y_common<N>(ysp);
+    if (rc.xs | ysv | pc.zs) {
+        if (ysv != 3) {
+            pml_dvel_v<R, N>(d, i, jb, pc.k, rc.xs, ysp, ysv, pc.zs, ax, ay, az, u0, v0, w0, gpX, gpY, gpZ, p0, pim,
+                             pjm, pkm, qp_old, rc.X, pc.Z, du, dv, dw);
+        } else {  // both y layers within N columns (very narrow grids): column by column
+#pragma unroll
+            for (int e = 0; e < N; ++e) {
+                const int s = (ysp >> (2 * e)) & 3;
+                Arr<R, 1> due = el(du, e), dve = el(dv, e), dwe = el(dw, e);
+                pml_dvel_v<R, 1>(d, i, jb + e, pc.k, rc.xs, s, s, pc.zs, ax, el(ay, e), az, el(u0, e), el(v0, e),
+                                 el(w0, e), el(gpX, e), el(gpY, e), el(gpZ, e), el(p0, e), el(pim, e), el(pjm, e),
+                                 el(pkm, e), qp_old, rc.X, pc.Z, due, dve, dwe);
+                du.e[e] = due.e[0];
+                dv.e[e] = dve.e[0];
+                dw.e[e] = dwe.e[0];
+            }
+        }
+    }
+#pragma unroll
+    for (int e = 0; e < N; ++e) {
+        r.u.e[e] = u0.e[e] + du.e[e];
+        r.v.e[e] = v0.e[e] + dv.e[e];
+        r.w.e[e] = w0.e[e] + dw.e[e];
+    }
+    if (rc.inmask) {
+#pragma unroll
+        for (int e = 0; e < N; ++e) {
+            const int mv = mask_at(d, i, jb + e, pc.k);
+            if (mv == 1 || mv == 2) {
+                const R a = mv == 1 ? d.m1_ibdteff : d.m2_ibdteff, b = mv == 1 ? d.m1_ib : d.m2_ib;
+                r.u.e[e] = u0.e[e] + (-a * gpX.e[e] + u0.e[e] * b - u0.e[e]);
+                r.v.e[e] = v0.e[e] + (-a * gpY.e[e] + v0.e[e] * b - v0.e[e]);
+                r.w.e[e] = w0.e[e] + (-a * gpZ.e[e] + w0.e[e] * b - w0.e[e]);
+            }
+        }
+    }
+    return r;
+}
+
+// -------------------------------------------------- node-wise front ends
+// Pressure at an interior node with every operand read from global memory
+// (two-pass form).
 template <typename R, bool WIND>
-__device__ Vel3<R> fresh_vel(const Dev<R>& d, int i, int j, int g, bool y1_on) {
+__device__ R fresh_p(const Dev<R>& d, int i, int j, int g, bool y1_on) {
+    using A = Arr<R, 1>;
+    const PlaneC<R> pc = plane_c(d, g);
+    const RowC<R> rc = row_c(d, pc, i);
+    const A ay{{ldg((pc.pore ? d.ayP : d.ayA) + j)}};
+    const int ysp = pc.pore ? 0 : y_side(d, j, y1_on);
+    const size_t c = d.ix(g, i, j);
+    const size_t si = d.NJP, sg = static_cast<size_t>(d.NI) * d.NJP;
+    const R* P = d.pold;
+    A pim{{R(0)}}, pjm{{R(0)}}, pkm{{R(0)}};
+    if (WIND && !pc.pore) {
+        pim.e[0] = P[c - si];
+        pjm.e[0] = P[c - 1];
+        pkm.e[0] = P[c - sg];
+    }
+    return p_vec<R, WIND, 1>(d, pc, rc, i, j, ay, ysp, A{{d.u_in[c]}}, A{{d.v_in[c]}}, A{{d.w_in[c]}}, A{{P[c]}},
+                             A{{d.u_in[c + si]}}, A{{d.v_in[c + 1]}}, A{{d.w_in[c + sg]}}, pim, pjm, pkm)
+        .e[0];
+}
+
+// Velocity at an interior node with the scheme's pressure read from global
+// memory and the Qp slabs already advanced (two-pass form).
+template <typename R, bool WIND>
+__device__ Vel<R, 1> fresh_vel(const Dev<R>& d, int i, int j, int g, bool y1_on) {
+    using A = Arr<R, 1>;
+    const PlaneC<R> pc = plane_c(d, g);
+    const RowC<R> rc = row_c(d, pc, i);
+    const A ay{{ldg((pc.pore ? d.ayP : d.ayA) + j)}};
+    const int ysp = pc.pore ? 0 : y_side(d, j, y1_on);
+    const size_t c = d.ix(g, i, j);
+    const size_t si = d.NJP, sg = static_cast<size_t>(d.NI) * d.NJP;
     const R* p = d.p_in;
-    return fresh_vel_core<R, WIND>(d, GlobalFields<R>{d}, i, j, g, y1_on, p[d.ix(g, i, j)], p[d.ix(g, i - 1, j)],
-                                   p[d.ix(g, i, j - 1)], p[d.ix(g - 1, i, j)], false);
+    WindNb<R, 1> nb{};
+    if (WIND && !pc.pore)
+        nb = {A{{d.u_in[c + si]}}, A{{d.u_in[c + 1]}}, A{{d.u_in[c + sg]}}, A{{d.v_in[c + si]}}, A{{d.v_in[c + 1]}},
+              A{{d.v_in[c + sg]}}, A{{d.w_in[c + si]}}, A{{d.w_in[c + 1]}}, A{{d.w_in[c + sg]}}};
+    return vel_vec<R, WIND, 1>(d, pc, rc, i, j, ay, ysp, A{{d.u_in[c]}}, A{{d.v_in[c]}}, A{{d.w_in[c]}}, A{{p[c]}},
+                               A{{p[c - si]}}, A{{p[c - 1]}}, A{{p[c - sg]}}, nb, false);
 }
 
 // ------------------------------------------------ boundary resolution
@@ -355,13 +672,12 @@ __device__ R final_p(const Dev<R>& d, int i, int j, int g, bool y1_on) {
     }
     const int jc = j < 1 ? 1 : j;
     if (jc == d.NJ - 1) {
-        const GlobalFields<R> gf{d};
-        const R a = fresh_p<R, WIND>(d, gf, ic, d.NJ - 2, gc, y1_on);
-        const R b = fresh_p<R, WIND>(d, gf, ic, d.NJ - 3, gc, y1_on);
-        const R e = fresh_p<R, WIND>(d, gf, ic, d.NJ - 4, gc, y1_on);
+        const R a = fresh_p<R, WIND>(d, ic, d.NJ - 2, gc, y1_on);
+        const R b = fresh_p<R, WIND>(d, ic, d.NJ - 3, gc, y1_on);
+        const R e = fresh_p<R, WIND>(d, ic, d.NJ - 4, gc, y1_on);
         return R(15.0 / 8.0) * a - R(5.0 / 4.0) * b + R(3.0 / 8.0) * e;
     }
-    return fresh_p<R, WIND>(d, GlobalFields<R>{d}, ic, jc, gc, y1_on);
+    return fresh_p<R, WIND>(d, ic, jc, gc, y1_on);
 }
 
 // TDBC normal velocity at east-face node (i, air k), Cal_TDBC
@@ -373,6 +689,16 @@ __device__ double tdbc_v(const Dev<R>& d, int i, int k, double p) {
 #pragma unroll
     for (int q = 0; q < 6; ++q) s += d.td_e[q] * ps[q];
     return d.td_den * (p / d.td_z - s);
+}
+
+// Update_Psi at east-face node (i, air k) with the node's own TDBC value
+// (calculation_2D.cpp:1012-1017)
+template <typename R>
+__device__ __forceinline__ void psi_update(const Dev<R>& d, int i, int k, double p) {
+    const double vt = tdbc_v(d, i, k, p);
+    const size_t o = (static_cast<size_t>(i) * d.Kair + k) * 6;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) d.psi_out[o + q] = d.td_e[q] * d.psi_in[o + q] + d.td_adt[q] * vt;
 }
 
 // ------------------------------------------------------------ kernels
@@ -418,8 +744,8 @@ __global__ void __launch_bounds__(256) k_pressure(__grid_constant__ const Dev<R>
         for (int s = 0; s < 6; ++s) {
             const Slab<R>& S = d.sl[s];
             if (S.ni == 0 || (s == 2 && !y1_on)) continue;
-            if (i < S.i0 || i >= S.i0 + S.ni || j < S.j0 || j >= S.j0 + S.nj || k < S.k0 || k >= S.k0 + S.nk) continue;
-            const size_t q = S.at(i, j, k);
+            if (!S.holds_i(i) || !S.holds_j(j) || !S.holds_k(k)) continue;
+            const int q = S.q(i, j, k);
             S.wr[3][q] = S.rd[3][q] + d.dt * p;
         }
     }
@@ -487,11 +813,11 @@ __global__ void __launch_bounds__(256) k_velocity(__grid_constant__ const Dev<R>
         if (onE) face_j_east();
         face_k(onN, d.NG - 2);
     }
-    Vel3<R> f{R(0), R(0), R(0)};
+    Vel<R, 1> f{};
     if (ku == 0 || kv == 0 || kw == 0) f = fresh_vel<R, WIND>(d, ii, jj, gg, y1_on);
-    R u = ku == 0 ? f.u : R(0);
-    R v = kv == 0 ? f.v : R(0);
-    R w = kw == 0 ? f.w : R(0);
+    R u = ku == 0 ? f.u.e[0] : R(0);
+    R v = kv == 0 ? f.v.e[0] : R(0);
+    R w = kw == 0 ? f.w.e[0] : R(0);
     // The TDBC reads the "nn" pressure (calculation_2D.cpp:1000). With
     // FB_v_p the velocity half step comes first, so on the very first step
     // that buffer has never been written: zero in a zero-initialised start
@@ -518,8 +844,8 @@ __global__ void __launch_bounds__(256) k_velocity(__grid_constant__ const Dev<R>
         for (int s = 0; s < 6; ++s) {
             const Slab<R>& S = d.sl[s];
             if (S.ni == 0 || (s == 2 && !y1_on)) continue;
-            if (i < S.i0 || i >= S.i0 + S.ni || j < S.j0 || j >= S.j0 + S.nj || k < S.k0 || k >= S.k0 + S.nk) continue;
-            const size_t q = S.at(i, j, k);
+            if (!S.holds_i(i) || !S.holds_j(j) || !S.holds_k(k)) continue;
+            const int q = S.q(i, j, k);
             S.wr[0][q] = S.rd[0][q] + d.dt * u;
             S.wr[1][q] = S.rd[1][q] + d.dt * v;
             S.wr[2][q] = S.rd[2][q] + d.dt * w;

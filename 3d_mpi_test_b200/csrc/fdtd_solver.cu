@@ -17,7 +17,7 @@
 #include <cuda_runtime.h>
 
 #include "fdtd_device.cuh"
-#include "fdtd_fused.cuh"
+#include "fdtd_march.cuh"
 
 namespace fdtd {
 
@@ -149,9 +149,12 @@ class SolverImpl final : public SolverImplBase {
         FDTD_CK(cudaEventCreate(&ev1_));
         allocate();
         FDTD_CK(cudaDeviceSynchronize());
-        // FB_p_v runs as one fused pass per step; FB_v_p keeps the two passes
-        fused_ = (in.scheme == FB_P_V);
-        if (fused_) set_tiling(4, 16, std::min(NJ_, 256), 0);
+        // FB_p_v runs as one marching pass per step when a 2-row tile fits
+        // (one thread per 16-byte column vector, at most 512 per row);
+        // FB_v_p and larger rows keep the two passes
+        const int nvec = NJP_ / kVecMax;
+        fused_ = (in.scheme == FB_P_V) && nvec <= kMarchThreads && march_smem_bytes(make_tiling(2, 16, 1, kVecMax)) <= kSmemMax;
+        if (fused_) set_tiling(4, 16, 256, 0);
         reset(in.time_domain);
     }
 
@@ -229,6 +232,9 @@ class SolverImpl final : public SolverImplBase {
             gOff_ = 0;
             NG_ = air_.K;
         }
+        // device indexing of fields and PML slabs is 32-bit
+        if (static_cast<double>(NG_) * NI_ * NJP_ >= 2147483647.0)
+            fail(-2, "domain holds 2^31 or more nodes per field (32-bit device indexing)");
         build_pml_static();
         build_hill();
         // TDBC constants: t_bar = dt / tau (airpore.cpp:333, calculation_2D.cpp:1012-1028)
@@ -437,15 +443,23 @@ class SolverImpl final : public SolverImplBase {
         sd[3] = {0, NJ_ - 1 - Y2_, 0, NI_, Y2_ ? Y2_ + 1 : 0, Kair_};
         sd[4] = {0, 0, 0, NI_, NJ_, K1_ ? K1_ + 1 : 0};
         sd[5] = {0, 0, Kair_ - 1 - K2_, NI_, NJ_, K2_ ? K2_ + 1 : 0};
+        // slab rows are padded to 16 bytes from a 16-byte-aligned column
+        // origin ja <= j0, so column vectors of the marching kernel load and
+        // store slab rows as whole 16-byte vectors
+        const int V = static_cast<int>(16 / sizeof(R));
         for (int s = 0; s < 6; ++s) {
+            sd[s].ja = sd[s].j0 / V * V;
+            sd[s].jp = (sd[s].j0 + sd[s].nj - sd[s].ja + V - 1) / V * V;
             slab_[s] = sd[s];
-            const size_t n = static_cast<size_t>(sd[s].ni) * sd[s].nj * sd[s].nk;
+            const size_t n = static_cast<size_t>(sd[s].ni) * sd[s].jp * sd[s].nk;
             slab_n_[s] = n;
             for (int b = 0; b < 2; ++b)
                 for (int c = 0; c < 4; ++c) Q_[s][b][c] = n ? track(dalloc<R>(n)) : nullptr;
         }
-        d_axA_ = track(dalloc<R>(NI_)); d_ayA_ = track(dalloc<R>(NJ_));
-        d_axP_ = track(dalloc<R>(NI_)); d_ayP_ = track(dalloc<R>(NJ_));
+        // per-column metric arrays padded to the row pitch: the marching kernel
+        // reads them as 16-byte vectors
+        d_axA_ = track(dalloc<R>(NI_)); d_ayA_ = track(dalloc<R>(NJP_));
+        d_axP_ = track(dalloc<R>(NI_)); d_ayP_ = track(dalloc<R>(NJP_));
         d_azG_ = track(dalloc<R>(NG_));
         for (int q = 0; q < 3; ++q) {
             d_sx_[q] = track(dalloc<R>(NI_));
@@ -666,6 +680,7 @@ class SolverImpl final : public SolverImplBase {
             Slab<R>& S = d.sl[s];
             S.i0 = slab_[s].i0; S.j0 = slab_[s].j0; S.k0 = slab_[s].k0;
             S.ni = slab_n_[s] ? slab_[s].ni : 0; S.nj = slab_[s].nj; S.nk = slab_[s].nk;
+            S.ja = slab_[s].ja; S.jp = slab_[s].jp;
             if (!slab_n_[s]) continue;
             // Qp: pressure pass reads old (o) writes new (nw); velocity pass reads the
             // Qp the pressure pass of this step wrote. Qu/Qv/Qw mirror that.
@@ -724,63 +739,99 @@ class SolverImpl final : public SolverImplBase {
         return d;
     }
 
-    // Tile choice for the fused pass: TI rows x all NJ columns x GC planes per
-    // block; nt threads stride the columns.
-    // shared memory of a fused tile (variant 0: two new-pressure slots;
-    // variant 1: plus the mbarriers and the bulk-copy ring)
-    size_t fused_smem_bytes(const FusedTiling& t, int variant) const {
-        const size_t srows = t.rows_max + 1, sr = t.rows_max + 3;
-        const size_t pslots = 2 * srows * NJ_ * sizeof(R);
-        if (variant == 0) return pslots;
-        return 128 + pslots + 16 + static_cast<size_t>(t.nstage) * 4 * sr * NJP_ * sizeof(R);
+    // Marching tile: TI rows x all NJ columns x GC planes per block; trows
+    // thread rows of NJP / VW threads (VW consecutive columns each).
+    static constexpr size_t kSmemMax = 227 * 1024;
+    static constexpr int kMarchThreads = 256;  // k_march launch bound
+    static constexpr int kVecMax = static_cast<int>(16 / sizeof(R));
+
+    // shared memory of a tile: mbarriers, two new-pressure slots of
+    // rows_max + 1 rows, and the ring of nstage planes; a stage holds at most
+    // n + 1 u rows and n + W v, w and p rows each (n = rows_max + 1 stencil
+    // rows, W = 1 with wind)
+    size_t march_smem_bytes(const MarchTiling& t) const {
+        const size_t row = static_cast<size_t>(NJP_) * sizeof(R);
+        const size_t n = t.rows_max + 1, W = wind_on_ ? 1 : 0;
+        return 128 + 2 * (t.rows_max + 1) * row + static_cast<size_t>(t.nstage) * (4 * n + 1 + 3 * W) * row;
     }
 
-    FusedTiling make_tiling(int TI, int GC) const {
-        FusedTiling t{};
-        t.TI = std::max(2, TI);
+    MarchTiling make_tiling(int TI, int GC, int trows, int VW) const {
+        MarchTiling t{};
+        t.TI = std::max(2, std::min(TI, NI_));
         t.nrb = std::max(1, NI_ / t.TI);
         t.rows_max = (t.nrb == 1) ? NI_ : t.TI + NI_ % t.TI;
         t.GC = std::max(1, GC);
         t.nchunk = (NG_ - 2 + t.GC - 1) / t.GC;
         t.nstage = 3 + (wind_on_ ? 1 : 0);  // planes g-1 (wind), g, g+1 resident, g+2 in flight
+        t.VW = VW;
+        const int nvec = NJP_ / VW;
+        t.trows = std::max(1, std::min({trows, kMarchThreads / nvec, t.rows_max + 1}));
         return t;
     }
 
-    // Tile choice for the fused pass: TI rows x all NJ columns x GC planes per
-    // block; nt threads stride the columns; variant 0 plain, 1 bulk-staged.
-    void set_tiling(int TI, int GC, int nt, int variant) {
-        const FusedTiling t = make_tiling(TI, GC);
-        if (variant != 0 && variant != 1) fail(-5, "variant must be 0 (plain) or 1 (bulk-staged)");
-        const size_t smem = fused_smem_bytes(t, variant);
-        if (smem > 227 * 1024) fail(-2, "fused tile does not fit shared memory");
-        nt = std::min(std::max(32, (nt + 31) / 32 * 32), 256);
+    // Tile choice: TI rows, GC planes, about nt threads per block (rounded to
+    // whole thread rows), vw columns per thread (0: 16 bytes; else 2 or 4
+    // with vw * sizeof(R) <= 16).
+    void set_tiling(int TI, int GC, int nt, int vw) {
+        const int VW = vw == 0 ? kVecMax : vw;
+        if (VW != 2 && VW != 4) fail(-5, "column vector width must be 0, 2 or 4");
+        if (VW > kVecMax) fail(-2, "column vector wider than 16 bytes");
+        const int nvec = NJP_ / VW;
+        if (nvec > kMarchThreads) fail(-2, "one thread row would exceed the marching kernel's block size");
+        const MarchTiling t = make_tiling(TI, GC, std::max(1, nt / nvec), VW);
+        const size_t smem = march_smem_bytes(t);
+        if (smem > kSmemMax) fail(-2, "marching tile does not fit shared memory");
         if (smem > 48 * 1024) {
             const int b = static_cast<int>(smem);
-            if (variant == 0) {
-                FDTD_CK(cudaFuncSetAttribute(k_fused<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
-                FDTD_CK(cudaFuncSetAttribute(k_fused<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
-            } else {
-                FDTD_CK(cudaFuncSetAttribute(k_fused_tma<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
-                FDTD_CK(cudaFuncSetAttribute(k_fused_tma<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
-            }
+            for_march_kernels([&](const void* k) {
+                FDTD_CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+            });
         }
         tiling_ = t;
-        fused_threads_ = nt;
+        fused_threads_ = t.trows * nvec;
         fused_smem_ = smem;
-        fused_variant_ = variant;
         graph_dirty_ = true;
+    }
+
+    template <typename F>
+    static void for_march_kernels(F f) {
+        f(reinterpret_cast<const void*>(k_march<R, true, 2>));
+        f(reinterpret_cast<const void*>(k_march<R, false, 2>));
+        if constexpr (sizeof(R) == 4) {
+            f(reinterpret_cast<const void*>(k_march<R, true, 4>));
+            f(reinterpret_cast<const void*>(k_march<R, false, 4>));
+        }
+    }
+
+    // resident blocks per SM of the marching kernel for a block shape
+    int march_occupancy(int VW, int threads, size_t smem) const {
+        int n = 0;
+        const void* k = reinterpret_cast<const void*>(k_march<R, false, 2>);
+        if constexpr (sizeof(R) == 4) {
+            if (VW == 4) k = wind_on_ ? reinterpret_cast<const void*>(k_march<R, true, 4>)
+                                      : reinterpret_cast<const void*>(k_march<R, false, 4>);
+        }
+        if (VW == 2 && wind_on_) k = reinterpret_cast<const void*>(k_march<R, true, 2>);
+        if (smem > 48 * 1024)
+            FDTD_CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+        FDTD_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, threads, smem));
+        return n;
     }
 
     void launch_fused(int par) {
         const dim3 grd(tiling_.nrb, tiling_.nchunk, 1), blk(fused_threads_, 1, 1);
         const Dev<R> d = params_fused(par);
-        if (fused_variant_ == 1) {
-            if (wind_on_) k_fused_tma<R, true><<<grd, blk, fused_smem_, stream_>>>(d, tiling_, par);
-            else k_fused_tma<R, false><<<grd, blk, fused_smem_, stream_>>>(d, tiling_, par);
-        } else {
-            if (wind_on_) k_fused<R, true><<<grd, blk, fused_smem_, stream_>>>(d, tiling_, par);
-            else k_fused<R, false><<<grd, blk, fused_smem_, stream_>>>(d, tiling_, par);
+        if constexpr (sizeof(R) == 4) {
+            if (tiling_.VW == 4) {
+                if (wind_on_) k_march<R, true, 4><<<grd, blk, fused_smem_, stream_>>>(d, tiling_, par);
+                else k_march<R, false, 4><<<grd, blk, fused_smem_, stream_>>>(d, tiling_, par);
+                FDTD_CK(cudaGetLastError());
+                ++launches_;
+                return;
+            }
         }
+        if (wind_on_) k_march<R, true, 2><<<grd, blk, fused_smem_, stream_>>>(d, tiling_, par);
+        else k_march<R, false, 2><<<grd, blk, fused_smem_, stream_>>>(d, tiling_, par);
         FDTD_CK(cudaGetLastError());
         ++launches_;
     }
@@ -844,7 +895,7 @@ class SolverImpl final : public SolverImplBase {
             if (!slab_n_[s]) continue;
             const int r = slab_[s].ni * slab_[s].nk;
             for (int c = 0; c < 4; ++c) {
-                k_shift_rows<R><<<(r + 127) / 128, 128, 0, stream_>>>(Q_[s][par_][c], r, slab_[s].nj, sh, lead, tempJ,
+                k_shift_rows<R><<<(r + 127) / 128, 128, 0, stream_>>>(Q_[s][par_][c], r, slab_[s].jp, sh, lead, tempJ,
                                                                       NJ_, 0);
                 FDTD_CK(cudaGetLastError());
                 ++launches_;
@@ -1003,8 +1054,8 @@ class SolverImpl final : public SolverImplBase {
             for (int a = 0; a < S.ni; ++a)
                 for (int b = 0; b < S.nj; ++b)
                     for (int c = 0; c < S.nk; ++c)
-                        out[(static_cast<size_t>(a) * S.nj + b) * S.nk + c] =
-                            static_cast<double>(h[(static_cast<size_t>(c) * S.ni + a) * S.nj + b]);
+                        out[(static_cast<size_t>(a) * S.nj + b) * S.nk + c] = static_cast<double>(
+                            h[(static_cast<size_t>(c) * S.ni + a) * S.jp + (b + S.j0 - S.ja)]);
         }
         return 1;
     }
@@ -1039,9 +1090,10 @@ class SolverImpl final : public SolverImplBase {
     }
 
     // Project autotuner: time every candidate tile on this domain and keep the
-    // fastest. Candidates: variant {plain, bulk-staged} x rows per block
-    // {2, 4, 8} x planes per block chosen so the grid fills the SMs 1, 2 or 4
-    // times x threads {64, 128, 256}; tiles that do not fit are skipped.
+    // fastest. Candidates: column vector width {2, 4} x rows per block
+    // {2, 4, 8} x thread rows {1, 2, 4} x plane chunks sized so the grid
+    // fills 1..4 whole waves of the resident-block slots the occupancy
+    // calculator reports for that tile; tiles that do not fit are skipped.
     std::array<int, 4> autotune(int nsteps) override {
         FDTD_CK(cudaSetDevice(device_));
         if (!fused_) fail(-2, "autotune applies to the fused FB_p_v pass only");
@@ -1049,22 +1101,31 @@ class SolverImpl final : public SolverImplBase {
         FDTD_CK(cudaGetDeviceProperties(&prop, device_));
         const int sms = prop.multiProcessorCount;
         std::vector<std::array<int, 4>> cands;
-        for (int variant : {0, 1})
+        auto add = [&](const std::array<int, 4>& c) {
+            if (std::find(cands.begin(), cands.end(), c) == cands.end()) cands.push_back(c);
+        };
+        for (int VW : {2, 4}) {
+            if (VW > kVecMax || NJP_ / VW > kMarchThreads) continue;
+            const int nvec = NJP_ / VW;
             for (int TI : {2, 4, 8}) {
-                const int nrb = std::max(1, NI_ / TI);
-                for (int waves : {1, 2, 4}) {
-                    const int chunks = std::max(1, (waves * sms + nrb - 1) / nrb);
-                    const int GC = std::max(1, (NG_ - 2 + chunks - 1) / chunks);
-                    for (int nt : {64, 128, 256}) {
-                        if (nt > ((NJ_ + 31) / 32) * 32 && nt != 64) continue;
-                        if (fused_smem_bytes(make_tiling(TI, GC), variant) > 227 * 1024) continue;
-                        cands.push_back({TI, GC, nt, variant});
+                for (int tr : {1, 2, 4}) {
+                    const MarchTiling t0 = make_tiling(TI, 1, tr, VW);
+                    const size_t smem = march_smem_bytes(t0);
+                    if (t0.trows != tr || smem > kSmemMax) continue;
+                    const int per_sm = march_occupancy(VW, tr * nvec, smem);
+                    if (per_sm < 1) continue;
+                    const int slots = per_sm * sms;
+                    for (int waves = 1; waves <= 4; ++waves) {
+                        const int chunks = std::max(1, (waves * slots) / t0.nrb);
+                        const int GC = std::max(1, (NG_ - 2 + chunks - 1) / chunks);
+                        add({TI, GC, tr * nvec, VW});
                     }
                 }
             }
+        }
         const int saved_horizon = horizon_;
         const int h = std::max(horizon_, (nsteps + 2) * static_cast<int>(cands.size()) + 4);
-        std::array<int, 4> best{tiling_.TI, tiling_.GC, fused_threads_, fused_variant_};
+        std::array<int, 4> best{tiling_.TI, tiling_.GC, fused_threads_, tiling_.VW};
         double best_ms = 1e300;
         reset(h);
         for (const auto& c : cands) {
@@ -1082,6 +1143,7 @@ class SolverImpl final : public SolverImplBase {
    private:
     struct SlabDesc {
         int i0, j0, k0, ni, nj, nk;
+        int ja = 0, jp = 0;  // 16-byte-aligned column origin and padded row pitch
     };
 
     int device_ = 0;
@@ -1126,9 +1188,8 @@ class SolverImpl final : public SolverImplBase {
     cudaGraphExec_t graph_exec_ = nullptr;
     bool graph_dirty_ = true;
     bool fused_ = false;
-    FusedTiling tiling_{};
+    MarchTiling tiling_{};
     int fused_threads_ = 0;
-    int fused_variant_ = 0;
     size_t fused_smem_ = 0;
     // receivers
     std::vector<std::array<int, 3>> rec_idx_;

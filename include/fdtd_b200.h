@@ -104,17 +104,19 @@ int fdtd_get_slab(fdtd_solver *h, int s, int comp, double *out, int *dims);
 size_t fdtd_state_elems(const fdtd_solver *h);
 int fdtd_copy_state(fdtd_solver *h, int dir, void *host);
 
-/* Tile shape of the fused FB_p_v pass: rows_per_block i-rows x all j
- * columns x planes_per_block g-planes per thread block, threads_per_block
- * threads striding the columns (multiple of 32, <= 256); variant 0 reads
- * the stencil inputs from global memory, 1 streams them into shared memory
- * with bulk asynchronous copies. Takes effect for the next step. Returns
- * FDTD_ERR_UNSUPPORTED when the tile does not fit shared memory. */
+/* Tile shape of the single-pass FB_p_v marching kernel: rows_per_block
+ * i-rows x all j columns x planes_per_block g-planes per thread block. A
+ * block has one thread per 16-byte column vector (NJP*size/16 threads) per
+ * "thread row"; threads_per_block is rounded down to whole thread rows
+ * (at least 1, at most 512 threads and rows_per_block + 1 thread rows).
+ * variant is reserved and must be 0 (FDTD_ERR_ARG otherwise). Takes effect
+ * for the next step. Returns FDTD_ERR_UNSUPPORTED when the tile does not
+ * fit shared memory. */
 int fdtd_set_tiling(fdtd_solver *h, int rows_per_block, int planes_per_block, int threads_per_block, int variant);
 
 /* Times each candidate tile on this handle's domain (nsteps FB steps each,
  * CUDA events), keeps the fastest and returns it in best[4] (rows, planes,
- * threads, variant); the state is reset to t = 0 afterwards. */
+ * threads, 0); the state is reset to t = 0 afterwards. */
 int fdtd_autotune(fdtd_solver *h, int nsteps, int *best);
 
 /* Kernel launches issued since creation (both passes, graphs included). */

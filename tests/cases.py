@@ -148,9 +148,35 @@ def stretched():
     return c, REC
 
 
+def odd_columns_wind():
+    """29 columns: the east face column (j = 28) starts a new 16-byte column
+    vector in both precisions; with the east TDBC and a log wind profile."""
+    c = _base(nj=29, bc=(PML, RIGID, TDBC, PML, PML, PML), pore=(1.79, 0.877, 5.1e4),
+              velocity_coef=1.5, velocity_method=5)
+    return c, REC
+
+
+def odd_columns_porous():
+    """29 columns over porous ground with the east TDBC."""
+    layer = 6
+    c = _base(nj=29, bc=(PML, POROUS, TDBC, PML, PML, PML), pore=(math.sqrt(1.8), 0.3, 2.0e5))
+    c.pore_Z = uniform_axis(layer + 2, -layer * D, D)
+    c.pore_dxyz = (D, D, D)
+    c.source = (0.5, 0.55, 0.15)
+    return c, REC
+
+
+def narrow_y():
+    """5 columns with 2-node y PML layers on both sides: one 16-byte column
+    vector holds nodes of both y layers."""
+    c = _base(ni=12, nj=5, nk=12, pml_nodes=(3, 3, 2, 2, 0, 3))
+    c.source = (0.3, 0.1, 0.3)
+    return c, [(0.3, 0.1, 0.25), (0.35, 0.15, 0.3)]
+
+
 CASES: Dict[str, Callable[[], Tuple[Case, List]]] = {
     f.__name__: f
     for f in [pml_rigid, tdbc_east, porous_ground, porous_tdbc_fine_pore, south_pml_all_faces, front_only_pml,
               back_only_pml, all_rigid, wind_linear, wind_log, wind_vortex, hill(1), hill(2), hill(3), hill(4),
-              hill(5), moving_frame, fb_v_p, delayed_y1, stretched]
+              hill(5), moving_frame, fb_v_p, delayed_y1, stretched, odd_columns_wind, odd_columns_porous, narrow_y]
 }

@@ -168,12 +168,14 @@ def test_nonfinite_watchdog(case_dirs):
         a.advance(2)  # usable after the error
 
 
-TILINGS = [(2, 1, 32, 0), (3, 5, 64, 0), (8, 7, 256, 0), (4, 16, 128, 0),
-           (2, 1, 32, 1), (3, 5, 64, 1), (8, 7, 256, 1), (4, 16, 128, 1)]
+# (rows, planes, threads): thread counts round down to whole thread rows of
+# NJP / V column-vector threads, so these give 1, 2, 4 and the maximum
+TILINGS = [(2, 1, 1, 0), (3, 5, 32, 0), (8, 7, 1000, 0), (4, 16, 64, 0), (5, 3, 48, 0)]
 
 
 @pytest.mark.parametrize("tiling", TILINGS)
-@pytest.mark.parametrize("name", ["porous_tdbc_fine_pore", "south_pml_all_faces", "wind_log", "moving_frame"])
+@pytest.mark.parametrize("name", ["porous_tdbc_fine_pore", "south_pml_all_faces", "wind_log", "moving_frame",
+                                  "odd_columns_wind", "odd_columns_porous"])
 def test_fused_tilings_match_oracle(name, tiling, case_dirs):
     """The fused FB_p_v pass is exact for any tile shape: halo rows,
     warm-up planes, odd row splits, single-plane chunks."""
@@ -199,7 +201,7 @@ def test_autotune_keeps_results_exact(case_dirs):
     ref = oracle.run_case(d, rec, n)
     with pkg.Airpore(d, "f32") as a:
         best = a.autotune(4)
-        assert best[0] >= 2 and best[1] >= 1 and best[2] % 32 == 0 and best[3] in (0, 1)
+        assert best[0] >= 2 and best[1] >= 1 and best[2] >= 1 and best[3] == 0
         a.set_receivers(rec)
         r = a.get_output(n)
     assert rel_l2(r, ref["receivers"]) <= TOL_F32
