@@ -212,10 +212,12 @@ class Airpore:
         self._check(self._L.fdtd_copy_state(self._h, 1 if to_device else 0, host.ctypes.data_as(ctypes.c_void_p)))
 
     def set_tiling(self, rows_per_block: int, planes_per_block: int, threads_per_block: int,
-                   variant: int = 0) -> None:
-        """Tile of the single-pass marching kernel (rows, planes, threads per
-        block; threads round down to whole rows of column-vector threads)."""
-        self._check(self._L.fdtd_set_tiling(self._h, rows_per_block, planes_per_block, threads_per_block, variant))
+                   vector_width: int = 0) -> None:
+        """Tile of the single-pass marching kernel: rows, planes and threads per
+        block (threads round down to whole rows of column-vector threads) and
+        columns per thread (0: 16 bytes of columns)."""
+        self._check(self._L.fdtd_set_tiling(self._h, rows_per_block, planes_per_block, threads_per_block,
+                                            vector_width))
 
     def autotune(self, nsteps: int = 20) -> Tuple[int, int, int, int]:
         best = (ctypes.c_int * 4)()

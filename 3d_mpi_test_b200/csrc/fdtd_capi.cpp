@@ -140,9 +140,9 @@ int fdtd_copy_state(fdtd_solver* h, int dir, void* host) {
     return guard([&] { h->s->copy_state(dir, host); });
 }
 
-int fdtd_set_tiling(fdtd_solver* h, int rows_per_block, int planes_per_block, int threads_per_block, int variant) {
+int fdtd_set_tiling(fdtd_solver* h, int rows_per_block, int planes_per_block, int threads_per_block, int vector_width) {
     if (!h) return bad("null handle");
-    return guard([&] { h->s->set_tiling(rows_per_block, planes_per_block, threads_per_block, variant); });
+    return guard([&] { h->s->set_tiling(rows_per_block, planes_per_block, threads_per_block, vector_width); });
 }
 
 int fdtd_autotune(fdtd_solver* h, int nsteps, int* best) {

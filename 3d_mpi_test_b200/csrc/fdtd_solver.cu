@@ -449,7 +449,7 @@ class SolverImpl final : public SolverImplBase {
         const int V = static_cast<int>(16 / sizeof(R));
         for (int s = 0; s < 6; ++s) {
             sd[s].ja = sd[s].j0 / V * V;
-            sd[s].jp = (sd[s].j0 + sd[s].nj - sd[s].ja + V - 1) / V * V;
+            sd[s].jp = sd[s].nj ? (sd[s].j0 + sd[s].nj - sd[s].ja + V - 1) / V * V : 0;
             slab_[s] = sd[s];
             const size_t n = static_cast<size_t>(sd[s].ni) * sd[s].jp * sd[s].nk;
             slab_n_[s] = n;

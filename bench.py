@@ -226,10 +226,15 @@ def run_gpu(args, rank, world, local_rank):
     for prec in ("f32", "f64"):
         word = 4 if prec == "f32" else 8
         a = pkg.Airpore(case_dir, prec, device=local_rank)
+        tile = None
         if args.tile:
             tile = tuple(int(x) for x in args.tile.split(","))
-            a.set_tiling(*tile)
-        else:
+            try:
+                a.set_tiling(*tile)
+            except pkg.FdtdError as e:
+                print(f"tile {tile} rejected for {prec} ({e}); autotuning", file=sys.stderr)
+                tile = None
+        if tile is None:
             tile = a.autotune(10)  # the project's tile autotuner, on this domain
         a.set_receivers(rec)
         a.reset(horizon)
@@ -289,13 +294,15 @@ def run_gpu(args, rank, world, local_rank):
     roof = {"bound": "hbm", "achieved": round(f32["achieved_gbs"], 1), "peak": hbm_peak, "unit": "GB/s",
             "frac": round(f32["achieved_gbs"] / hbm_peak, 4), "traffic": None,
             "peak_kind": peak_kind,
-            "kernel": "k_fused (one launch = one FB step of the whole domain), FP32",
-            "tile_rows_planes_threads_variant": list(f32["tile"]),
+            "kernel": "k_march (one launch = one FB step of the whole domain), FP32",
+            "tile_rows_planes_threads_width": list(f32["tile"]),
             "algorithmic_bytes_per_step": f32["bytes_per_step"]}
-    prof = os.path.join(ROOT, "profiles", "traffic.json")
+    prof = os.path.join(ROOT, "profiles", "traffic.txt")
     if os.path.exists(prof):
         with open(prof) as fh:
-            roof["traffic"] = json.load(fh).get("f32_bytes_per_step")
+            for ln in fh:
+                if ln.startswith("f32_bytes_per_step:"):
+                    roof["traffic"] = int(ln.split(":")[1])
     line = {
         "metric": METRIC, "value": round(f32["gcell"], 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(f32["ms_per_bench_step"], 4), "higher_is_better": True,
@@ -304,7 +311,7 @@ def run_gpu(args, rank, world, local_rank):
                    "cells_per_fb_step": cells, "l2": "flushed (512 MB write) between bench steps",
                    "parallelism": f"replicas x{world}" if world > 1 else "single device-resident domain"},
         "fp64": {"value": round(f64["gcell"], 3), "ms_per_step": round(f64["ms_per_bench_step"], 4),
-                 "tile_rows_planes_threads_variant": list(f64["tile"]),
+                 "tile_rows_planes_threads_width": list(f64["tile"]),
                  "achieved_gbs": round(f64["achieved_gbs"], 1),
                  "frac": round(f64["achieved_gbs"] / hbm_peak, 4),
                  "fp32_speedup": round(f32["gcell"] / f64["gcell"], 3)},
@@ -359,7 +366,7 @@ def main():
     ap.add_argument("--inner", type=int, default=200)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--tile", default="", help="rows,planes,threads,variant of the fused pass (default: autotune)")
+    ap.add_argument("--tile", default="", help="rows,planes,threads,vector-width of the marching kernel (default: autotune)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

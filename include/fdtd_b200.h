@@ -106,17 +106,19 @@ int fdtd_copy_state(fdtd_solver *h, int dir, void *host);
 
 /* Tile shape of the single-pass FB_p_v marching kernel: rows_per_block
  * i-rows x all j columns x planes_per_block g-planes per thread block. A
- * block has one thread per 16-byte column vector (NJP*size/16 threads) per
- * "thread row"; threads_per_block is rounded down to whole thread rows
- * (at least 1, at most 512 threads and rows_per_block + 1 thread rows).
- * variant is reserved and must be 0 (FDTD_ERR_ARG otherwise). Takes effect
- * for the next step. Returns FDTD_ERR_UNSUPPORTED when the tile does not
- * fit shared memory. */
-int fdtd_set_tiling(fdtd_solver *h, int rows_per_block, int planes_per_block, int threads_per_block, int variant);
+ * thread owns vector_width consecutive columns (0: 16 bytes of columns, i.e.
+ * 4 in FP32 and 2 in FP64; else 2 or 4 with vector_width * element size <=
+ * 16); a "thread row" is NJP / vector_width threads and threads_per_block
+ * is rounded down to whole thread rows (at least 1, at most 256 threads and
+ * rows_per_block + 1 thread rows). Takes effect for the next step. Returns
+ * FDTD_ERR_ARG for a bad vector width and FDTD_ERR_UNSUPPORTED when the
+ * tile does not fit shared memory or one thread row exceeds 256 threads. */
+int fdtd_set_tiling(fdtd_solver *h, int rows_per_block, int planes_per_block, int threads_per_block,
+                    int vector_width);
 
 /* Times each candidate tile on this handle's domain (nsteps FB steps each,
  * CUDA events), keeps the fastest and returns it in best[4] (rows, planes,
- * threads, 0); the state is reset to t = 0 afterwards. */
+ * threads, vector width); the state is reset to t = 0 afterwards. */
 int fdtd_autotune(fdtd_solver *h, int nsteps, int *best);
 
 /* Kernel launches issued since creation (both passes, graphs included). */

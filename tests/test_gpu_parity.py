@@ -201,7 +201,7 @@ def test_autotune_keeps_results_exact(case_dirs):
     ref = oracle.run_case(d, rec, n)
     with pkg.Airpore(d, "f32") as a:
         best = a.autotune(4)
-        assert best[0] >= 2 and best[1] >= 1 and best[2] >= 1 and best[3] == 0
+        assert best[0] >= 2 and best[1] >= 1 and best[2] >= 1 and best[3] in (2, 4)
         a.set_receivers(rec)
         r = a.get_output(n)
     assert rel_l2(r, ref["receivers"]) <= TOL_F32
