@@ -199,10 +199,12 @@ def run_gpu(args, rank, world, local_rank):
     import torch
 
     pkg = importlib.import_module("3d_mpi_test_b200")
+    replicas = importlib.import_module("3d_mpi_test_b200.replicas")
     torch.cuda.set_device(local_rank)
     dist = None
     if world > 1:
         import torch.distributed as dist  # noqa: F811
+    group = replicas.ReplicaGroup(dist, "cuda")
     tmp = tempfile.mkdtemp(prefix=f"bench_r{rank}_")
     case_dir, rec, cells, case = make_case(tmp)
     inner = args.inner
@@ -212,15 +214,9 @@ def run_gpu(args, rank, world, local_rank):
 
     def barrier():
         torch.cuda.synchronize()
-        if dist is not None:
-            dist.barrier()
+        group.barrier()
 
-    def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    max_over_ranks = group.max_over_ranks
 
     results = {}
     for prec in ("f32", "f64"):
@@ -261,9 +257,9 @@ def run_gpu(args, rank, world, local_rank):
         barrier()
         wall = time.perf_counter() - t0
         launches = a.launch_count() - launches0
-        dev_ms = max_over_ranks(dev_ms)
         steps_total = args.steps * inner
-        gcell = world * cells * steps_total / (dev_ms * 1e-3) / 1e9
+        gcell = group.throughput(cells, steps_total, dev_ms)  # whole job: all ranks' cells / slowest rank
+        dev_ms = max_over_ranks(dev_ms)
         ab = algorithmic_bytes(case, word)
         achieved = ab["bytes_per_step"] / (dev_ms * 1e-3 / steps_total) / 1e9
         results[prec] = {"gcell": gcell, "ms_per_bench_step": dev_ms / args.steps, "wall_s": wall, "tile": tile,
