@@ -36,6 +36,7 @@ EXPORTS = (
     "fdtd_run", "fdtd_advance", "fdtd_step_pressure", "fdtd_step_velocity", "fdtd_get_field",
     "fdtd_set_field", "fdtd_get_psi", "fdtd_get_slab", "fdtd_state_elems", "fdtd_copy_state",
     "fdtd_launch_count", "fdtd_last_device_ms", "fdtd_fb_step_noalloc", "fdtd_set_tiling", "fdtd_autotune",
+    "fdtd_fft", "fdtd_spectrum", "fdtd_band_levels",
 )
 
 
@@ -79,8 +80,11 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
         "fdtd_launch_count": ([vp], ctypes.c_longlong),
         "fdtd_last_device_ms": ([vp, dp], i),
         "fdtd_fb_step_noalloc": ([i, i, i, i, dp, dp, dp] + [ctypes.c_double] * 7 + [vp] * 9, i),
-        "fdtd_set_tiling": ([vp, i, i, i, i], i),
+        "fdtd_set_tiling": ([vp, i, i, i, i, i], i),
         "fdtd_autotune": ([vp, i, ip], i),
+        "fdtd_fft": ([i, dp, i, i, i, dp, dp], i),
+        "fdtd_spectrum": ([i, dp, i, i, i, ctypes.c_longlong, ctypes.c_longlong, dp], i),
+        "fdtd_band_levels": ([i, dp, i, i, i, ctypes.c_double, i, dp, dp], i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -212,15 +216,16 @@ class Airpore:
         self._check(self._L.fdtd_copy_state(self._h, 1 if to_device else 0, host.ctypes.data_as(ctypes.c_void_p)))
 
     def set_tiling(self, rows_per_block: int, planes_per_block: int, threads_per_block: int,
-                   vector_width: int = 0) -> None:
+                   vector_width: int = 0, ring_stages: int = 0) -> None:
         """Tile of the single-pass marching kernel: rows, planes and threads per
-        block (threads round down to whole rows of column-vector threads) and
-        columns per thread (0: 16 bytes of columns)."""
+        block (threads round down to whole rows of column-vector threads),
+        columns per thread (0: 16 bytes of columns) and staging-ring planes
+        (0: the minimum)."""
         self._check(self._L.fdtd_set_tiling(self._h, rows_per_block, planes_per_block, threads_per_block,
-                                            vector_width))
+                                            vector_width, ring_stages))
 
-    def autotune(self, nsteps: int = 20) -> Tuple[int, int, int, int]:
-        best = (ctypes.c_int * 4)()
+    def autotune(self, nsteps: int = 20) -> Tuple[int, int, int, int, int]:
+        best = (ctypes.c_int * 5)()
         self._check(self._L.fdtd_autotune(self._h, nsteps, best))
         return tuple(best)
 
@@ -231,3 +236,75 @@ class Airpore:
         v = ctypes.c_double()
         self._check(self._L.fdtd_last_device_ms(self._h, ctypes.byref(v)))
         return v.value
+
+
+# --------------------------------------------------------------- spectra
+# Base-2 third-octave centres 1000 * 2^(n/3) Hz from 50 Hz to 2 kHz (17 bands).
+THIRD_OCTAVE_50_2K = tuple(1000.0 * 2.0 ** (n / 3.0) for n in range(-13, 4))
+
+
+def _check_rc(L, rc: int) -> None:
+    if rc != FDTD_OK:
+        raise FdtdError(rc, L.fdtd_last_error().decode())
+
+
+def _fft_m(fft_m: int) -> int:
+    if not 1 <= fft_m <= 24:
+        raise FdtdError(FDTD_ERR_ARG, "fft_m must be 1..24")
+    return 1 << fft_m
+
+
+def _traces(traces) -> np.ndarray:
+    a = np.ascontiguousarray(np.atleast_2d(np.asarray(traces, dtype=np.float64)))
+    if a.ndim != 2 or a.shape[1] < 1:
+        raise FdtdError(FDTD_ERR_ARG, "traces must be [nrec][nt]")
+    return a
+
+
+def fft(traces, fft_m: int, device: int = 0, lib_path: Optional[str] = None) -> Tuple[np.ndarray, np.ndarray]:
+    """The reference's post-processing transform (airpore::get_FFT_y1 with
+    FFT(1, m, ...)) of every receiver trace on the GPU: zero-padded to 2^m
+    points, forward, scaled by 1/2^m. Returns re, im [nrec][2^m]."""
+    L = load_library(lib_path)
+    t = _traces(traces)
+    n = _fft_m(fft_m)
+    re = np.empty((t.shape[0], n))
+    im = np.empty((t.shape[0], n))
+    _check_rc(L, L.fdtd_fft(device, _dp(t), t.shape[0], t.shape[1], fft_m, _dp(re), _dp(im)))
+    return re, im
+
+
+def spectrum(traces, fft_m: int, dt: float, k0: int = 0, nk: Optional[int] = None, device: int = 0,
+             lib_path: Optional[str] = None) -> Tuple[np.ndarray, np.ndarray]:
+    """FFT_output's spectrum: frequencies k / (dt 2^m) and magnitudes |X_k|
+    [nrec][nk] for k = k0 .. k0+nk-1 (default: all 2^(m-1)+1 bins)."""
+    L = load_library(lib_path)
+    t = _traces(traces)
+    n = _fft_m(fft_m)
+    if nk is None:
+        nk = n // 2 + 1 - k0
+    mag = np.empty((t.shape[0], nk))
+    _check_rc(L, L.fdtd_spectrum(device, _dp(t), t.shape[0], t.shape[1], fft_m, k0, nk, _dp(mag)))
+    return (k0 + np.arange(nk)) / (dt * n), mag
+
+
+def band_levels(traces, fft_m: int, dt: float, centres=THIRD_OCTAVE_50_2K, device: int = 0,
+                lib_path: Optional[str] = None) -> np.ndarray:
+    """Band levels 10 log10(sum |X_k|^2) over each band [fc 2^-1/6, fc 2^1/6)
+    per receiver trace: [nrec][nband] dB."""
+    L = load_library(lib_path)
+    t = _traces(traces)
+    fc = np.ascontiguousarray(centres, dtype=np.float64)
+    out = np.empty((t.shape[0], len(fc)))
+    _check_rc(L, L.fdtd_band_levels(device, _dp(t), t.shape[0], t.shape[1], fft_m, dt, len(fc), _dp(fc), _dp(out)))
+    return out
+
+
+def excess_attenuation(traces, free_field_traces, fft_m: int, dt: float, centres=THIRD_OCTAVE_50_2K,
+                       device: int = 0, lib_path: Optional[str] = None) -> np.ndarray:
+    """Excess attenuation per band [nrec][nband] dB: the band levels of the
+    solve with ground (and terrain, wind) minus those of the same source and
+    receivers in a free field (all faces absorbing)."""
+    return band_levels(traces, fft_m, dt, centres, device, lib_path) - \
+        band_levels(free_field_traces, fft_m, dt, centres, device, lib_path)
+

@@ -22,7 +22,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
               "--expt-relaxed-constexpr", "-I", os.path.join(ROOT, "include")]
 
-SOURCES = ["fdtd_solver.cu", "fdtd_input.cpp", "fdtd_capi.cpp", "fdtd_noalloc.cu"]
+SOURCES = ["fdtd_solver.cu", "fdtd_input.cpp", "fdtd_capi.cpp", "fdtd_noalloc.cu", "fdtd_spectra.cu"]
 
 
 def nvcc() -> str:

@@ -140,16 +140,17 @@ int fdtd_copy_state(fdtd_solver* h, int dir, void* host) {
     return guard([&] { h->s->copy_state(dir, host); });
 }
 
-int fdtd_set_tiling(fdtd_solver* h, int rows_per_block, int planes_per_block, int threads_per_block, int vector_width) {
+int fdtd_set_tiling(fdtd_solver* h, int rows_per_block, int planes_per_block, int threads_per_block, int vector_width,
+                    int ring_stages) {
     if (!h) return bad("null handle");
-    return guard([&] { h->s->set_tiling(rows_per_block, planes_per_block, threads_per_block, vector_width); });
+    return guard([&] { h->s->set_tiling(rows_per_block, planes_per_block, threads_per_block, vector_width, ring_stages); });
 }
 
 int fdtd_autotune(fdtd_solver* h, int nsteps, int* best) {
     if (!h || !best || nsteps <= 0) return bad("bad autotune arguments");
     return guard([&] {
         const auto b = h->s->autotune(nsteps);
-        for (int q = 0; q < 4; ++q) best[q] = b[q];
+        for (int q = 0; q < 5; ++q) best[q] = b[q];
     });
 }
 
@@ -162,3 +163,20 @@ int fdtd_last_device_ms(const fdtd_solver* h, double* ms) {
 }
 
 }  // extern "C"
+
+int fdtd_fft(int device, const double* traces, int nrec, int nt, int fft_m, double* re, double* im) {
+    if (!traces || !re || !im) return bad("null argument");
+    return guard([&] { fdtd::fft_forward(device, traces, nrec, nt, fft_m, re, im); });
+}
+
+int fdtd_spectrum(int device, const double* traces, int nrec, int nt, int fft_m, long long k0, long long nk,
+                  double* mag) {
+    if (!traces || !mag) return bad("null argument");
+    return guard([&] { fdtd::spectrum_bins(device, traces, nrec, nt, fft_m, static_cast<long>(k0), static_cast<long>(nk), mag); });
+}
+
+int fdtd_band_levels(int device, const double* traces, int nrec, int nt, int fft_m, double dt, int nband,
+                     const double* fc, double* levels_db) {
+    if (!traces || !fc || !levels_db) return bad("null argument");
+    return guard([&] { fdtd::band_levels(device, traces, nrec, nt, fft_m, dt, nband, fc, levels_db); });
+}

@@ -41,7 +41,7 @@ struct MarchTiling {
     int GC;        // core planes per block
     int nchunk;    // plane chunks
     int rows_max;  // most rows any block owns (shared-memory sizing)
-    int nstage;    // bulk-copy ring depth
+    int nstage;    // bulk-copy ring depth: W + 2 planes in use, the rest in flight
     int trows;     // thread rows: a block is trows x (NJP / VW) threads
     int VW;        // columns per thread
 };
@@ -434,9 +434,10 @@ __global__ void __launch_bounds__(256) k_march(__grid_constant__ const Dev<R> d,
     for (int q = first; q < c1; ++q) {
         const int slot = q & 1;
         if (tid == 0) {
-            if (q + 2 <= c1 && q + 2 > issued_hi) {
-                issue(q + 2);
-                issued_hi = q + 2;
+            const int x = q + G.ns - 1 - W;  // into the stage plane q-1-W used last
+            if (x <= c1 && x > issued_hi) {
+                issue(x);
+                issued_hi = x;
             }
             if (q + 3 <= c1) prefetch_slabs(q + 3);
         }

@@ -124,8 +124,8 @@ class SolverImplBase {
     virtual void copy_state(int dir, void* host) = 0;
     virtual long long launch_count() const = 0;
     virtual double last_device_ms() const = 0;
-    virtual void set_tiling_api(int TI, int GC, int nt, int variant) = 0;
-    virtual std::array<int, 4> autotune(int nsteps) = 0;
+    virtual void set_tiling_api(int TI, int GC, int nt, int vw, int stages) = 0;
+    virtual std::array<int, 5> autotune(int nsteps) = 0;
 };
 
 template <typename R>
@@ -153,8 +153,8 @@ class SolverImpl final : public SolverImplBase {
         // (one thread per 16-byte column vector, at most 512 per row);
         // FB_v_p and larger rows keep the two passes
         const int nvec = NJP_ / kVecMax;
-        fused_ = (in.scheme == FB_P_V) && nvec <= kMarchThreads && march_smem_bytes(make_tiling(2, 16, 1, kVecMax)) <= kSmemMax;
-        if (fused_) set_tiling(4, 16, 256, 0);
+        fused_ = (in.scheme == FB_P_V) && nvec <= kMarchThreads && march_smem_bytes(make_tiling(2, 16, 1, kVecMax, 0)) <= kSmemMax;
+        if (fused_) set_tiling(4, 16, 256, 0, 0);
         reset(in.time_domain);
     }
 
@@ -744,6 +744,7 @@ class SolverImpl final : public SolverImplBase {
     static constexpr size_t kSmemMax = 227 * 1024;
     static constexpr int kMarchThreads = 256;  // k_march launch bound
     static constexpr int kVecMax = static_cast<int>(16 / sizeof(R));
+    static constexpr int kMaxStages = 12;  // mbarriers fit the 128-byte head of shared memory
 
     // shared memory of a tile: mbarriers, two new-pressure slots of
     // rows_max + 1 rows, and the ring of nstage planes; a stage holds at most
@@ -755,14 +756,17 @@ class SolverImpl final : public SolverImplBase {
         return 128 + 2 * (t.rows_max + 1) * row + static_cast<size_t>(t.nstage) * (4 * n + 1 + 3 * W) * row;
     }
 
-    MarchTiling make_tiling(int TI, int GC, int trows, int VW) const {
+    // stages: staging-ring planes (0: the minimum; planes g-1 with wind, g and
+    // g+1 are in use while the later planes are in flight)
+    MarchTiling make_tiling(int TI, int GC, int trows, int VW, int stages) const {
         MarchTiling t{};
         t.TI = std::max(2, std::min(TI, NI_));
         t.nrb = std::max(1, NI_ / t.TI);
         t.rows_max = (t.nrb == 1) ? NI_ : t.TI + NI_ % t.TI;
         t.GC = std::max(1, GC);
         t.nchunk = (NG_ - 2 + t.GC - 1) / t.GC;
-        t.nstage = 3 + (wind_on_ ? 1 : 0);  // planes g-1 (wind), g, g+1 resident, g+2 in flight
+        const int smin = 3 + (wind_on_ ? 1 : 0);
+        t.nstage = stages == 0 ? smin : std::max(stages, smin);
         t.VW = VW;
         const int nvec = NJP_ / VW;
         t.trows = std::max(1, std::min({trows, kMarchThreads / nvec, t.rows_max + 1}));
@@ -772,13 +776,14 @@ class SolverImpl final : public SolverImplBase {
     // Tile choice: TI rows, GC planes, about nt threads per block (rounded to
     // whole thread rows), vw columns per thread (0: 16 bytes; else 2 or 4
     // with vw * sizeof(R) <= 16).
-    void set_tiling(int TI, int GC, int nt, int vw) {
+    void set_tiling(int TI, int GC, int nt, int vw, int stages) {
+        if (stages < 0 || stages > kMaxStages) fail(-5, "ring stages must be 0..12");
         const int VW = vw == 0 ? kVecMax : vw;
         if (VW != 2 && VW != 4) fail(-5, "column vector width must be 0, 2 or 4");
         if (VW > kVecMax) fail(-2, "column vector wider than 16 bytes");
         const int nvec = NJP_ / VW;
         if (nvec > kMarchThreads) fail(-2, "one thread row would exceed the marching kernel's block size");
-        const MarchTiling t = make_tiling(TI, GC, std::max(1, nt / nvec), VW);
+        const MarchTiling t = make_tiling(TI, GC, std::max(1, nt / nvec), VW, stages);
         const size_t smem = march_smem_bytes(t);
         if (smem > kSmemMax) fail(-2, "marching tile does not fit shared memory");
         if (smem > 48 * 1024) {
@@ -1083,58 +1088,60 @@ class SolverImpl final : public SolverImplBase {
     }
     long long launch_count() const override { return launches_; }
 
-    void set_tiling_api(int TI, int GC, int nt, int variant) override {
+    void set_tiling_api(int TI, int GC, int nt, int vw, int stages) override {
         FDTD_CK(cudaSetDevice(device_));
         if (!fused_) fail(-2, "tiling applies to the fused FB_p_v pass only");
-        set_tiling(TI, GC, nt, variant);
+        set_tiling(TI, GC, nt, vw, stages);
     }
 
     // Project autotuner: time every candidate tile on this domain and keep the
     // fastest. Candidates: column vector width {2, 4} x rows per block
-    // {2, 4, 8} x thread rows {1, 2, 4} x plane chunks sized so the grid
-    // fills 1..4 whole waves of the resident-block slots the occupancy
-    // calculator reports for that tile; tiles that do not fit are skipped.
-    std::array<int, 4> autotune(int nsteps) override {
+    // {2, 4, 8} x thread rows {1, 2, 4} x ring stages {minimum, +1, +2} x
+    // plane chunks sized so the grid fills 1..4 whole waves of the
+    // resident-block slots the occupancy calculator reports for that tile;
+    // tiles that do not fit are skipped.
+    std::array<int, 5> autotune(int nsteps) override {
         FDTD_CK(cudaSetDevice(device_));
         if (!fused_) fail(-2, "autotune applies to the fused FB_p_v pass only");
         cudaDeviceProp prop{};
         FDTD_CK(cudaGetDeviceProperties(&prop, device_));
         const int sms = prop.multiProcessorCount;
-        std::vector<std::array<int, 4>> cands;
-        auto add = [&](const std::array<int, 4>& c) {
+        const int smin = 3 + (wind_on_ ? 1 : 0);
+        std::vector<std::array<int, 5>> cands;
+        auto add = [&](const std::array<int, 5>& c) {
             if (std::find(cands.begin(), cands.end(), c) == cands.end()) cands.push_back(c);
         };
         for (int VW : {2, 4}) {
             if (VW > kVecMax || NJP_ / VW > kMarchThreads) continue;
             const int nvec = NJP_ / VW;
-            for (int TI : {2, 4, 8}) {
-                for (int tr : {1, 2, 4}) {
-                    const MarchTiling t0 = make_tiling(TI, 1, tr, VW);
-                    const size_t smem = march_smem_bytes(t0);
-                    if (t0.trows != tr || smem > kSmemMax) continue;
-                    const int per_sm = march_occupancy(VW, tr * nvec, smem);
-                    if (per_sm < 1) continue;
-                    const int slots = per_sm * sms;
-                    for (int waves = 1; waves <= 4; ++waves) {
-                        const int chunks = std::max(1, (waves * slots) / t0.nrb);
-                        const int GC = std::max(1, (NG_ - 2 + chunks - 1) / chunks);
-                        add({TI, GC, tr * nvec, VW});
+            for (int TI : {2, 4, 8})
+                for (int tr : {1, 2, 4})
+                    for (int extra = 0; extra <= 2; ++extra) {
+                        const MarchTiling t0 = make_tiling(TI, 1, tr, VW, smin + extra);
+                        const size_t smem = march_smem_bytes(t0);
+                        if (t0.trows != tr || smem > kSmemMax) continue;
+                        const int per_sm = march_occupancy(VW, tr * nvec, smem);
+                        if (per_sm < 1) continue;
+                        const int slots = per_sm * sms;
+                        for (int waves = 1; waves <= 4; ++waves) {
+                            const int chunks = std::max(1, (waves * slots) / t0.nrb);
+                            const int GC = std::max(1, (NG_ - 2 + chunks - 1) / chunks);
+                            add({TI, GC, tr * nvec, VW, smin + extra});
+                        }
                     }
-                }
-            }
         }
         const int saved_horizon = horizon_;
         const int h = std::max(horizon_, (nsteps + 2) * static_cast<int>(cands.size()) + 4);
-        std::array<int, 4> best{tiling_.TI, tiling_.GC, fused_threads_, tiling_.VW};
+        std::array<int, 5> best{tiling_.TI, tiling_.GC, fused_threads_, tiling_.VW, tiling_.nstage};
         double best_ms = 1e300;
         reset(h);
         for (const auto& c : cands) {
-            set_tiling(c[0], c[1], c[2], c[3]);
+            set_tiling(c[0], c[1], c[2], c[3], c[4]);
             advance(2, nullptr);  // graph build and first-touch outside the timing
             advance(nsteps, nullptr);
             if (last_ms_ < best_ms) { best_ms = last_ms_; best = c; }
         }
-        set_tiling(best[0], best[1], best[2], best[3]);
+        set_tiling(best[0], best[1], best[2], best[3], best[4]);
         reset(saved_horizon);
         return best;
     }
@@ -1227,8 +1234,8 @@ int Solver::get_slab(int s, int c, double* out, int* dims) { return impl_->get_s
 size_t Solver::state_elems() const { return impl_->state_elems(); }
 void Solver::copy_state(int dir, void* host) { impl_->copy_state(dir, host); }
 long long Solver::launch_count() const { return impl_->launch_count(); }
-void Solver::set_tiling(int TI, int GC, int nt, int variant) { impl_->set_tiling_api(TI, GC, nt, variant); }
-std::array<int, 4> Solver::autotune(int nsteps) { return impl_->autotune(nsteps); }
+void Solver::set_tiling(int TI, int GC, int nt, int vw, int stages) { impl_->set_tiling_api(TI, GC, nt, vw, stages); }
+std::array<int, 5> Solver::autotune(int nsteps) { return impl_->autotune(nsteps); }
 double Solver::last_device_ms() const { return impl_->last_device_ms(); }
 
 }  // namespace fdtd

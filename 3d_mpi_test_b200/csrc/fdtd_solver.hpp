@@ -19,6 +19,15 @@ struct SolverError {
 
 class SolverImplBase;
 
+// Receiver post-processing on a device (fdtd_spectra.cu): the reference's
+// zero-padded, 1/2^m-scaled forward FFT of each trace [nrec][nt], as the
+// complex spectra [nrec][2^m], as magnitudes of bins [k0, k0 + nk), or as
+// third-octave-style band levels 10 log10(sum |X_k|^2) [nrec][nband].
+void fft_forward(int device, const double* traces, int nrec, int nt, int m, double* re, double* im);
+void spectrum_bins(int device, const double* traces, int nrec, int nt, int m, long k0, long nk, double* mag);
+void band_levels(int device, const double* traces, int nrec, int nt, int m, double dt, int nband, const double* fc,
+                 double* levels);
+
 class Solver {
    public:
     // precision: 0 FP64, 1 FP32. Throws SolverError.
@@ -50,8 +59,9 @@ class Solver {
     size_t state_elems() const;
     void copy_state(int dir, void* host);
     long long launch_count() const;
-    void set_tiling(int rows_per_block, int planes_per_block, int threads_per_block, int variant);
-    std::array<int, 4> autotune(int nsteps);
+    void set_tiling(int rows_per_block, int planes_per_block, int threads_per_block, int vector_width,
+                    int ring_stages);
+    std::array<int, 5> autotune(int nsteps);
     double last_device_ms() const;
 
    private:

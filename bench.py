@@ -291,7 +291,7 @@ def run_gpu(args, rank, world, local_rank):
             "frac": round(f32["achieved_gbs"] / hbm_peak, 4), "traffic": None,
             "peak_kind": peak_kind,
             "kernel": "k_march (one launch = one FB step of the whole domain), FP32",
-            "tile_rows_planes_threads_width": list(f32["tile"]),
+            "tile_rows_planes_threads_width_stages": list(f32["tile"]),
             "algorithmic_bytes_per_step": f32["bytes_per_step"]}
     prof = os.path.join(ROOT, "profiles", "traffic.txt")
     if os.path.exists(prof):
@@ -307,7 +307,7 @@ def run_gpu(args, rank, world, local_rank):
                    "cells_per_fb_step": cells, "l2": "flushed (512 MB write) between bench steps",
                    "parallelism": f"replicas x{world}" if world > 1 else "single device-resident domain"},
         "fp64": {"value": round(f64["gcell"], 3), "ms_per_step": round(f64["ms_per_bench_step"], 4),
-                 "tile_rows_planes_threads_width": list(f64["tile"]),
+                 "tile_rows_planes_threads_width_stages": list(f64["tile"]),
                  "achieved_gbs": round(f64["achieved_gbs"], 1),
                  "frac": round(f64["achieved_gbs"] / hbm_peak, 4),
                  "fp32_speedup": round(f32["gcell"] / f64["gcell"], 3)},
@@ -362,7 +362,7 @@ def main():
     ap.add_argument("--inner", type=int, default=200)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--tile", default="", help="rows,planes,threads,vector-width of the marching kernel (default: autotune)")
+    ap.add_argument("--tile", default="", help="rows,planes,threads,vector-width,ring-stages of the marching kernel (default: autotune)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

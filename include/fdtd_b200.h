@@ -110,15 +110,19 @@ int fdtd_copy_state(fdtd_solver *h, int dir, void *host);
  * 4 in FP32 and 2 in FP64; else 2 or 4 with vector_width * element size <=
  * 16); a "thread row" is NJP / vector_width threads and threads_per_block
  * is rounded down to whole thread rows (at least 1, at most 256 threads and
- * rows_per_block + 1 thread rows). Takes effect for the next step. Returns
- * FDTD_ERR_ARG for a bad vector width and FDTD_ERR_UNSUPPORTED when the
- * tile does not fit shared memory or one thread row exceeds 256 threads. */
+ * rows_per_block + 1 thread rows). ring_stages: planes of the shared-memory
+ * staging ring (0: the minimum, 3, or 4 with wind; each further stage keeps
+ * one more plane in flight; at most 12). Takes effect for the next step.
+ * Returns FDTD_ERR_ARG for a bad vector width or stage count and
+ * FDTD_ERR_UNSUPPORTED when the tile does not fit shared memory or one
+ * thread row exceeds 256 threads. */
 int fdtd_set_tiling(fdtd_solver *h, int rows_per_block, int planes_per_block, int threads_per_block,
-                    int vector_width);
+                    int vector_width, int ring_stages);
 
 /* Times each candidate tile on this handle's domain (nsteps FB steps each,
- * CUDA events), keeps the fastest and returns it in best[4] (rows, planes,
- * threads, vector width); the state is reset to t = 0 afterwards. */
+ * CUDA events), keeps the fastest and returns it in best[5] (rows, planes,
+ * threads, vector width, ring stages); the state is reset to t = 0
+ * afterwards. */
 int fdtd_autotune(fdtd_solver *h, int nsteps, int *best);
 
 /* Kernel launches issued since creation (both passes, graphs included). */
@@ -126,6 +130,30 @@ long long fdtd_launch_count(const fdtd_solver *h);
 
 /* CUDA events around the last fdtd_advance's device work: milliseconds. */
 int fdtd_last_device_ms(const fdtd_solver *h, double *ms);
+
+/* Receiver post-processing (replaces airpore::get_FFT_y1, airpore.cpp:966-1011,
+ * with FFT / FFT_output, FFT.cpp:15-120). traces: host [nrec][nt] pressure
+ * histories (fdtd_run output); each is zero-padded (or cut) to 2^fft_m
+ * points and transformed on `device` by the reference's radix-2 FFT,
+ * forward and scaled by 1/2^fft_m, with the reference's twiddle sequence
+ * and rounding -- bit for bit the reference's result. fdtd_fft returns the
+ * complex spectra re, im [nrec][2^fft_m]. 1 <= fft_m <= 24. */
+int fdtd_fft(int device, const double *traces, int nrec, int nt, int fft_m, double *re, double *im);
+
+/* Magnitudes |X_k| of the same transform for bins k = k0 .. k0+nk-1
+ * (FFT_output prints k = 0 .. 2^(fft_m-1) at frequency k / (dt 2^fft_m));
+ * mag [nrec][nk]. */
+int fdtd_spectrum(int device, const double *traces, int nrec, int nt, int fft_m, long long k0, long long nk,
+                  double *mag);
+
+/* Band levels (extension, no counterpart in the reference): for each trace
+ * and each band centre fc[b] > 0, 10 log10 of the sum of |X_k|^2 over the
+ * bins whose frequency k / (dt 2^fft_m) lies in [fc 2^(-1/6), fc 2^(1/6))
+ * -- third-octave bands for base-2 centres 1000 * 2^(n/3); -inf for a band
+ * without bins. levels_db [nrec][nband]. The difference of two runs' levels
+ * (ground minus free field) is the excess attenuation per band. */
+int fdtd_band_levels(int device, const double *traces, int nrec, int nt, int fft_m, double dt, int nband,
+                     const double *fc, double *levels_db);
 
 /* Allocation-free single FB_p_v step. No counterpart in the reference: it
  * serves callers that cannot allocate device memory (a host that owns all

@@ -1593,3 +1593,58 @@ int orc_get_wind(const orc *o, int comp, double *out)
     memcpy(out, src, sizeof(double) * o->air.g.I * o->air.g.J * o->air.g.K);
     return 0;
 }
+
+/* ------------------------------------------------------------------ */
+/* Post-processing: the reference's in-place radix-2 FFT (FFT.cpp:15-83),
+ * used by airpore::get_FFT_y1 (airpore.cpp:966-1011) on zero-padded
+ * receiver traces.  Restated step for step so that, without FMA
+ * contraction, the result matches the compiled reference bit for bit:
+ *   1. bit-reversal permutation of the 2^m points;
+ *   2. m butterfly stages; within a stage the twiddle factor starts at 1
+ *      and is advanced by complex multiplication with the stage root, and
+ *      the next stage's root follows from the half-angle formulas
+ *      (cos -> sqrt((1+cos)/2), sin -> -+sqrt((1-cos)/2));
+ *   3. the forward transform (dir = 1) divides by the point count. */
+void orc_fft(int dir, int m, double *re, double *im) {
+    long n = 1;
+    for (int s = 0; s < m; ++s) n *= 2;
+    /* 1. bit reversal: walk j through the reversed counter */
+    long j = 0;
+    for (long i = 0; i < n - 1; ++i) {
+        if (i < j) {
+            double t = re[i]; re[i] = re[j]; re[j] = t;
+            t = im[i]; im[i] = im[j]; im[j] = t;
+        }
+        long bit = n >> 1;
+        while (bit <= j) { j -= bit; bit >>= 1; }
+        j += bit;
+    }
+    /* 2. butterflies */
+    double root_c = -1.0, root_s = 0.0;
+    long half = 1;
+    for (int s = 0; s < m; ++s) {
+        const long span = half * 2;
+        double wc = 1.0, ws = 0.0;
+        for (long a = 0; a < half; ++a) {
+            for (long i = a; i < n; i += span) {
+                const long b = i + half;
+                const double tr = wc * re[b] - ws * im[b];
+                const double ti = wc * im[b] + ws * re[b];
+                re[b] = re[i] - tr;
+                im[b] = im[i] - ti;
+                re[i] += tr;
+                im[i] += ti;
+            }
+            const double next_c = wc * root_c - ws * root_s;
+            ws = wc * root_s + ws * root_c;
+            wc = next_c;
+        }
+        root_s = sqrt((1.0 - root_c) / 2.0);
+        if (dir == 1) root_s = -root_s;
+        root_c = sqrt((1.0 + root_c) / 2.0);
+        half = span;
+    }
+    /* 3. forward scaling */
+    if (dir == 1)
+        for (long i = 0; i < n; ++i) { re[i] /= n; im[i] /= n; }
+}

@@ -42,6 +42,10 @@ int orc_get_slab(const orc *o, int slab, int comp, double *out, int *dims);
 /* Wind arrays Uav/Vav/Wav [i][j][k] (comp 0/1/2). */
 int orc_get_wind(const orc *o, int comp, double *out);
 
+/* In-place radix-2 FFT of 2^m points (FFT.cpp:15-83): dir 1 forward
+ * (scaled by 1/2^m), -1 inverse. */
+void orc_fft(int dir, int m, double *re, double *im);
+
 #ifdef __cplusplus
 }
 #endif

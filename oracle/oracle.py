@@ -48,6 +48,8 @@ def lib():
         L.orc_get_slab.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                    ctypes.POINTER(ctypes.c_int)]
         L.orc_get_wind.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+        L.orc_fft.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+        L.orc_fft.restype = None
         _lib = L
     return _lib
 
@@ -154,3 +156,28 @@ def run_case(case_dir: str, receivers: Sequence[Tuple[float, float, float]], nst
     out["slabs"] = oc.slabs()
     oc.close()
     return out
+
+
+def fft(re: np.ndarray, im: np.ndarray, direction: int = 1) -> Tuple[np.ndarray, np.ndarray]:
+    """The reference's radix-2 FFT (FFT.cpp:15-83) on copies of re, im
+    (length 2^m); direction 1 is forward and scaled by 1/2^m."""
+    n = len(re)
+    m = n.bit_length() - 1
+    if n != 1 << m or len(im) != n:
+        raise ValueError("length must be a power of two")
+    r = np.ascontiguousarray(re, dtype=np.float64).copy()
+    i = np.ascontiguousarray(im, dtype=np.float64).copy()
+    lib().orc_fft(direction, m, _dp(r), _dp(i))
+    return r, i
+
+
+def spectrum(trace: np.ndarray, m: int, dt: float) -> Tuple[np.ndarray, np.ndarray]:
+    """airpore::get_FFT_y1 + FFT_output (airpore.cpp:966-1011, FFT.cpp:86-120):
+    zero-pad the trace to 2^m points, forward FFT, and return the bin
+    frequencies k / (dt 2^m) and magnitudes |X_k| for k = 0 .. 2^(m-1)."""
+    n = 1 << m
+    re = np.zeros(n)
+    re[:min(len(trace), n)] = trace[:n]
+    r, i = fft(re, np.zeros(n), 1)
+    k = np.arange(n // 2 + 1)
+    return k / dt / n, np.hypot(r[: n // 2 + 1], i[: n // 2 + 1])

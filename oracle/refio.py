@@ -12,6 +12,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_HARNESS = os.path.join(HERE, "_ref", "ref_harness")
+REF_FFT = os.path.join(HERE, "_ref", "ref_fft")
 
 SLAB_NAMES = {0: "x1", 1: "x2", 2: "y1", 3: "y2", 4: "z1", 5: "z2"}
 
@@ -64,3 +65,13 @@ def run_reference(case_dir: str, out_path: str, receivers_file: Optional[str] = 
         cmd += ["--steps", str(steps)]
     subprocess.run(cmd, check=True)
     return read_dump(out_path)
+
+
+def run_reference_fft(re, im, direction: int = 1, exe: str = REF_FFT):
+    """The compiled reference FFT() on copies of re, im (length 2^m)."""
+    n = len(re)
+    m = n.bit_length() - 1
+    buf = np.concatenate([np.asarray(re, np.float64), np.asarray(im, np.float64)]).tobytes()
+    out = subprocess.run([exe, str(m), str(direction)], input=buf, capture_output=True, check=True).stdout
+    a = np.frombuffer(out, dtype=np.float64)
+    return a[:n].copy(), a[n:].copy()
