@@ -36,7 +36,7 @@ EXPORTS = (
     "fdtd_run", "fdtd_advance", "fdtd_step_pressure", "fdtd_step_velocity", "fdtd_get_field",
     "fdtd_set_field", "fdtd_get_psi", "fdtd_get_slab", "fdtd_state_elems", "fdtd_copy_state",
     "fdtd_launch_count", "fdtd_last_device_ms", "fdtd_fb_step_noalloc", "fdtd_set_tiling", "fdtd_autotune",
-    "fdtd_fft", "fdtd_spectrum", "fdtd_band_levels",
+    "fdtd_fft", "fdtd_spectrum", "fdtd_band_levels", "fdtd_save_restart", "fdtd_load_restart",
 )
 
 
@@ -85,6 +85,8 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
         "fdtd_fft": ([i, dp, i, i, i, dp, dp], i),
         "fdtd_spectrum": ([i, dp, i, i, i, ctypes.c_longlong, ctypes.c_longlong, dp], i),
         "fdtd_band_levels": ([i, dp, i, i, i, ctypes.c_double, i, dp, dp], i),
+        "fdtd_save_restart": ([vp, cp], i),
+        "fdtd_load_restart": ([vp, cp, i], i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -214,6 +216,18 @@ class Airpore:
 
     def copy_state(self, host: np.ndarray, to_device: bool) -> None:
         self._check(self._L.fdtd_copy_state(self._h, 1 if to_device else 0, host.ctypes.data_as(ctypes.c_void_p)))
+
+    def Save_restart(self, path: str) -> None:
+        """airpore::Save_restart: the state in the reference's restart layout
+        plus the frame counters and TDBC state."""
+        self._check(self._L.fdtd_save_restart(self._h, os.fsencode(path)))
+
+    def Read_restart(self, path: str, reference_semantics: bool = False) -> None:
+        """airpore::Read_restart: load a restart file (this library's or the
+        reference's) for the same case; continue with advance. With
+        reference_semantics the PML integrals and TDBC state restart from zero,
+        as the reference's own restart continues."""
+        self._check(self._L.fdtd_load_restart(self._h, os.fsencode(path), 1 if reference_semantics else 0))
 
     def set_tiling(self, rows_per_block: int, planes_per_block: int, threads_per_block: int,
                    vector_width: int = 0, ring_stages: int = 0) -> None:

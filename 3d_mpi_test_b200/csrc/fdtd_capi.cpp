@@ -180,3 +180,13 @@ int fdtd_band_levels(int device, const double* traces, int nrec, int nt, int fft
     if (!traces || !fc || !levels_db) return bad("null argument");
     return guard([&] { fdtd::band_levels(device, traces, nrec, nt, fft_m, dt, nband, fc, levels_db); });
 }
+
+int fdtd_save_restart(fdtd_solver* h, const char* path) {
+    if (!h || !path) return bad("null argument");
+    return guard([&] { h->s->save_restart(path); });
+}
+
+int fdtd_load_restart(fdtd_solver* h, const char* path, int reference_semantics) {
+    if (!h || !path) return bad("null argument");
+    return guard([&] { h->s->load_restart(path, reference_semantics != 0); });
+}

@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <fstream>
 #include <cuda_runtime.h>
 
 #include "fdtd_device.cuh"
@@ -122,6 +123,8 @@ class SolverImplBase {
     virtual int get_slab(int s, int comp, double* out, int* dims) = 0;
     virtual size_t state_elems() const = 0;
     virtual void copy_state(int dir, void* host) = 0;
+    virtual void save_restart(const std::string& path) = 0;
+    virtual void load_restart(const std::string& path, bool reference_semantics) = 0;
     virtual long long launch_count() const = 0;
     virtual double last_device_ms() const = 0;
     virtual void set_tiling_api(int TI, int GC, int nt, int vw, int stages) = 0;
@@ -1049,6 +1052,182 @@ class SolverImpl final : public SolverImplBase {
         d2h(out, d_psi_[par_], sizeof(double) * NI_ * Kair_ * 6);
     }
 
+    // ------------------------------------------------------- restart
+    // File layout of one rank of the reference (airpore::Save_restart /
+    // save_restartfile, airpore.cpp:664-796; calculation_2D::save_restart_cal,
+    // calculation_2D.cpp:497-520; air::save_restart_air, air.cpp:1305-1379):
+    //   "size rank index"
+    //   air u v w p per node [i][j][k]
+    //   air wind U V W per node [i][j][k], then the PML integrals Qu Qv Qw Qp
+    //   per node: x1, x2 as [i][j][k], y1, y2 as [j][k][i], z1, z2 as [k][i][j]
+    //   porous u v w p per node [i][j][k] (porous south face only)
+    // each block on one line, scientific, sign shown, 10 digits. This library
+    // appends one block the reference does not write (its reader stops
+    // before it): "B200 1 MF_count temp_time n_in_frame frame_started" and
+    // the TDBC state Psi [i][air k][6], so that a restart is exact for the
+    // moving frame and the TDBC too.
+    void save_restart(const std::string& path) override {
+        FDTD_CK(cudaSetDevice(device_));
+        std::ofstream f(path, std::ios::out | std::ios::trunc | std::ios::binary);
+        if (!f) fail(-1, "cannot write restart file " + path);
+        f << 1 << " " << 0 << " " << steps_ << std::endl;
+        f.setf(std::ios::scientific, std::ios::floatfield);
+        f.setf(std::ios::showpos);
+        f.precision(10);
+        auto section = [&](auto&& body) {
+            f.width(18);  // the reference sets it once per block; it pads the first value only
+            body();
+            f << std::endl;
+        };
+        auto put = [&](double v) { f << v << " "; };
+        const size_t na = static_cast<size_t>(NI_) * NJ_ * Kair_;
+        std::vector<double> fa[4];
+        for (int c = 0; c < 4; ++c) { fa[c].resize(na); get_field(0, c, fa[c].data()); }  // p u v w
+        section([&] {
+            for (size_t n = 0; n < na; ++n) { put(fa[1][n]); put(fa[2][n]); put(fa[3][n]); put(fa[0][n]); }
+        });
+        section([&] {
+            for (int i = 0; i < NI_; ++i)
+                for (int j = 0; j < NJ_; ++j)
+                    for (int k = 0; k < Kair_; ++k) {
+                        double U = 0, V = 0, W = 0;
+                        if (wind_on_) wind_at(in.velocity_method, in.velocity_coef, air_.Y[j], air_.Z[k], U, V, W);
+                        put(U); put(V); put(W);
+                    }
+            for (int sl = 0; sl < 6; ++sl) {
+                if (!slab_n_[sl]) continue;
+                const SlabDesc& S = slab_[sl];
+                std::vector<double> q[4];
+                int dims[3];
+                for (int c = 0; c < 4; ++c) { q[c].resize(slab_n_[sl]); get_slab(sl, c, q[c].data(), dims); }
+                auto node = [&](int a, int b, int c) {
+                    const size_t n = (static_cast<size_t>(a) * S.nj + b) * S.nk + c;
+                    put(q[0][n]); put(q[1][n]); put(q[2][n]); put(q[3][n]);
+                };
+                if (sl < 2) { for (int a = 0; a < S.ni; ++a) for (int b = 0; b < S.nj; ++b) for (int c = 0; c < S.nk; ++c) node(a, b, c); }
+                else if (sl < 4) { for (int b = 0; b < S.nj; ++b) for (int c = 0; c < S.nk; ++c) for (int a = 0; a < S.ni; ++a) node(a, b, c); }
+                else { for (int c = 0; c < S.nk; ++c) for (int a = 0; a < S.ni; ++a) for (int b = 0; b < S.nj; ++b) node(a, b, c); }
+            }
+        });
+        if (porous_) {
+            const size_t np = static_cast<size_t>(NI_) * NJ_ * pore_.K;
+            std::vector<double> fp[4];
+            for (int c = 0; c < 4; ++c) { fp[c].resize(np); get_field(1, c, fp[c].data()); }
+            section([&] {
+                for (size_t n = 0; n < np; ++n) { put(fp[1][n]); put(fp[2][n]); put(fp[3][n]); put(fp[0][n]); }
+            });
+        }
+        f.unsetf(std::ios::showpos);
+        f << "B200 1 " << mf_count_ << " " << temp_time_ << " " << n_in_frame_ << " " << (frame_started_ ? 1 : 0)
+          << std::endl;
+        f.setf(std::ios::showpos);
+        std::vector<double> psi(static_cast<size_t>(NI_) * Kair_ * 6);
+        get_psi(psi.data());
+        section([&] { for (double v : psi) put(v); });
+        if (!f) fail(-1, "writing restart file " + path + " failed");
+    }
+
+    // Reads a restart file of the layout above (reference files included:
+    // without this library's block the TDBC state starts at zero and the run
+    // continues in frame 0) and makes it the current state; the next step is
+    // step `index`. reference_semantics: continue as airpore::get_output does
+    // after Read_restart (airpore.cpp:499-571) -- its frame loop then starts
+    // frame 0 with air::SetQMove(0), which zeroes every PML integral
+    // (air.cpp:2453-2517), and the TDBC state is not in its files -- so the
+    // integrals and Psi restart from zero in frame 0.
+    void load_restart(const std::string& path, bool reference_semantics) override {
+        FDTD_CK(cudaSetDevice(device_));
+        std::ifstream f(path, std::ios::in | std::ios::binary);
+        if (!f) fail(-1, "cannot read restart file " + path);
+        int size = 0, rank = 0, index = 0;
+        f >> size >> rank >> index;
+        if (!f) fail(-1, "restart file " + path + ": bad header");
+        if (size != 1) fail(-2, "restart files of a multi-rank run (one file per rank) are not supported");
+        if (index < 0 || index >= horizon_) fail(-6, "restart step outside the horizon set by reset()");
+        auto get = [&](double& v) {
+            if (!(f >> v)) fail(-1, "restart file " + path + ": truncated");
+        };
+        const size_t na = static_cast<size_t>(NI_) * NJ_ * Kair_;
+        std::vector<double> fa[4];
+        for (auto& v : fa) v.resize(na);
+        for (size_t n = 0; n < na; ++n) { get(fa[1][n]); get(fa[2][n]); get(fa[3][n]); get(fa[0][n]); }
+        double skip;
+        for (size_t n = 0; n < 3 * na; ++n) get(skip);  // wind: recomputed from input.txt for the frame
+        std::vector<double> q[6][4];
+        for (int sl = 0; sl < 6; ++sl) {
+            if (!slab_n_[sl]) continue;
+            const SlabDesc& S = slab_[sl];
+            for (auto& v : q[sl]) v.assign(static_cast<size_t>(S.ni) * S.nj * S.nk, 0.0);
+            auto node = [&](int a, int b, int c) {
+                const size_t n = (static_cast<size_t>(a) * S.nj + b) * S.nk + c;
+                get(q[sl][0][n]); get(q[sl][1][n]); get(q[sl][2][n]); get(q[sl][3][n]);
+            };
+            if (sl < 2) { for (int a = 0; a < S.ni; ++a) for (int b = 0; b < S.nj; ++b) for (int c = 0; c < S.nk; ++c) node(a, b, c); }
+            else if (sl < 4) { for (int b = 0; b < S.nj; ++b) for (int c = 0; c < S.nk; ++c) for (int a = 0; a < S.ni; ++a) node(a, b, c); }
+            else { for (int c = 0; c < S.nk; ++c) for (int a = 0; a < S.ni; ++a) for (int b = 0; b < S.nj; ++b) node(a, b, c); }
+        }
+        std::vector<double> fp[4];
+        if (porous_) {
+            const size_t np = static_cast<size_t>(NI_) * NJ_ * pore_.K;
+            for (auto& v : fp) v.resize(np);
+            for (size_t n = 0; n < np; ++n) { get(fp[1][n]); get(fp[2][n]); get(fp[3][n]); get(fp[0][n]); }
+        }
+        int mf = 0, tt = 0, nin = index, started = 1;
+        std::vector<double> psi(static_cast<size_t>(NI_) * Kair_ * 6, 0.0);
+        if (reference_semantics && mf_.Judge == 1) fail(-2, "the reference's restart cannot resume a moving frame");
+        std::string tag;
+        if (f >> tag) {
+            int version = 0;
+            if (tag != "B200" || !(f >> version >> mf >> tt >> nin >> started) || version != 1)
+                fail(-1, "restart file " + path + ": unknown trailing block");
+            for (double& v : psi) get(v);
+        } else if (mf_.Judge == 1 && !reference_semantics) {
+            fail(-1, "restart file " + path + " lacks the frame count a moving-frame run needs");
+        }
+        if (reference_semantics) {
+            mf = 0; tt = 0; nin = index; started = 1;
+            std::fill(psi.begin(), psi.end(), 0.0);
+            for (auto& sq : q)
+                for (auto& v : sq) std::fill(v.begin(), v.end(), 0.0);
+        }
+        // the state becomes time level 0 of step `index`
+        FDTD_CK(cudaStreamSynchronize(stream_));
+        par_ = 0;
+        for (int lvl = 0; lvl < 2; ++lvl)
+            for (int c = 0; c < 4; ++c) zero(F_[lvl][c], nodes_ * sizeof(R));
+        if (porous_)
+            for (int c = 0; c < 4; ++c) set_field(1, c, fp[c].data());
+        for (int c = 0; c < 4; ++c) set_field(0, c, fa[c].data());
+        for (int sl = 0; sl < 6; ++sl) {
+            if (!slab_n_[sl]) continue;
+            const SlabDesc& S = slab_[sl];
+            for (int c = 0; c < 4; ++c) {
+                std::vector<R> h(slab_n_[sl], R(0));
+                for (int a = 0; a < S.ni; ++a)
+                    for (int b = 0; b < S.nj; ++b)
+                        for (int cc = 0; cc < S.nk; ++cc)
+                            h[(static_cast<size_t>(cc) * S.ni + a) * S.jp + (b + S.j0 - S.ja)] =
+                                static_cast<R>(q[sl][c][(static_cast<size_t>(a) * S.nj + b) * S.nk + cc]);
+                h2d(Q_[sl][0][c], h.data(), slab_n_[sl] * sizeof(R));
+                zero(Q_[sl][1][c], slab_n_[sl] * sizeof(R));
+            }
+        }
+        h2d(d_psi_[0], psi.data(), psi.size() * sizeof(double));
+        zero(d_psi_[1], psi.size() * sizeof(double));
+        const int counters[2] = {index, index};
+        h2d(d_counters_, counters, sizeof counters);
+        zero(d_status_, sizeof(int));
+        steps_ = index;
+        mf_count_ = mf;
+        temp_time_ = tt;
+        n_in_frame_ = nin;
+        frame_started_ = started != 0;
+        done_ = false;
+        upload_frame(mf_count_);
+        if (frame_started_) mf_limit_ = frame_limit();
+        FDTD_CK(cudaStreamSynchronize(stream_));
+    }
+
     int get_slab(int s, int comp, double* out, int* dims) override {
         if (s < 0 || s > 5 || comp < 0 || comp > 3) fail(-5, "slab 0..5, comp 0..3");
         if (!slab_n_[s]) { dims[0] = dims[1] = dims[2] = 0; return 0; }
@@ -1235,6 +1414,10 @@ size_t Solver::state_elems() const { return impl_->state_elems(); }
 void Solver::copy_state(int dir, void* host) { impl_->copy_state(dir, host); }
 long long Solver::launch_count() const { return impl_->launch_count(); }
 void Solver::set_tiling(int TI, int GC, int nt, int vw, int stages) { impl_->set_tiling_api(TI, GC, nt, vw, stages); }
+void Solver::save_restart(const std::string& path) { impl_->save_restart(path); }
+void Solver::load_restart(const std::string& path, bool reference_semantics) {
+    impl_->load_restart(path, reference_semantics);
+}
 std::array<int, 5> Solver::autotune(int nsteps) { return impl_->autotune(nsteps); }
 double Solver::last_device_ms() const { return impl_->last_device_ms(); }
 

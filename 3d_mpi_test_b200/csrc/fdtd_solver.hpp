@@ -58,6 +58,8 @@ class Solver {
     int get_slab(int s, int comp, double* out, int* dims);
     size_t state_elems() const;
     void copy_state(int dir, void* host);
+    void save_restart(const std::string& path);
+    void load_restart(const std::string& path, bool reference_semantics);
     long long launch_count() const;
     void set_tiling(int rows_per_block, int planes_per_block, int threads_per_block, int vector_width,
                     int ring_stages);

@@ -131,6 +131,26 @@ long long fdtd_launch_count(const fdtd_solver *h);
 /* CUDA events around the last fdtd_advance's device work: milliseconds. */
 int fdtd_last_device_ms(const fdtd_solver *h, double *ms);
 
+/* Restart files (airpore::Save_restart / Read_restart, airpore.cpp:664-879;
+ * calculation_2D::save/input_restart_cal, calculation_2D.cpp:497-545;
+ * air::save/input_restart_air, air.cpp:1305-1474). fdtd_save_restart writes
+ * the current state in the reference's single-rank text layout (header
+ * "size rank index", then air fields, wind and PML integrals, porous fields)
+ * followed by one block the reference does not write -- the moving-frame
+ * counters and the TDBC state Psi -- so the restart is exact for those too;
+ * the reference's reader ignores it. fdtd_load_restart reads such a file,
+ * or a file written by the reference itself (no extra block: Psi starts at
+ * zero and the run continues in frame 0, as the reference's restart does),
+ * into a handle created for the same case; the index must lie below the
+ * horizon of the last fdtd_reset. Values carry 11 significant digits.
+ * reference_semantics = 1 continues exactly as the reference does after its
+ * Read_restart: its frame loop restarts frame 0 with air::SetQMove(0), which
+ * zeroes all PML integrals (air.cpp:2453-2517), and it has no TDBC state in
+ * the file -- so those start from zero (no moving frame). 0 keeps every
+ * value the file holds (an exact restart for files of this library). */
+int fdtd_save_restart(fdtd_solver *h, const char *path);
+int fdtd_load_restart(fdtd_solver *h, const char *path, int reference_semantics);
+
 /* Receiver post-processing (replaces airpore::get_FFT_y1, airpore.cpp:966-1011,
  * with FFT / FFT_output, FFT.cpp:15-120). traces: host [nrec][nt] pressure
  * histories (fdtd_run output); each is zero-padded (or cut) to 2^fft_m

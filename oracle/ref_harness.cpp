@@ -19,6 +19,17 @@
  *   --steps overrides input.txt's time_domain (airpore.cpp:171).
  *   --receivers: text file, one "X Y Z" per line (reference axes).
  *   --time: no dump; prints one JSON line with ms per step.
+ *   --restart-out FILE: after the run, write the reference's restart file
+ *     (the header line of airpore::Save_restart, airpore.cpp:686-689, then
+ *     airpore::save_restartfile, airpore.cpp:782-796) for the step reached.
+ *   --restart-in FILE: before the run, load a restart file with the
+ *     reference's airpore::input_restartfile (airpore.cpp:798-863, the
+ *     timer as in get_output, airpore.cpp:499-504); the run then takes
+ *     --steps further steps. Only without a moving frame (the reference does
+ *     not store the frame count). The reference passes its short restart
+ *     name to the porous reader (airpore.cpp:869) and keeps names in
+ *     char[20]; here both readers get a copy named rs_in.dat in the case
+ *     directory.
  */
 #include <chrono>
 #include <cmath>
@@ -96,7 +107,7 @@ int main(int argc, char **argv)
         std::fprintf(stderr, "usage: %s case_dir [--steps N] [--receivers F] [--out F] [--time W K]\n", argv[0]);
         return 2;
     }
-    std::string case_dir = argv[1], rec_file, out_file = "ref_out.bin";
+    std::string case_dir = argv[1], rec_file, out_file = "ref_out.bin", restart_out, restart_in;
     long steps_override = -1;
     int time_w = -1, time_k = -1;
     for (int a = 2; a < argc; ++a) {
@@ -105,6 +116,8 @@ int main(int argc, char **argv)
         else if (s == "--receivers" && a + 1 < argc) rec_file = argv[++a];
         else if (s == "--out" && a + 1 < argc) out_file = argv[++a];
         else if (s == "--time" && a + 2 < argc) { time_w = std::atoi(argv[++a]); time_k = std::atoi(argv[++a]); }
+        else if (s == "--restart-out" && a + 1 < argc) restart_out = argv[++a];
+        else if (s == "--restart-in" && a + 1 < argc) restart_in = argv[++a];
         else { std::fprintf(stderr, "bad argument %s\n", s.c_str()); return 2; }
     }
     /* Resolve output/receiver paths before changing directory. */
@@ -116,6 +129,8 @@ int main(int argc, char **argv)
     };
     rec_file = absolutize(rec_file);
     out_file = absolutize(out_file);
+    restart_out = absolutize(restart_out);
+    restart_in = absolutize(restart_in);
 
     std::vector<Rec> recs;
     if (!rec_file.empty()) {
@@ -148,6 +163,28 @@ int main(int argc, char **argv)
         if (ii == 0 && jj == 0 && kk == 0) { ii = 1; jj = 1; kk = 1; }
         if (ii > IMAXw || jj > JMAXw || kk > KMAXw) { ii = 1; jj = 1; kk = 1; }
         r.i = ii; r.j = jj; r.k = kk;
+    }
+
+    int restart_index = 0;
+    if (!restart_in.empty()) {
+        if (ap->move_frame.Judge == 1) { std::fprintf(stderr, "--restart-in needs a case without moving frame\n"); return 2; }
+        std::ifstream hin(restart_in, std::ios::in | std::ios::binary);
+        int re_size = 0, re_rank = 0;
+        hin >> re_size >> re_rank >> restart_index;
+        hin.ignore(100, '\n');
+        int pos = (int)hin.tellg();
+        hin.close();
+        // the reference keeps the name in char[20] (airpore.h:30): read a copy
+        // under a short name in the case directory (the working directory)
+        {
+            std::ifstream src(restart_in, std::ios::binary);
+            std::ofstream dst("rs_in.dat", std::ios::binary | std::ios::trunc);
+            dst << src.rdbuf();
+        }
+        std::snprintf(ap->restart_infile1, sizeof ap->restart_infile1, "%s", "rs_in.dat");
+        std::snprintf(ap->restart_infile, sizeof ap->restart_infile, "%s", "rs_in.dat");
+        ap->input_restartfile(&pos);
+        A->Set_Timer(restart_index);
     }
 
     const int time_domain = ap->time_domain;
@@ -196,6 +233,14 @@ int main(int argc, char **argv)
     } while ((MF_count <= (int)((JMAX - mf.JMAX) / (mf.lead_DJ - 1) + 1.e-6)) && (temp_time < time_domain) &&
              mf.Judge == 1);
     t_end = std::chrono::steady_clock::now();
+    if (!restart_out.empty()) {
+        std::ofstream hout(restart_out, std::ios::out | std::ios::trunc | std::ios::binary);
+        hout << ap->mpi_size << " " << ap->mpi_rank << " " << restart_index + index_pressure << std::endl;
+        hout.close();
+        std::vector<char> name(restart_out.begin(), restart_out.end());
+        name.push_back('\0');
+        ap->save_restartfile(name.data());
+    }
     std::cout.rdbuf(old_cout);
 
     if (time_w >= 0) {
