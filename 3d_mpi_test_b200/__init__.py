@@ -37,6 +37,7 @@ EXPORTS = (
     "fdtd_set_field", "fdtd_get_psi", "fdtd_get_slab", "fdtd_state_elems", "fdtd_copy_state",
     "fdtd_launch_count", "fdtd_last_device_ms", "fdtd_fb_step_noalloc", "fdtd_set_tiling", "fdtd_autotune",
     "fdtd_fft", "fdtd_spectrum", "fdtd_band_levels", "fdtd_save_restart", "fdtd_load_restart",
+    "fdtd_write_contour",
 )
 
 
@@ -87,6 +88,7 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
         "fdtd_band_levels": ([i, dp, i, i, i, ctypes.c_double, i, dp, dp], i),
         "fdtd_save_restart": ([vp, cp], i),
         "fdtd_load_restart": ([vp, cp, i], i),
+        "fdtd_write_contour": ([vp, cp, i], i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -216,6 +218,12 @@ class Airpore:
 
     def copy_state(self, host: np.ndarray, to_device: bool) -> None:
         self._check(self._L.fdtd_copy_state(self._h, 1 if to_device else 0, host.ctypes.data_as(ctypes.c_void_p)))
+
+    def get_data_contour(self, path: str, binary: bool = False) -> None:
+        """airpore::get_data_contour: the pressure contour of the current state
+        (every 4th node plus the last) as the reference's Tecplot file, or
+        the binary variant."""
+        self._check(self._L.fdtd_write_contour(self._h, os.fsencode(path), 1 if binary else 0))
 
     def Save_restart(self, path: str) -> None:
         """airpore::Save_restart: the state in the reference's restart layout

@@ -190,3 +190,8 @@ int fdtd_load_restart(fdtd_solver* h, const char* path, int reference_semantics)
     if (!h || !path) return bad("null argument");
     return guard([&] { h->s->load_restart(path, reference_semantics != 0); });
 }
+
+int fdtd_write_contour(fdtd_solver* h, const char* path, int format) {
+    if (!h || !path) return bad("null argument");
+    return guard([&] { h->s->write_contour(path, format); });
+}

@@ -124,6 +124,7 @@ class SolverImplBase {
     virtual size_t state_elems() const = 0;
     virtual void copy_state(int dir, void* host) = 0;
     virtual void save_restart(const std::string& path) = 0;
+    virtual void write_contour(const std::string& path, int format) = 0;
     virtual void load_restart(const std::string& path, bool reference_semantics) = 0;
     virtual long long launch_count() const = 0;
     virtual double last_device_ms() const = 0;
@@ -1052,6 +1053,76 @@ class SolverImpl final : public SolverImplBase {
         d2h(out, d_psi_[par_], sizeof(double) * NI_ * Kair_ * 6);
     }
 
+    // ------------------------------------------------------- contour
+    // Pressure contour of the current state, airpore::get_data_contour
+    // (airpore.cpp:1014-1056) with calculation_2D::mpi_send_data and
+    // operator<< (calculation_2D.cpp:1030-1190): every 4th node along each
+    // axis plus the last one, X Y Z P per line with k outermost and i
+    // innermost, scientific with 6 digits, Y shifted to the current frame;
+    // a second zone for the porous ground. format 0 writes that Tecplot ASCII
+    // file; format 1 a binary file: "FDTDCNT1", int32 zone count, then per
+    // zone int32 I J K and float64 X[I], Y[J], Z[K], P[K][J][I].
+    void write_contour(const std::string& path, int format) override {
+        FDTD_CK(cudaSetDevice(device_));
+        if (format != 0 && format != 1) fail(-5, "contour format must be 0 (Tecplot ASCII) or 1 (binary)");
+        struct Zone {
+            std::string title;
+            std::vector<double> x, y, z, p;  // p [k][j][i] over the kept nodes
+        };
+        auto keep = [](int n) {
+            std::vector<int> idx;
+            for (int q = 0; q < n; ++q)
+                if (q % 4 == 0 || q == n - 1) idx.push_back(q);
+            return idx;
+        };
+        auto zone = [&](int medium, const Medium& m, const char* title) {
+            int I, J, K, g0;
+            medium_dims(medium, I, J, K, g0);
+            std::vector<double> f(static_cast<size_t>(I) * J * K);
+            get_field(medium, 0, f.data());
+            Zone z;
+            z.title = title;
+            const std::vector<int> ki = keep(I), kj = keep(J), kk = keep(K);
+            for (int i : ki) z.x.push_back(m.X[i]);
+            for (int j : kj) z.y.push_back(m.Y[j]);
+            for (int k : kk) z.z.push_back(m.Z[k]);
+            for (int k : kk)
+                for (int j : kj)
+                    for (int i : ki) z.p.push_back(f[(static_cast<size_t>(i) * J + j) * K + k]);
+            return z;
+        };
+        std::vector<Zone> zones;
+        zones.push_back(zone(0, air_, "Air Zone"));
+        if (porous_) zones.push_back(zone(1, pore_, "south pore Zone"));
+        std::ofstream f(path, std::ios::out | std::ios::trunc | std::ios::binary);
+        if (!f) fail(-1, "cannot write contour file " + path);
+        if (format == 0) {
+            f.setf(std::ios::scientific, std::ios::floatfield);
+            f.precision(6);
+            if (!porous_) f << "VARIABLES = \"X\", \"Y\", \"Z\", \"P\"" << std::endl;
+            for (const Zone& z : zones) {
+                f << "ZONE T = \"" << z.title << "\",";
+                f << "I=" << z.x.size() << ",J=" << z.y.size() << ",K=" << z.z.size() << ",F=POINT" << std::endl;
+                size_t n = 0;
+                for (double zz : z.z)
+                    for (double yy : z.y)
+                        for (double xx : z.x) f << xx << " " << yy << " " << zz << " " << z.p[n++] << " " << std::endl;
+            }
+        } else {
+            f.write("FDTDCNT1", 8);
+            const int32_t nz = static_cast<int32_t>(zones.size());
+            f.write(reinterpret_cast<const char*>(&nz), 4);
+            for (const Zone& z : zones) {
+                const int32_t d[3] = {static_cast<int32_t>(z.x.size()), static_cast<int32_t>(z.y.size()),
+                                      static_cast<int32_t>(z.z.size())};
+                f.write(reinterpret_cast<const char*>(d), sizeof d);
+                for (const auto* v : {&z.x, &z.y, &z.z, &z.p})
+                    f.write(reinterpret_cast<const char*>(v->data()), static_cast<std::streamsize>(v->size() * 8));
+            }
+        }
+        if (!f) fail(-1, "writing contour file " + path + " failed");
+    }
+
     // ------------------------------------------------------- restart
     // File layout of one rank of the reference (airpore::Save_restart /
     // save_restartfile, airpore.cpp:664-796; calculation_2D::save_restart_cal,
@@ -1414,6 +1485,7 @@ size_t Solver::state_elems() const { return impl_->state_elems(); }
 void Solver::copy_state(int dir, void* host) { impl_->copy_state(dir, host); }
 long long Solver::launch_count() const { return impl_->launch_count(); }
 void Solver::set_tiling(int TI, int GC, int nt, int vw, int stages) { impl_->set_tiling_api(TI, GC, nt, vw, stages); }
+void Solver::write_contour(const std::string& path, int format) { impl_->write_contour(path, format); }
 void Solver::save_restart(const std::string& path) { impl_->save_restart(path); }
 void Solver::load_restart(const std::string& path, bool reference_semantics) {
     impl_->load_restart(path, reference_semantics);

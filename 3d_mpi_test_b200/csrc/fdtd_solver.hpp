@@ -59,6 +59,7 @@ class Solver {
     size_t state_elems() const;
     void copy_state(int dir, void* host);
     void save_restart(const std::string& path);
+    void write_contour(const std::string& path, int format);
     void load_restart(const std::string& path, bool reference_semantics);
     long long launch_count() const;
     void set_tiling(int rows_per_block, int planes_per_block, int threads_per_block, int vector_width,

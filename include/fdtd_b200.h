@@ -131,6 +131,16 @@ long long fdtd_launch_count(const fdtd_solver *h);
 /* CUDA events around the last fdtd_advance's device work: milliseconds. */
 int fdtd_last_device_ms(const fdtd_solver *h, double *ms);
 
+/* Pressure contour of the current state (airpore::get_data_contour,
+ * airpore.cpp:1014-1056; calculation_2D::mpi_send_data and operator<<,
+ * calculation_2D.cpp:1030-1190) to `path` instead of the reference's
+ * hard-coded cluster path: every 4th node along each axis plus the last,
+ * Y of the current moving frame, the porous ground as a second zone.
+ * format 0: the reference's Tecplot ASCII POINT file, byte for byte;
+ * 1: binary -- "FDTDCNT1", int32 zones, per zone int32 I J K then float64
+ * X[I], Y[J], Z[K], P[K][J][I]. */
+int fdtd_write_contour(fdtd_solver *h, const char *path, int format);
+
 /* Restart files (airpore::Save_restart / Read_restart, airpore.cpp:664-879;
  * calculation_2D::save/input_restart_cal, calculation_2D.cpp:497-545;
  * air::save/input_restart_air, air.cpp:1305-1474). fdtd_save_restart writes

@@ -22,6 +22,10 @@
  *   --restart-out FILE: after the run, write the reference's restart file
  *     (the header line of airpore::Save_restart, airpore.cpp:686-689, then
  *     airpore::save_restartfile, airpore.cpp:782-796) for the step reached.
+ *   --contour-out FILE: after the run, the pressure contour of the last step
+ *     as airpore::get_data_contour writes it (airpore.cpp:1014-1056, with the
+ *     reference's own operator<<, calculation_2D.cpp:1171-1190), to FILE
+ *     instead of its hard-coded cluster path.
  *   --restart-in FILE: before the run, load a restart file with the
  *     reference's airpore::input_restartfile (airpore.cpp:798-863, the
  *     timer as in get_output, airpore.cpp:499-504); the run then takes
@@ -107,7 +111,7 @@ int main(int argc, char **argv)
         std::fprintf(stderr, "usage: %s case_dir [--steps N] [--receivers F] [--out F] [--time W K]\n", argv[0]);
         return 2;
     }
-    std::string case_dir = argv[1], rec_file, out_file = "ref_out.bin", restart_out, restart_in;
+    std::string case_dir = argv[1], rec_file, out_file = "ref_out.bin", restart_out, restart_in, contour_out;
     long steps_override = -1;
     int time_w = -1, time_k = -1;
     for (int a = 2; a < argc; ++a) {
@@ -118,6 +122,7 @@ int main(int argc, char **argv)
         else if (s == "--time" && a + 2 < argc) { time_w = std::atoi(argv[++a]); time_k = std::atoi(argv[++a]); }
         else if (s == "--restart-out" && a + 1 < argc) restart_out = argv[++a];
         else if (s == "--restart-in" && a + 1 < argc) restart_in = argv[++a];
+        else if (s == "--contour-out" && a + 1 < argc) contour_out = argv[++a];
         else { std::fprintf(stderr, "bad argument %s\n", s.c_str()); return 2; }
     }
     /* Resolve output/receiver paths before changing directory. */
@@ -131,6 +136,7 @@ int main(int argc, char **argv)
     out_file = absolutize(out_file);
     restart_out = absolutize(restart_out);
     restart_in = absolutize(restart_in);
+    contour_out = absolutize(contour_out);
 
     std::vector<Rec> recs;
     if (!rec_file.empty()) {
@@ -233,6 +239,22 @@ int main(int argc, char **argv)
     } while ((MF_count <= (int)((JMAX - mf.JMAX) / (mf.lead_DJ - 1) + 1.e-6)) && (temp_time < time_domain) &&
              mf.Judge == 1);
     t_end = std::chrono::steady_clock::now();
+    if (!contour_out.empty()) {
+        ap->mpisend_data_contour(MF_count > 0 ? MF_count - 1 : 0);
+        std::ofstream fp_p_t(contour_out, std::ios::out | std::ios::trunc | std::ios::binary);
+        fp_p_t.setf(std::ios::scientific, std::ios::floatfield);
+        fp_p_t.precision(6);
+        if (ap->air_boundary.air_south == rigid || ap->air_boundary.air_south == absorbing) {
+            fp_p_t << "VARIABLES = \"X\", \"Y\", \"Z\", \"P\"" << std::endl;
+            fp_p_t << "ZONE T = \"Air Zone\",";
+            fp_p_t << *ap->AirMedia;
+        } else {
+            fp_p_t << "ZONE T = \"Air Zone\",";
+            fp_p_t << *ap->AirMedia;
+            fp_p_t << "ZONE T = \"south pore Zone\",";
+            fp_p_t << *ap->south_pore;
+        }
+    }
     if (!restart_out.empty()) {
         std::ofstream hout(restart_out, std::ios::out | std::ios::trunc | std::ios::binary);
         hout << ap->mpi_size << " " << ap->mpi_rank << " " << restart_index + index_pressure << std::endl;
