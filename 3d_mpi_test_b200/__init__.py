@@ -28,6 +28,7 @@ FDTD_ERR_CUDA = -3
 FDTD_ERR_NONFINITE = -4
 FDTD_ERR_ARG = -5
 FDTD_ERR_STATE = -6
+FDTD_ERR_TIMEOUT = -7
 F64, F32 = 0, 1
 
 # Every function declared in include/fdtd_b200.h.
@@ -37,7 +38,9 @@ EXPORTS = (
     "fdtd_set_field", "fdtd_get_psi", "fdtd_get_slab", "fdtd_state_elems", "fdtd_copy_state",
     "fdtd_launch_count", "fdtd_last_device_ms", "fdtd_fb_step_noalloc", "fdtd_set_tiling", "fdtd_autotune",
     "fdtd_fft", "fdtd_spectrum", "fdtd_band_levels", "fdtd_save_restart", "fdtd_load_restart",
-    "fdtd_write_contour",
+    "fdtd_write_contour", "fdtd_get_receivers", "fdtd_set_wait_limit", "fdtd_ensemble_create",
+    "fdtd_ensemble_destroy", "fdtd_ensemble_advance", "fdtd_ensemble_autotune", "fdtd_ensemble_info",
+    "fdtd_ensemble_last_device_ms",
 )
 
 
@@ -89,6 +92,14 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
         "fdtd_save_restart": ([vp, cp], i),
         "fdtd_load_restart": ([vp, cp, i], i),
         "fdtd_write_contour": ([vp, cp, i], i),
+        "fdtd_get_receivers": ([vp, i, i, dp], i),
+        "fdtd_set_wait_limit": ([vp, ctypes.c_longlong], i),
+        "fdtd_ensemble_create": ([ctypes.POINTER(vp), i, ctypes.POINTER(vp)], i),
+        "fdtd_ensemble_destroy": ([vp], i),
+        "fdtd_ensemble_advance": ([vp, i, ip], i),
+        "fdtd_ensemble_autotune": ([vp, i, ip], i),
+        "fdtd_ensemble_info": ([vp, ctypes.POINTER(ctypes.c_longlong)], i),
+        "fdtd_ensemble_last_device_ms": ([vp, dp], i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -257,6 +268,80 @@ class Airpore:
     def last_device_ms(self) -> float:
         v = ctypes.c_double()
         self._check(self._L.fdtd_last_device_ms(self._h, ctypes.byref(v)))
+        return v.value
+
+    def receivers(self, first_step: int, nsteps: int) -> np.ndarray:
+        """Receiver pressure of steps [first_step, first_step + nsteps) already
+        taken (by ``advance`` or an :class:`Ensemble`): [nsteps][nrec]."""
+        out = np.zeros((nsteps, max(self.nrec, 1)))
+        self._check(self._L.fdtd_get_receivers(self._h, first_step, nsteps, _dp(out)))
+        return out[:, : self.nrec]
+
+    def set_wait_limit(self, polls: int) -> None:
+        """Polls a staged-copy wait of the marching kernel makes before the
+        step reports FDTD_ERR_TIMEOUT (0: at the first wait; < 0: default)."""
+        self._check(self._L.fdtd_set_wait_limit(self._h, polls))
+
+
+class Ensemble:
+    """Independent :class:`Airpore` solves of one precision on one device
+    stepped together: one batched marching launch per group of members per
+    step, the time loop in a CUDA graph. Members keep their own receivers,
+    horizon (``reset``) and read-out, and must stay open while the ensemble
+    is used."""
+
+    def __init__(self, members: Sequence[Airpore], lib_path: Optional[str] = None):
+        if not members:
+            raise FdtdError(FDTD_ERR_ARG, "an ensemble needs at least one member")
+        self._L = members[0]._L if lib_path is None else load_library(lib_path)
+        self.members = list(members)
+        arr = (ctypes.c_void_p * len(members))(*[m._h.value for m in members])
+        self._h = ctypes.c_void_p()
+        self._check(self._L.fdtd_ensemble_create(arr, len(members), ctypes.byref(self._h)))
+
+    def _check(self, rc: int) -> None:
+        if rc < 0:
+            raise FdtdError(rc, self._L.fdtd_last_error().decode())
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            self._L.fdtd_ensemble_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def advance(self, nsteps: int) -> int:
+        """Lock-step steps of every member; returns the steps taken (bounded by
+        the nearest member horizon)."""
+        n = ctypes.c_int()
+        self._check(self._L.fdtd_ensemble_advance(self._h, nsteps, ctypes.byref(n)))
+        return n.value
+
+    def autotune(self, nsteps: int = 10) -> Tuple[int, int]:
+        """One tile rule (rows, planes per block) for all members, timed on the
+        whole ensemble; members end reset to t = 0."""
+        best = (ctypes.c_int * 2)()
+        self._check(self._L.fdtd_ensemble_autotune(self._h, nsteps, best))
+        return best[0], best[1]
+
+    def info(self) -> dict:
+        v = (ctypes.c_longlong * 3)()
+        self._check(self._L.fdtd_ensemble_info(self._h, v))
+        return {"launches": v[0], "groups": v[1], "blocks_per_step": v[2]}
+
+    def last_device_ms(self) -> float:
+        v = ctypes.c_double()
+        self._check(self._L.fdtd_ensemble_last_device_ms(self._h, ctypes.byref(v)))
         return v.value
 
 

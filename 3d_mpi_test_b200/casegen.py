@@ -260,3 +260,91 @@ def porous_ground(ni=128, nj=256, nk=96, layer=16, d=0.05, steps=4000, pml=20, s
         pore_Z=pore_Z, pore_dxyz=(d, d, d),
     )
     return case, receivers
+
+
+ENSEMBLE_SIZES = ((64, 512), (32, 192), (32, 96))  # NJ, NK, 3D NI: inclusive ranges
+
+
+def ensemble_member(seed: int, index: int, d: float = 0.1, pml: int = 10, layer: int = 8, steps: int = 100,
+                    n_receivers: int = 8, sizes=ENSEMBLE_SIZES):
+    """Member ``index`` of the seeded batched-ensemble workload: one
+    independent outdoor-sound solve whose size and physics are drawn from
+    ``numpy.random.default_rng([seed, index])``:
+
+    - range NJ uniform in [64, 512] nodes, height NK uniform in [32, 192];
+      the transverse axis is NI = 3 for even ``index`` -- a 2D (y-z) solve:
+      Front/Back rigid and no x PML, so the single interior row i = 1 is
+      exactly two-dimensional (calculation_2D.cpp:835-860) -- and uniform in
+      [32, 96] with x PML otherwise;
+    - porous Zwikker-Kosten ground ``layer`` cells deep: flow resistivity
+      log-uniform in 1e4..2e6 Pa s/m^2, porosity uniform in 0.2..0.6,
+      tortuosity uniform in 1..2.5 (input line 13 holds its square root);
+    - source height uniform in 0.1..3 m (kept below the top PML), source
+      10 cells past the west PML;
+    - a porous hill: a half sphere of height uniform in 0..2 m on the
+      ground half way down the range, made with the reference's sphere
+      inclusion (curve_judge 1, air.cpp:1019-1031) and its canopy
+      parameters; heights under two cells leave it out;
+    - logarithmic wind V(z) = b ln(z / 0.1 + 1) (velocity_method 5,
+      air.cpp:175-177) with b = u* / 0.4 and u* uniform in 0..0.6 m/s.
+
+    Uniform spacing ``d``, PML of ``pml`` nodes on every air face but the
+    ground, CFL 0.5. ``sizes`` replaces the three node-count ranges (small
+    members for tests). Receivers: ``n_receivers`` on a line at 1.2 m height
+    (lower in short domains) from 1 m past the source to the east PML.
+    Returns (Case, receivers, params) with the drawn parameters."""
+    import numpy as np
+
+    rng = np.random.default_rng([seed, index])
+    (j0, j1), (k0, k1), (i0, i1) = sizes
+    nj = int(rng.integers(j0, j1 + 1))
+    nk = int(rng.integers(k0, k1 + 1))
+    two_d = index % 2 == 0
+    ni = 3 if two_d else int(rng.integers(i0, i1 + 1))
+    sigma = float(10.0 ** rng.uniform(4.0, math.log10(2.0e6)))
+    porosity = float(rng.uniform(0.2, 0.6))
+    tortuosity = float(rng.uniform(1.0, 2.5))
+    src_h = float(rng.uniform(0.1, 3.0))
+    hill_h = float(rng.uniform(0.0, 2.0))
+    ustar = float(rng.uniform(0.0, 0.6))
+
+    c0, rho0, gamma = 343.0, 1.2, 1.4
+    P0 = rho0 * c0 * c0 / gamma
+    X = uniform_axis(ni, 0.0, d)
+    Y = uniform_axis(nj, 0.0, d)
+    Z = uniform_axis(nk, 0.0, d)
+    top = (nk - pml - 3) * d  # highest height clear of the top PML
+    src_h = round(min(src_h, top), 6)
+    xc = round(X[ni // 2], 9)  # short text: input.txt lines hold under 100 characters
+    src = (xc, round(Y[pml + 10], 9), src_h)
+    if two_d:
+        bc = (PML, POROUS, PML, PML, RIGID, RIGID)
+        pml_nodes = (0, 0, pml, pml, 0, pml)
+    else:
+        bc = (PML, POROUS, PML, PML, PML, PML)
+        pml_nodes = (pml, pml, pml, pml, 0, pml)
+    rec_h = round(min(1.2, top), 9)
+    y0, y1 = src[1] + 1.0, Y[nj - pml - 2]
+    y0 = min(y0, y1)
+    receivers = [(xc, round(y0 + r * (y1 - y0) / max(n_receivers - 1, 1), 9), rec_h) for r in range(n_receivers)]
+    case = Case(
+        X=X, Y=Y, Z=Z, pml_nodes=pml_nodes, gauss_width=6 * d, bc=bc, time_domain=steps,
+        gamma=gamma, P0=P0, c0=c0, pml_y=(2.0, 1000.0, 0),
+        pore=(math.sqrt(tortuosity), porosity, sigma), source=src, receiver=receivers[0],
+        dt=0.5 * d / c0, velocity_coef=ustar / 0.4, velocity_method=5,
+        pore_Z=uniform_axis(layer + 2, -layer * d, d), pore_dxyz=(d, d, d),
+    )
+    # hill: nodes of its bounding box, snapped to the grid, below the top PML
+    r_cells = int(round(hill_h / d))
+    r_cells = min(r_cells, nk - pml - 4, (nj - 2 * pml) // 4)
+    if r_cells >= 2:
+        jc = (pml + 10 + nj - pml - 2) // 2
+        r = r_cells * d
+        i_lo, i_hi = max(ni // 2 - r_cells, 1), min(ni // 2 + r_cells, ni - 2)
+        case.curve = (1, 0.0, round(r, 9), xc, round(Y[jc], 9), 0.0) + (0.0,) * 7 + (0,)
+        case.hill_box = tuple(round(v, 9) for v in (X[i_lo], X[i_hi], Y[jc - r_cells], Y[jc + r_cells], Z[0],
+                                                     Z[r_cells]))
+    params = dict(index=index, NI=ni, NJ=nj, NK=nk, two_d=two_d, sigma=sigma, porosity=porosity,
+                  tortuosity=tortuosity, source_height=src_h, hill_height=r_cells * d if r_cells >= 2 else 0.0,
+                  ustar=ustar)
+    return case, receivers, params

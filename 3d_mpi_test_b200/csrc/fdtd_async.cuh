@@ -59,13 +59,14 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Bounded wait for the phase with the given parity: gives up after
-// kMbarSpin polls (each poll may suspend the thread for a while), so a copy
-// that never lands cannot hang the kernel; the caller records the failure.
-constexpr long kMbarSpin = 1L << 22;
+// Bounded wait for the phase with the given parity: gives up after `spin`
+// polls (each poll may suspend the thread for a while; 0 polls gives up at
+// once), so a copy that never lands cannot hang the kernel; the caller
+// records the failure.
+constexpr long long kMbarSpin = 1LL << 22;
 
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-    for (long it = 0; it < kMbarSpin; ++it)
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long long spin = kMbarSpin) {
+    for (long long it = 0; it < spin; ++it)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }

@@ -4,12 +4,17 @@
 #include <exception>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "../../include/fdtd_b200.h"
 #include "fdtd_solver.hpp"
 
 struct fdtd_solver {
     fdtd::Solver* s;
+};
+
+struct fdtd_ensemble {
+    fdtd::Ensemble* e;
 };
 
 namespace {
@@ -194,4 +199,68 @@ int fdtd_load_restart(fdtd_solver* h, const char* path, int reference_semantics)
 int fdtd_write_contour(fdtd_solver* h, const char* path, int format) {
     if (!h || !path) return bad("null argument");
     return guard([&] { h->s->write_contour(path, format); });
+}
+
+int fdtd_get_receivers(fdtd_solver* h, int first_step, int nsteps, double* out) {
+    if (!h || (!out && nsteps > 0)) return bad("null argument");
+    return guard([&] { h->s->get_receivers(first_step, nsteps, out); });
+}
+
+int fdtd_set_wait_limit(fdtd_solver* h, long long polls) {
+    if (!h) return bad("null argument");
+    return guard([&] { h->s->set_wait_limit(polls); });
+}
+
+int fdtd_ensemble_create(fdtd_solver* const* members, int n, fdtd_ensemble** out) {
+    if (!members || !out || n < 1) return bad("bad ensemble arguments");
+    *out = nullptr;
+    return guard([&] {
+        std::vector<fdtd::Solver*> m;
+        for (int i = 0; i < n; ++i) {
+            if (!members[i]) throw fdtd::SolverError{FDTD_ERR_ARG, "null ensemble member"};
+            m.push_back(members[i]->s);
+        }
+        fdtd::Ensemble* e = new fdtd::Ensemble(m);
+        *out = new fdtd_ensemble{e};
+    });
+}
+
+int fdtd_ensemble_destroy(fdtd_ensemble* e) {
+    if (!e) return FDTD_OK;
+    const int rc = guard([&] { delete e->e; });
+    delete e;
+    return rc;
+}
+
+int fdtd_ensemble_advance(fdtd_ensemble* e, int nsteps, int* taken) {
+    if (!e || nsteps < 0) return bad("bad ensemble advance arguments");
+    return guard([&] {
+        const int n = e->e->advance(nsteps);
+        if (taken) *taken = n;
+    });
+}
+
+int fdtd_ensemble_autotune(fdtd_ensemble* e, int nsteps, int* best) {
+    if (!e || !best || nsteps <= 0) return bad("bad autotune arguments");
+    return guard([&] {
+        const auto b = e->e->autotune(nsteps);
+        best[0] = b[0];
+        best[1] = b[1];
+    });
+}
+
+int fdtd_ensemble_info(const fdtd_ensemble* e, long long* info) {
+    if (!e || !info) return bad("null argument");
+    return guard([&] {
+        const auto s = e->e->shape();
+        info[0] = e->e->launch_count();
+        info[1] = s[0];
+        info[2] = s[1];
+    });
+}
+
+int fdtd_ensemble_last_device_ms(const fdtd_ensemble* e, double* ms) {
+    if (!e || !ms) return bad("null argument");
+    *ms = e->e->last_device_ms();
+    return FDTD_OK;
 }

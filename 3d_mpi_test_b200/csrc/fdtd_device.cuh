@@ -98,6 +98,7 @@ struct Dev {
     double* rec_out;            // [step][nrec]
     int* counters;              // step counters (see k_pressure)
     int* status;                // bit 0: non-finite pressure seen; bit 1: staged-copy timeout
+    long long wait_spin;        // polls of a staged-copy wait before it reports a timeout
 
     __device__ __forceinline__ size_t ix(int g, int i, int j) const {
         return (static_cast<size_t>(g) * NI + i) * NJP + j;

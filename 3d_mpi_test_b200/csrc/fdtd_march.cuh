@@ -73,15 +73,15 @@ struct MarchGeo {
 // step counter: even steps read counters[0] and publish counters[1], odd
 // steps the reverse (no block reads the word this launch writes)
 template <typename R>
-__device__ __forceinline__ void march_bookkeeping(const Dev<R>& d, int par, int step) {
-    if (blockIdx.x == 0 && blockIdx.y == 0) {
+__device__ __forceinline__ void march_bookkeeping(const Dev<R>& d, int par, int step, bool first_block) {
+    if (first_block) {
         const int tt = threadIdx.x;
-        if (tt < d.nrec) {
-            const long long n = d.rec_node[tt];
+        for (int r = tt; r < d.nrec; r += blockDim.x) {  // blocks may be narrower than the receiver list
+            const long long n = d.rec_node[r];
             double val = 0.0;
             if (n >= 0) val = static_cast<double>(d.pold[n]);
             if (fabs(val) < 1.0e-100) val = 0.0;
-            d.rec_out[static_cast<size_t>(step) * d.nrec + tt] = val;
+            d.rec_out[static_cast<size_t>(step) * d.nrec + r] = val;
         }
         if (tt == 0) d.counters[par ^ 1] = step + 1;
     }
@@ -324,23 +324,28 @@ __device__ __forceinline__ void march_emit(const Dev<R>& d, const PlaneC<R>& pc,
     }
 }
 
+// One block of the march: row block bx, plane chunk by of domain d. A block
+// may have more threads than the tile's trows thread rows (batched launches
+// over domains of different widths): the extra threads only take part in
+// the block barriers.
 template <typename R, bool WIND, int VW>
-__global__ void __launch_bounds__(256) k_march(__grid_constant__ const Dev<R> d, const MarchTiling t, int par) {
+__device__ __forceinline__ void march_block(const Dev<R>& d, const MarchTiling& t, int par, int bx, int by) {
     static_assert(VW >= 2 && VW * sizeof(R) <= 16, "a thread owns 2..16 bytes of columns");
     constexpr int V = VW;
     const int NI = d.NI, NJ = d.NJ, NG = d.NG, pitch = d.NJP;
     const int nvec = pitch / V;
     const int tid = threadIdx.x;
-    const int jv = tid % nvec, tr = tid / nvec, m = t.trows;
+    const int m = t.trows;
+    const int jv = tid % nvec, tr = tid / nvec < m ? tid / nvec : NI + 1;  // idle threads start past every row
     const int jb = jv * V;
-    const int i0 = blockIdx.x * t.TI;
-    const int i1 = (blockIdx.x == t.nrb - 1) ? NI : i0 + t.TI;
+    const int i0 = bx * t.TI;
+    const int i1 = (bx == t.nrb - 1) ? NI : i0 + t.TI;
     const int rlo = i0 > 0 ? i0 - 1 : 0;
-    const int c0 = 1 + blockIdx.y * t.GC;
+    const int c0 = 1 + by * t.GC;
     const int c1 = min(c0 + t.GC, NG - 1);
     const int step = d.counters[par];
     const bool y1_on = step + 1 >= d.pml_y_time;
-    march_bookkeeping(d, par, step);
+    march_bookkeeping(d, par, step, bx == 0 && by == 0);
 
     // column data of this thread's vector, fixed for the whole march
     const Arr<R, VW> ayA = ldn<R, VW>(d.ayA + jb), ayP = ldn<R, VW>(d.ayP + jb);
@@ -417,9 +422,15 @@ __global__ void __launch_bounds__(256) k_march(__grid_constant__ const Dev<R> d,
             for (int c = 0; c < 4; ++c) bulk_prefetch_l2(S.rd[c] + q0, bytes);
         }
     };
+    // A wait that runs out marks the block failed: that thread skips its
+    // later waits, and once the issuing thread has failed it issues no more
+    // copies, so every stage keeps at most one copy in flight for the drain
+    // below (a stage is only refilled after its previous copy was seen).
     bool timed_out = false;
+    const long long spin = d.wait_spin;
     auto wait_plane = [&](int x) {
-        if (!mbar_wait(&bar[x % G.ns], static_cast<uint32_t>(((x - plo) / G.ns) & 1))) timed_out = true;
+        if (timed_out) return;
+        if (!mbar_wait(&bar[x % G.ns], static_cast<uint32_t>(((x - plo) / G.ns) & 1), spin)) timed_out = true;
     };
     int issued_hi = plo - 1;
     if (tid == 0) {
@@ -435,7 +446,7 @@ __global__ void __launch_bounds__(256) k_march(__grid_constant__ const Dev<R> d,
         const int slot = q & 1;
         if (tid == 0) {
             const int x = q + G.ns - 1 - W;  // into the stage plane q-1-W used last
-            if (x <= c1 && x > issued_hi) {
+            if (x <= c1 && x > issued_hi && !timed_out) {
                 issue(x);
                 issued_hi = x;
             }
@@ -473,6 +484,37 @@ __global__ void __launch_bounds__(256) k_march(__grid_constant__ const Dev<R> d,
             for (int x = max(plo, issued_hi - G.ns + 1); x <= issued_hi; ++x)
                 mbar_wait(&bar[x % G.ns], static_cast<uint32_t>(((x - plo) / G.ns) & 1));
     }
+}
+
+template <typename R, bool WIND, int VW>
+__global__ void __launch_bounds__(256) k_march(__grid_constant__ const Dev<R> d, const MarchTiling t, int par) {
+    march_block<R, WIND, VW>(d, t, par, blockIdx.x, blockIdx.y);
+}
+
+// One block of a batched launch over independent domains (an ensemble of
+// solves): block b runs row block bx, plane chunk by of domain `member`.
+struct BatchWork {
+    int member, bx, by;
+};
+
+// A domain of a batched launch: its fused-pass parameters at the parity of
+// the step, that parity and its tile.
+template <typename R>
+struct BatchEntry {
+    Dev<R> d;
+    MarchTiling t;
+    int par;
+};
+
+// entries [2][nmem]: phase 0 holds every member at the parity of the first
+// step of the sequence, phase 1 at the other one; step s of a sequence
+// passes phase s & 1.
+template <typename R, bool WIND, int VW>
+__global__ void __launch_bounds__(256) k_march_batch(const BatchWork* __restrict__ work,
+                                                     const BatchEntry<R>* __restrict__ entries, int nmem, int phase) {
+    const BatchWork w = work[blockIdx.x];
+    const BatchEntry<R>& e = entries[phase * nmem + w.member];
+    march_block<R, WIND, VW>(e.d, e.t, e.par, w.bx, w.by);
 }
 
 }  // namespace fdtd

@@ -130,6 +130,8 @@ class SolverImplBase {
     virtual double last_device_ms() const = 0;
     virtual void set_tiling_api(int TI, int GC, int nt, int vw, int stages) = 0;
     virtual std::array<int, 5> autotune(int nsteps) = 0;
+    virtual void get_receivers(int first_step, int nsteps, double* out) = 0;
+    virtual void set_wait_limit(long long polls) = 0;
 };
 
 template <typename R>
@@ -158,7 +160,10 @@ class SolverImpl final : public SolverImplBase {
         // FB_v_p and larger rows keep the two passes
         const int nvec = NJP_ / kVecMax;
         fused_ = (in.scheme == FB_P_V) && nvec <= kMarchThreads && march_smem_bytes(make_tiling(2, 16, 1, kVecMax, 0)) <= kSmemMax;
-        if (fused_) set_tiling(4, 16, 256, 0, 0);
+        if (fused_) {  // 4-row tiles where they fit shared memory, else 2-row
+            const int TI = march_smem_bytes(make_tiling(4, 16, 256 / nvec, kVecMax, 0)) <= kSmemMax ? 4 : 2;
+            set_tiling(TI, 16, 256, 0, 0);
+        }
         reset(in.time_domain);
     }
 
@@ -166,6 +171,7 @@ class SolverImpl final : public SolverImplBase {
         cudaSetDevice(device_);
         if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
         for (void* p : allocs_) cudaFree(p);
+        if (d_rec_out_) cudaFree(d_rec_out_);
         if (ev0_) cudaEventDestroy(ev0_);
         if (ev1_) cudaEventDestroy(ev1_);
         if (stream_) cudaStreamDestroy(stream_);
@@ -709,6 +715,7 @@ class SolverImpl final : public SolverImplBase {
         d.rec_out = d_rec_out_;
         d.counters = d_counters_;
         d.status = d_status_;
+        d.wait_spin = wait_spin_;
         return d;
     }
 
@@ -790,10 +797,11 @@ class SolverImpl final : public SolverImplBase {
         const MarchTiling t = make_tiling(TI, GC, std::max(1, nt / nvec), VW, stages);
         const size_t smem = march_smem_bytes(t);
         if (smem > kSmemMax) fail(-2, "marching tile does not fit shared memory");
+        // the limit is per kernel and process-wide: always the largest tile,
+        // so other solvers' larger tiles keep launching
         if (smem > 48 * 1024) {
-            const int b = static_cast<int>(smem);
             for_march_kernels([&](const void* k) {
-                FDTD_CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+                FDTD_CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSmemMax)));
             });
         }
         tiling_ = t;
@@ -822,7 +830,7 @@ class SolverImpl final : public SolverImplBase {
         }
         if (VW == 2 && wind_on_) k = reinterpret_cast<const void*>(k_march<R, true, 2>);
         if (smem > 48 * 1024)
-            FDTD_CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+            FDTD_CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSmemMax)));
         FDTD_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, threads, smem));
         return n;
     }
@@ -938,6 +946,17 @@ class SolverImpl final : public SolverImplBase {
         return lim;
     }
 
+    // end of a frame: next frame index, and the end of the run after the
+    // last frame or at the horizon (airpore.cpp:621-624)
+    void close_frame_if_full() {
+        if (n_in_frame_ < mf_limit_) return;
+        mf_count_ += 1;
+        temp_time_ += mf_limit_;
+        frame_started_ = false;
+        const int last = static_cast<int>((ijkmax_ - mf_.JMAX) / (mf_.lead_DJ - 1) + 1.e-6);
+        if (!(mf_count_ <= last && temp_time_ < horizon_ && mf_.Judge == 1)) done_ = true;
+    }
+
     int advance(int nsteps, double* rec_out) override {
         FDTD_CK(cudaSetDevice(device_));
         const int start = steps_;
@@ -955,13 +974,7 @@ class SolverImpl final : public SolverImplBase {
             if (todo > 0) run_steps(todo);
             left -= std::max(todo, 0);
             n_in_frame_ += std::max(todo, 0);
-            if (n_in_frame_ >= mf_limit_) {
-                mf_count_ += 1;
-                temp_time_ += mf_limit_;
-                frame_started_ = false;
-                const int last = static_cast<int>((ijkmax_ - mf_.JMAX) / (mf_.lead_DJ - 1) + 1.e-6);
-                if (!(mf_count_ <= last && temp_time_ < horizon_ && mf_.Judge == 1)) done_ = true;
-            }
+            close_frame_if_full();
         }
         FDTD_CK(cudaEventRecord(ev1_, stream_));
         FDTD_CK(cudaStreamSynchronize(stream_));
@@ -975,8 +988,15 @@ class SolverImpl final : public SolverImplBase {
             d2h(rec_out, d_rec_out_ + static_cast<size_t>(start) * rec_idx_.size(),
                 sizeof(double) * taken * rec_idx_.size());
         }
-        if (st & 1) fail(-4, "pressure became non-finite");
+        check_status(st);
         return taken;
+    }
+
+    // a timed-out wait leaves the step's values meaningless, so it is
+    // reported before a non-finite pressure
+    void check_status(int st) const {
+        if (st & 2) fail(-7, "a staged plane copy did not complete within the wait limit");
+        if (st & 1) fail(-4, "pressure became non-finite");
     }
 
     // half steps (FB_p_v): airpore::Cal_pressure, then Cal_velocity + UpdateInitialCond
@@ -1397,6 +1417,79 @@ class SolverImpl final : public SolverImplBase {
     }
     double last_device_ms() const override { return last_ms_; }
 
+    // receiver samples of steps [first_step, first_step + nsteps) already
+    // taken, [nsteps][n_receivers]
+    void get_receivers(int first_step, int nsteps, double* out) override {
+        FDTD_CK(cudaSetDevice(device_));
+        if (first_step < 0 || nsteps < 0 || first_step + nsteps > steps_)
+            fail(-5, "receiver range outside the steps taken so far");
+        if (rec_idx_.empty() || nsteps == 0) return;
+        d2h(out, d_rec_out_ + static_cast<size_t>(first_step) * rec_idx_.size(),
+            sizeof(double) * static_cast<size_t>(nsteps) * rec_idx_.size());
+    }
+
+    // polls a staged-copy wait of the fused pass makes before it reports a
+    // timeout (0 gives up at once; < 0 restores the default)
+    void set_wait_limit(long long polls) override {
+        wait_spin_ = polls < 0 ? kMbarSpin : polls;
+        graph_dirty_ = true;  // the limit is a captured kernel argument
+    }
+
+    // ------------------------------------------------- ensemble member
+    // What a batched launch needs from this domain: the fused-pass
+    // parameters of both parities, its tile and block shape.
+    struct BatchView {
+        Dev<R> dev[2];
+        MarchTiling tile;
+        int threads;
+        size_t smem;
+        bool wind;
+        int par;
+    };
+    int device() const { return device_; }
+    int horizon() const { return horizon_; }
+    // Readies the domain for lock-step steps taken by batched launches
+    // (frame data uploaded and complete) and returns how many of n steps it
+    // can take before its horizon.
+    int batch_prepare(int n) {
+        FDTD_CK(cudaSetDevice(device_));
+        if (!fused_) fail(-2, "ensemble members need the fused FB_p_v pass");
+        if (mf_.Judge == 1) fail(-2, "ensemble members cannot use the moving frame");
+        if (done_) return 0;
+        if (!frame_started_) {
+            mf_limit_ = frame_limit();
+            upload_frame(mf_count_);
+            frame_started_ = true;
+            n_in_frame_ = 0;
+        }
+        FDTD_CK(cudaStreamSynchronize(stream_));
+        return std::max(0, std::min(n, mf_limit_ - n_in_frame_));
+    }
+    BatchView batch_view() const {
+        BatchView v{};
+        v.dev[0] = params_fused(0);
+        v.dev[1] = params_fused(1);
+        v.tile = tiling_;
+        v.threads = fused_threads_;
+        v.smem = fused_smem_;
+        v.wind = wind_on_;
+        v.par = par_;
+        return v;
+    }
+    // n steps were taken by batched launches
+    void batch_commit(int n, double ms) {
+        if (n & 1) par_ ^= 1;
+        steps_ += n;
+        n_in_frame_ += n;
+        last_ms_ = ms;
+        close_frame_if_full();
+    }
+    void batch_check_status() {
+        int st = 0;
+        d2h(&st, d_status_, sizeof(int));
+        check_status(st);
+    }
+
    private:
     struct SlabDesc {
         int i0, j0, k0, ni, nj, nk;
@@ -1448,6 +1541,7 @@ class SolverImpl final : public SolverImplBase {
     MarchTiling tiling_{};
     int fused_threads_ = 0;
     size_t fused_smem_ = 0;
+    long long wait_spin_ = kMbarSpin;
     // receivers
     std::vector<std::array<int, 3>> rec_idx_;
     // time loop
@@ -1492,5 +1586,318 @@ void Solver::load_restart(const std::string& path, bool reference_semantics) {
 }
 std::array<int, 5> Solver::autotune(int nsteps) { return impl_->autotune(nsteps); }
 double Solver::last_device_ms() const { return impl_->last_device_ms(); }
+void Solver::get_receivers(int first_step, int nsteps, double* out) { impl_->get_receivers(first_step, nsteps, out); }
+void Solver::set_wait_limit(long long polls) { impl_->set_wait_limit(polls); }
+
+// ---------------------------------------------------------------- Ensemble
+class EnsembleImplBase {
+   public:
+    virtual ~EnsembleImplBase() = default;
+    virtual int advance(int nsteps) = 0;
+    virtual std::array<int, 2> autotune(int nsteps) = 0;
+    virtual double last_device_ms() const = 0;
+    virtual long long launch_count() const = 0;
+    virtual std::array<long long, 2> shape() const = 0;
+};
+
+// Independent domains of one precision on one device stepped together.
+// Members are grouped by kernel form (wind, column vector width) and block
+// size class; every step is one launch of k_march_batch per group over the
+// group's work list of (member, row block, plane chunk), heaviest blocks
+// first. Groups are independent chains on their own streams, forked from
+// and joined to the ensemble stream, and the time loop runs as a CUDA graph
+// of kGraphSteps steps of every chain.
+template <typename R>
+class EnsembleImpl final : public EnsembleImplBase {
+   public:
+    explicit EnsembleImpl(std::vector<SolverImpl<R>*> members) : mem_(std::move(members)) {
+        if (mem_.empty()) fail(-5, "an ensemble needs at least one member");
+        device_ = mem_[0]->device();
+        for (size_t a = 0; a < mem_.size(); ++a) {
+            if (mem_[a]->device() != device_) fail(-5, "ensemble members must share one device");
+            for (size_t b = 0; b < a; ++b)
+                if (mem_[a] == mem_[b]) fail(-5, "a solver appears twice in the ensemble");
+        }
+        FDTD_CK(cudaSetDevice(device_));
+        FDTD_CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+        FDTD_CK(cudaEventCreate(&ev0_));
+        FDTD_CK(cudaEventCreate(&ev1_));
+        FDTD_CK(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming));
+    }
+    ~EnsembleImpl() override {
+        cudaSetDevice(device_);
+        if (stream_) cudaStreamSynchronize(stream_);
+        if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+        for (Group& g : groups_) release(g);
+        if (fork_) cudaEventDestroy(fork_);
+        if (ev0_) cudaEventDestroy(ev0_);
+        if (ev1_) cudaEventDestroy(ev1_);
+        if (stream_) cudaStreamDestroy(stream_);
+    }
+
+    int advance(int nsteps) override {
+        FDTD_CK(cudaSetDevice(device_));
+        if (nsteps < 0) fail(-5, "negative step count");
+        int n = nsteps;
+        for (SolverImpl<R>* s : mem_) n = std::min(n, s->batch_prepare(nsteps));
+        if (n <= 0) {
+            if (nsteps > 0) fail(-6, "an ensemble member has reached its horizon; reset it");
+            return 0;
+        }
+        plan();
+        FDTD_CK(cudaEventRecord(ev0_, stream_));
+        int s = 0;
+        if (n >= kGraphSteps) {
+            ensure_graph();
+            for (; s + kGraphSteps <= n; s += kGraphSteps) {
+                FDTD_CK(cudaGraphLaunch(graph_exec_, stream_));
+                launches_ += static_cast<long long>(kGraphSteps) * groups_.size();
+            }
+        }
+        if (s < n) enqueue_steps(n - s);
+        FDTD_CK(cudaEventRecord(ev1_, stream_));
+        FDTD_CK(cudaStreamSynchronize(stream_));
+        float ms = 0.f;
+        FDTD_CK(cudaEventElapsedTime(&ms, ev0_, ev1_));
+        last_ms_ = ms;
+        for (SolverImpl<R>* m : mem_) m->batch_commit(n, ms);
+        for (SolverImpl<R>* m : mem_) m->batch_check_status();
+        return n;
+    }
+
+    // Project autotuner for the ensemble: one tile rule for every member,
+    // rows per block {2, 4, 8} x plane chunk {4, 8, 16, 32} (256-thread
+    // blocks of 16-byte column vectors; a member whose tile does not fit
+    // shared memory keeps 2 rows), each timed over nsteps steps of the whole
+    // ensemble. Every member ends reset to t = 0 with its horizon kept.
+    std::array<int, 2> autotune(int nsteps) override {
+        FDTD_CK(cudaSetDevice(device_));
+        nsteps = std::max(nsteps, 1);
+        std::vector<int> saved;
+        for (SolverImpl<R>* m : mem_) saved.push_back(m->horizon());
+        const std::array<int, 3> TIs{2, 4, 8};
+        const std::array<int, 4> GCs{4, 8, 16, 32};
+        const int h = (nsteps + 2) * static_cast<int>(TIs.size() * GCs.size()) + 4;
+        for (SolverImpl<R>* m : mem_) m->reset(h);
+        std::array<int, 2> best{0, 0};
+        double best_ms = 1e300;
+        for (int TI : TIs)
+            for (int GC : GCs) {
+                apply_tiling(TI, GC);
+                advance(2);  // graph build outside the timing
+                advance(nsteps);
+                if (last_ms_ < best_ms) { best_ms = last_ms_; best = {TI, GC}; }
+            }
+        apply_tiling(best[0], best[1]);
+        for (size_t i = 0; i < mem_.size(); ++i) mem_[i]->reset(saved[i]);
+        return best;
+    }
+
+    double last_device_ms() const override { return last_ms_; }
+    long long launch_count() const override { return launches_; }
+    std::array<long long, 2> shape() const override {
+        long long blocks = 0;
+        for (const Group& g : groups_) blocks += static_cast<long long>(g.work.size());
+        return {static_cast<long long>(groups_.size()), blocks};
+    }
+
+   private:
+    static constexpr int kGraphSteps = 16;  // even: the phase pattern repeats
+
+    struct Group {
+        bool wind = false;
+        int VW = 0, threads = 0;
+        size_t smem = 0;
+        std::vector<int> members;  // indices into mem_
+        std::vector<BatchWork> work;
+        std::vector<BatchEntry<R>> entries;  // host copy, [2][members]
+        BatchWork* d_work = nullptr;
+        BatchEntry<R>* d_entries = nullptr;
+        cudaStream_t stream = nullptr;
+        cudaEvent_t done = nullptr;
+    };
+
+    void apply_tiling(int TI, int GC) {
+        for (SolverImpl<R>* m : mem_) {
+            try {
+                m->set_tiling_api(TI, GC, 256, 0, 0);
+            } catch (const SolverError&) {
+                m->set_tiling_api(2, GC, 256, 0, 0);
+            }
+        }
+    }
+
+    static void release(Group& g) {
+        if (g.d_work) cudaFree(g.d_work);
+        if (g.d_entries) cudaFree(g.d_entries);
+        if (g.done) cudaEventDestroy(g.done);
+        if (g.stream) cudaStreamDestroy(g.stream);
+        g = Group{};
+    }
+
+    // Groups, work lists and parameter tables for the members' current
+    // tiles and parities. The work lists (and so the graph) are rebuilt only
+    // when a member's tile changed; the tables are refreshed every call.
+    void plan() {
+        std::vector<typename SolverImpl<R>::BatchView> v;
+        v.reserve(mem_.size());
+        for (SolverImpl<R>* m : mem_) v.push_back(m->batch_view());
+        // block size class: 64-thread steps, so narrow (2D) members do not
+        // share a launch with 256-thread blocks
+        auto key_of = [&](size_t i) {
+            const int cls = (v[i].threads + 63) / 64;
+            return std::array<int, 3>{v[i].wind ? 1 : 0, v[i].tile.VW, cls};
+        };
+        std::vector<std::array<int, 3>> keys;
+        std::vector<int> gi(mem_.size());
+        for (size_t i = 0; i < mem_.size(); ++i) {
+            const auto k = key_of(i);
+            auto it = std::find(keys.begin(), keys.end(), k);
+            gi[i] = static_cast<int>(it - keys.begin());
+            if (it == keys.end()) keys.push_back(k);
+        }
+        std::vector<int> sig;  // everything the captured launches depend on
+        for (size_t i = 0; i < mem_.size(); ++i) {
+            const MarchTiling& tl = v[i].tile;
+            sig.insert(sig.end(), {gi[i], tl.TI, tl.nrb, tl.GC, tl.nchunk, tl.rows_max, tl.nstage, tl.trows, tl.VW,
+                                   v[i].threads, static_cast<int>(v[i].smem)});
+        }
+        if (sig != sig_ || groups_.empty()) {
+            if (graph_exec_) { cudaGraphExecDestroy(graph_exec_); graph_exec_ = nullptr; }
+            for (Group& g : groups_) release(g);
+            groups_.assign(keys.size(), Group{});
+            for (size_t i = 0; i < mem_.size(); ++i) groups_[gi[i]].members.push_back(static_cast<int>(i));
+            for (size_t k = 0; k < keys.size(); ++k) {
+                Group& g = groups_[k];
+                g.wind = keys[k][0] != 0;
+                g.VW = keys[k][1];
+                struct Costed { long long cost; BatchWork w; };
+                std::vector<Costed> blocks;
+                for (int a = 0; a < static_cast<int>(g.members.size()); ++a) {
+                    const auto& m = v[g.members[a]];
+                    g.threads = std::max(g.threads, m.threads);
+                    g.smem = std::max(g.smem, m.smem);
+                    const MarchTiling& tl = m.tile;
+                    const long long row = m.dev[0].NJP;
+                    for (int by = 0; by < tl.nchunk; ++by)
+                        for (int bx = 0; bx < tl.nrb; ++bx) {
+                            const int rows = bx == tl.nrb - 1 ? m.dev[0].NI - bx * tl.TI : tl.TI;
+                            const int planes = std::min(tl.GC, m.dev[0].NG - 2 - by * tl.GC);
+                            blocks.push_back({static_cast<long long>(rows + 1) * row * (planes + 2), {a, bx, by}});
+                        }
+                }
+                // longest blocks first: the short ones fill the last wave
+                std::stable_sort(blocks.begin(), blocks.end(),
+                                 [](const Costed& x, const Costed& y) { return x.cost > y.cost; });
+                for (const Costed& c : blocks) g.work.push_back(c.w);
+                g.threads = (g.threads + 31) / 32 * 32;
+                FDTD_CK(cudaMalloc(&g.d_work, sizeof(BatchWork) * g.work.size()));
+                FDTD_CK(cudaMalloc(&g.d_entries, sizeof(BatchEntry<R>) * 2 * g.members.size()));
+                FDTD_CK(cudaMemcpy(g.d_work, g.work.data(), sizeof(BatchWork) * g.work.size(), cudaMemcpyHostToDevice));
+                FDTD_CK(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
+                FDTD_CK(cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming));
+                if (g.smem > 48 * 1024)  // process-wide per kernel: the largest tile
+                    FDTD_CK(cudaFuncSetAttribute(kernel(g), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 static_cast<int>(SolverImpl<R>::kSmemMax)));
+            }
+            sig_ = sig;
+        }
+        for (Group& g : groups_) {
+            const size_t nm = g.members.size();
+            g.entries.resize(2 * nm);
+            for (size_t a = 0; a < nm; ++a) {
+                const auto& m = v[g.members[a]];
+                for (int ph = 0; ph < 2; ++ph) {
+                    const int par = (m.par + ph) & 1;
+                    g.entries[ph * nm + a] = BatchEntry<R>{m.dev[par], m.tile, par};
+                }
+            }
+            FDTD_CK(cudaMemcpyAsync(g.d_entries, g.entries.data(), sizeof(BatchEntry<R>) * g.entries.size(),
+                                    cudaMemcpyHostToDevice, stream_));
+        }
+    }
+
+    static const void* kernel(const Group& g) {
+        if constexpr (sizeof(R) == 4) {
+            if (g.VW == 4)
+                return g.wind ? reinterpret_cast<const void*>(k_march_batch<R, true, 4>)
+                              : reinterpret_cast<const void*>(k_march_batch<R, false, 4>);
+        }
+        return g.wind ? reinterpret_cast<const void*>(k_march_batch<R, true, 2>)
+                      : reinterpret_cast<const void*>(k_march_batch<R, false, 2>);
+    }
+
+    void launch(const Group& g, int phase) {
+        const dim3 grd(static_cast<unsigned>(g.work.size())), blk(g.threads);
+        const int nm = static_cast<int>(g.members.size());
+        if constexpr (sizeof(R) == 4) {
+            if (g.VW == 4) {
+                if (g.wind) k_march_batch<R, true, 4><<<grd, blk, g.smem, g.stream>>>(g.d_work, g.d_entries, nm, phase);
+                else k_march_batch<R, false, 4><<<grd, blk, g.smem, g.stream>>>(g.d_work, g.d_entries, nm, phase);
+                FDTD_CK(cudaGetLastError());
+                return;
+            }
+        }
+        if (g.wind) k_march_batch<R, true, 2><<<grd, blk, g.smem, g.stream>>>(g.d_work, g.d_entries, nm, phase);
+        else k_march_batch<R, false, 2><<<grd, blk, g.smem, g.stream>>>(g.d_work, g.d_entries, nm, phase);
+        FDTD_CK(cudaGetLastError());
+    }
+
+    // n steps of every group's chain, forked from and joined to stream_
+    void enqueue_steps(int n) {
+        FDTD_CK(cudaEventRecord(fork_, stream_));
+        for (Group& g : groups_) {
+            FDTD_CK(cudaStreamWaitEvent(g.stream, fork_, 0));
+            for (int s = 0; s < n; ++s) launch(g, s & 1);
+            FDTD_CK(cudaEventRecord(g.done, g.stream));
+            FDTD_CK(cudaStreamWaitEvent(stream_, g.done, 0));
+        }
+        launches_ += static_cast<long long>(n) * groups_.size();
+    }
+
+    void ensure_graph() {
+        if (graph_exec_) return;
+        cudaGraph_t gr;
+        const long long before = launches_;
+        FDTD_CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+        enqueue_steps(kGraphSteps);
+        FDTD_CK(cudaStreamEndCapture(stream_, &gr));
+        launches_ = before;
+        FDTD_CK(cudaGraphInstantiate(&graph_exec_, gr, 0));
+        cudaGraphDestroy(gr);
+    }
+
+    std::vector<SolverImpl<R>*> mem_;
+    int device_ = 0;
+    cudaStream_t stream_ = nullptr;
+    cudaEvent_t ev0_ = nullptr, ev1_ = nullptr, fork_ = nullptr;
+    cudaGraphExec_t graph_exec_ = nullptr;
+    std::vector<Group> groups_;
+    std::vector<int> sig_;
+    long long launches_ = 0;
+    double last_ms_ = 0;
+};
+
+Ensemble::Ensemble(const std::vector<Solver*>& members) {
+    if (members.empty()) fail(-5, "an ensemble needs at least one member");
+    const int prec = members[0]->precision();
+    for (Solver* s : members)
+        if (!s || s->precision() != prec) fail(-5, "ensemble members must be valid solvers of one precision");
+    if (prec == 0) {
+        std::vector<SolverImpl<double>*> m;
+        for (Solver* s : members) m.push_back(static_cast<SolverImpl<double>*>(s->impl_.get()));
+        impl_.reset(new EnsembleImpl<double>(m));
+    } else {
+        std::vector<SolverImpl<float>*> m;
+        for (Solver* s : members) m.push_back(static_cast<SolverImpl<float>*>(s->impl_.get()));
+        impl_.reset(new EnsembleImpl<float>(m));
+    }
+}
+Ensemble::~Ensemble() = default;
+int Ensemble::advance(int nsteps) { return impl_->advance(nsteps); }
+std::array<int, 2> Ensemble::autotune(int nsteps) { return impl_->autotune(nsteps); }
+double Ensemble::last_device_ms() const { return impl_->last_device_ms(); }
+long long Ensemble::launch_count() const { return impl_->launch_count(); }
+std::array<long long, 2> Ensemble::shape() const { return impl_->shape(); }
 
 }  // namespace fdtd

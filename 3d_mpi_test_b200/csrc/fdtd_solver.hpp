@@ -18,6 +18,7 @@ struct SolverError {
 };
 
 class SolverImplBase;
+class EnsembleImplBase;
 
 // Receiver post-processing on a device (fdtd_spectra.cu): the reference's
 // zero-padded, 1/2^m-scaled forward FFT of each trace [nrec][nt], as the
@@ -66,10 +67,40 @@ class Solver {
                     int ring_stages);
     std::array<int, 5> autotune(int nsteps);
     double last_device_ms() const;
+    // receiver samples of steps [first_step, first_step + nsteps) already taken
+    void get_receivers(int first_step, int nsteps, double* out);
+    // polls of a staged-copy wait before the fused pass reports a timeout
+    // (0: at once; < 0: the default)
+    void set_wait_limit(long long polls);
 
    private:
+    friend class Ensemble;
     int precision_;
     std::unique_ptr<SolverImplBase> impl_;
+};
+
+// Independent solvers of one precision on one device stepped together by
+// batched launches of the marching kernel (fused FB_p_v members without the
+// moving frame). The solvers stay owned by the caller and keep their own
+// setup, read-out and receiver buffers; they must outlive the ensemble.
+class Ensemble {
+   public:
+    explicit Ensemble(const std::vector<Solver*>& members);
+    ~Ensemble();
+    Ensemble(const Ensemble&) = delete;
+    Ensemble& operator=(const Ensemble&) = delete;
+    // lock-step steps of every member; returns the steps taken (the nearest
+    // member horizon bounds it)
+    int advance(int nsteps);
+    // one tile rule for all members: returns {rows per block, planes per block}
+    std::array<int, 2> autotune(int nsteps);
+    double last_device_ms() const;
+    long long launch_count() const;
+    // {launch groups, blocks per step}
+    std::array<long long, 2> shape() const;
+
+   private:
+    std::unique_ptr<EnsembleImplBase> impl_;
 };
 
 }  // namespace fdtd

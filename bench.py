@@ -17,6 +17,14 @@ reference's MPI decomposition has no MPI here), aggregate throughput.
 
 Multi-GPU: replicas only -- each rank runs its own independent solve, no
 collective on the data path; value = all ranks' cell updates / max time.
+
+``--workload ensemble`` measures the batched ensemble instead: ``--members``
+independent FP32 solves drawn by casegen.ensemble_member (seed = rank),
+stepped by batched marching launches in a graph-captured loop, tile rule
+from the ensemble autotuner; value = all members' cell updates / device
+time. Every member (or the first ``--check-members``) is then checked
+against its own FP64 single solve (receiver relative L2 over
+``--check-steps`` steps).
 """
 
 from __future__ import annotations
@@ -194,6 +202,112 @@ def cpu_baseline(case_dir: str, cells: int):
 
 
 # ---------------------------------------------------------------- GPU side
+ENS_WORKLOAD = ("batched ensemble: seeded members, NJ U[64,512] x NK U[32,192], NI 3 (2D) for half and "
+                "U[32,96] else, porous ground 8 cells, porous hill, log wind, 10-node PML, FP32")
+
+
+def run_ensemble(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+
+    pkg = importlib.import_module("3d_mpi_test_b200")
+    casegen = importlib.import_module("3d_mpi_test_b200.casegen")
+    replicas = importlib.import_module("3d_mpi_test_b200.replicas")
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist  # noqa: F811
+    group = replicas.ReplicaGroup(dist, "cuda")
+    tmp = tempfile.mkdtemp(prefix=f"bench_ens_r{rank}_")
+    inner = args.inner
+    horizon = (args.warmup + args.steps) * inner + 8
+    specs, cells, mem = [], 0, []
+    t_setup = time.perf_counter()
+    for i in range(args.members):
+        c, rec, p = casegen.ensemble_member(rank, i, steps=horizon)
+        d = c.write(os.path.join(tmp, f"m{i:03d}"))
+        specs.append((d, rec, p))
+        cells += c.NI * c.NJ * (c.NK + len(c.pore_Z))
+        a = pkg.Airpore(d, "f32", device=local_rank)
+        a.set_receivers(rec)
+        a.reset(horizon)
+        mem.append(a)
+    ens = pkg.Ensemble(mem)
+    tile = ens.autotune(3)
+    for a in mem:
+        a.reset(horizon)
+    setup_s = time.perf_counter() - t_setup
+    for _ in range(args.warmup):
+        ens.advance(inner)
+    group.barrier()
+    torch.cuda.synchronize()
+    launches0 = ens.info()["launches"]
+    dev_ms = 0.0
+    sampler = ClockSampler(local_rank)
+    with sampler:
+        for _ in range(args.steps):
+            ens.advance(inner)  # inputs (hundreds of MB per member set) are far larger than L2
+            dev_ms += ens.last_device_ms()
+    torch.cuda.synchronize()
+    group.barrier()
+    info = ens.info()
+    steps_total = args.steps * inner
+    gcell = group.throughput(cells, steps_total, dev_ms)
+    dev_ms = group.max_over_ranks(dev_ms)
+    # end to end: each bench step starts every member from its initial
+    # condition (host-side Gaussian, H2D upload), steps it and reads all
+    # receiver series back
+    h2d = sum(a.state_elems() for a in mem) * 4  # the initial FP32 pressure field of each member
+    e2e_n = 2
+    t1 = time.perf_counter()
+    nrec_words = 0
+    for _ in range(e2e_n):
+        for a in mem:
+            a.reset(horizon)
+        ens.advance(inner)
+        nrec_words = 0
+        for a in mem:
+            nrec_words += a.receivers(0, inner).size
+    torch.cuda.synchronize()
+    e2e_s = group.max_over_ranks(time.perf_counter() - t1)
+    e2e = {"value": round(world * cells * inner * e2e_n / e2e_s / 1e9, 3), "unit": UNIT,
+           "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(nrec_words * 8)}
+    # every member against its own FP64 single solve
+    nchk = min(args.check_members, len(mem)) if args.check_members >= 0 else len(mem)
+    for a in mem:
+        a.reset(horizon)
+    ens.advance(args.check_steps)
+    errs = []
+    for (d, rec, p), a in zip(specs[:nchk], mem[:nchk]):
+        r32 = a.receivers(0, args.check_steps)
+        with pkg.Airpore(d, "f64", device=local_rank) as b:
+            b.set_receivers(rec)
+            r64 = b.get_output(args.check_steps)
+        errs.append(float(np.linalg.norm(r32 - r64) / np.linalg.norm(r64)))
+    ens.close()
+    for a in mem:
+        a.close()
+    shutil.rmtree(tmp, ignore_errors=True)
+    if rank != 0:
+        return None
+    return {
+        "metric": "Gcell-upd/s of a batched ensemble (FP32), each member checked against its FP64 single solve",
+        "value": round(gcell, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(dev_ms / args.steps, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded ensemble generator)",
+        "config": {"workload": ENS_WORKLOAD, "members": args.members, "cells_per_fb_step": cells,
+                   "inner_fb_steps_per_bench_step": inner, "l2": "inputs larger than L2",
+                   "tile_rows_planes": list(tile), "launch_groups": info["groups"],
+                   "blocks_per_fb_step": info["blocks_per_step"], "setup_s": round(setup_s, 1),
+                   "parallelism": f"replicas x{world}" if world > 1 else "one device"},
+        "check": {"members": nchk, "steps": args.check_steps, "max_rel_l2_receivers_vs_fp64": max(errs),
+                  "median_rel_l2": statistics.median(errs)},
+        "e2e": e2e,
+        "gpu_launches": int(info["launches"] - launches0),
+        "clocks": sampler.summary(),
+    }
+
+
 def run_gpu(args, rank, world, local_rank):
     import numpy as np
     import torch
@@ -363,6 +477,10 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tile", default="", help="rows,planes,threads,vector-width,ring-stages of the marching kernel (default: autotune)")
+    ap.add_argument("--workload", default="domain", choices=["domain", "ensemble"])
+    ap.add_argument("--members", type=int, default=256, help="ensemble members (--workload ensemble)")
+    ap.add_argument("--check-members", type=int, default=-1, help="members checked against FP64 (-1: all)")
+    ap.add_argument("--check-steps", type=int, default=200)
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -383,7 +501,10 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     try:
-        line = run_gpu(args, rank, world, local_rank)
+        if args.workload == "ensemble":
+            line = run_ensemble(args, rank, world, local_rank)
+        else:
+            line = run_gpu(args, rank, world, local_rank)
     finally:
         if world > 1:
             import torch.distributed as dist

@@ -28,6 +28,11 @@
  *                      calculation_2D.cpp:522-545)
  *   fdtd_get_psi       calculation_2D::Psi (TDBC state, calculation_2D.h:71)
  *   fdtd_get_slab      air::Qux1..Qpz2 PML integrals (air.h:40-42)
+ *   fdtd_get_receivers the receiver series airpore::get_output collects
+ *                      through get_pressure (airpore.cpp:566-580)
+ *   fdtd_ensemble_*    no counterpart: the reference runs one case per MPI
+ *                      job; an ensemble steps many handles' get_output loops
+ *                      together
  */
 #ifndef FDTD_B200_H
 #define FDTD_B200_H
@@ -45,6 +50,7 @@ extern "C" {
 #define FDTD_ERR_NONFINITE (-4)   /* a pressure value became Inf/NaN */
 #define FDTD_ERR_ARG (-5)         /* bad argument (null pointer, range) */
 #define FDTD_ERR_STATE (-6)       /* time loop finished; call fdtd_reset */
+#define FDTD_ERR_TIMEOUT (-7)     /* a staged plane copy did not land within the wait limit */
 
 #define FDTD_F64 0
 #define FDTD_F32 1
@@ -130,6 +136,41 @@ long long fdtd_launch_count(const fdtd_solver *h);
 
 /* CUDA events around the last fdtd_advance's device work: milliseconds. */
 int fdtd_last_device_ms(const fdtd_solver *h, double *ms);
+
+/* Receiver samples of steps [first_step, first_step + nsteps) already
+ * taken since the last reset (fdtd_advance, fdtd_ensemble_advance), as
+ * out [nsteps][n_receivers] FP64. */
+int fdtd_get_receivers(fdtd_solver *h, int first_step, int nsteps, double *out);
+
+/* Polls a staged-copy wait of the marching kernel makes before the kernel
+ * gives up on the plane, records the failure and finishes without hanging
+ * (the step then returns FDTD_ERR_TIMEOUT; the state is not meaningful and
+ * the handle needs fdtd_reset). 0 gives up at the first wait, which lets a
+ * caller exercise the error path; < 0 restores the default (2^22 polls). */
+int fdtd_set_wait_limit(fdtd_solver *h, long long polls);
+
+/* Ensembles: independent handles of one precision on one device stepped
+ * together. Each step is one launch of the batched marching kernel per
+ * group of members (same kernel form and block size class) over a work
+ * list of (member, row block, plane chunk), heaviest blocks first; groups
+ * run as parallel chains and the time loop is captured in a CUDA graph.
+ * Members must use the fused FB_p_v pass (FDTD_ERR_UNSUPPORTED otherwise)
+ * and no moving frame; they keep their receivers, horizon and read-out, and
+ * must outlive the ensemble. fdtd_ensemble_advance takes min(nsteps, the
+ * steps left to the nearest member horizon) steps of every member and
+ * stores that count in *taken (FDTD_ERR_STATE if a member has none left).
+ * fdtd_ensemble_autotune times one tile rule for all members (rows per
+ * block x planes per block, nsteps steps each), keeps the fastest in
+ * best[2] and resets every member to t = 0 with its horizon kept.
+ * fdtd_ensemble_info: info[0] launches so far, info[1] groups (launches per
+ * step), info[2] thread blocks per step. */
+typedef struct fdtd_ensemble fdtd_ensemble;
+int fdtd_ensemble_create(fdtd_solver *const *members, int n, fdtd_ensemble **out);
+int fdtd_ensemble_destroy(fdtd_ensemble *e);
+int fdtd_ensemble_advance(fdtd_ensemble *e, int nsteps, int *taken);
+int fdtd_ensemble_autotune(fdtd_ensemble *e, int nsteps, int *best);
+int fdtd_ensemble_info(const fdtd_ensemble *e, long long *info);
+int fdtd_ensemble_last_device_ms(const fdtd_ensemble *e, double *ms);
 
 /* Pressure contour of the current state (airpore::get_data_contour,
  * airpore.cpp:1014-1056; calculation_2D::mpi_send_data and operator<<,

@@ -174,9 +174,26 @@ def narrow_y():
     return c, [(0.3, 0.1, 0.25), (0.35, 0.15, 0.3)]
 
 
+ENS_SMALL = ((24, 36), (16, 20), (10, 13))  # NJ, NK, 3D NI ranges of the small ensemble members
+
+
+def ensemble_member_2d():
+    """A small member of the seeded batched-ensemble generator: 2D (NI = 3,
+    Front/Back rigid), porous ground, porous hill, logarithmic wind."""
+    c, rec, _ = casegen.ensemble_member(5, 0, pml=4, layer=4, steps=40, n_receivers=3, sizes=ENS_SMALL)
+    return c, rec
+
+
+def ensemble_member_3d():
+    """A small 3D member of the same generator (x PML on both sides)."""
+    c, rec, _ = casegen.ensemble_member(5, 3, pml=4, layer=4, steps=40, n_receivers=3, sizes=ENS_SMALL)
+    return c, rec
+
+
 CASES: Dict[str, Callable[[], Tuple[Case, List]]] = {
     f.__name__: f
     for f in [pml_rigid, tdbc_east, porous_ground, porous_tdbc_fine_pore, south_pml_all_faces, front_only_pml,
               back_only_pml, all_rigid, wind_linear, wind_log, wind_vortex, hill(1), hill(2), hill(3), hill(4),
-              hill(5), moving_frame, fb_v_p, delayed_y1, stretched, odd_columns_wind, odd_columns_porous, narrow_y]
+              hill(5), moving_frame, fb_v_p, delayed_y1, stretched, odd_columns_wind, odd_columns_porous, narrow_y,
+              ensemble_member_2d, ensemble_member_3d]
 }
