@@ -31,7 +31,7 @@ FDTD_ERR_STATE = -6
 FDTD_ERR_TIMEOUT = -7
 F64, F32 = 0, 1
 
-# Every function declared in include/fdtd_b200.h.
+# Every function declared in include/*.h.
 EXPORTS = (
     "fdtd_create", "fdtd_destroy", "fdtd_dims", "fdtd_last_error", "fdtd_set_receivers", "fdtd_reset",
     "fdtd_run", "fdtd_advance", "fdtd_step_pressure", "fdtd_step_velocity", "fdtd_get_field",
@@ -41,6 +41,10 @@ EXPORTS = (
     "fdtd_write_contour", "fdtd_get_receivers", "fdtd_set_wait_limit", "fdtd_ensemble_create",
     "fdtd_ensemble_destroy", "fdtd_ensemble_advance", "fdtd_ensemble_autotune", "fdtd_ensemble_info",
     "fdtd_ensemble_last_device_ms",
+    # include/fdtd_surrogate.h (signatures in surrogate.py)
+    "fdtd_tc_gemm", "fdtd_net_create", "fdtd_net_destroy", "fdtd_net_n_params", "fdtd_net_get_params",
+    "fdtd_net_set_params", "fdtd_net_set_data", "fdtd_net_get_normalization", "fdtd_net_set_normalization",
+    "fdtd_net_train", "fdtd_net_gradients", "fdtd_net_predict", "fdtd_net_predict_device", "fdtd_net_info",
 )
 
 

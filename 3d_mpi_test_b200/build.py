@@ -1,8 +1,9 @@
 """Build recipe for the in-tree native library (sm_100a only).
 
 Produces ``3d_mpi_test_b200/lib/libfdtd_b200.so`` (the C ABI declared in
-``include/fdtd_b200.h``) with explicit nvcc calls; no JIT cache, so the
-built file travels with the source tree.
+``include/fdtd_b200.h`` and ``include/fdtd_surrogate.h``) with explicit
+nvcc calls; no JIT cache, so the built file travels with the source tree.
+An object is rebuilt when its source or any header is newer.
 """
 
 from __future__ import annotations
@@ -22,7 +23,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
               "--expt-relaxed-constexpr", "-I", os.path.join(ROOT, "include")]
 
-SOURCES = ["fdtd_solver.cu", "fdtd_input.cpp", "fdtd_capi.cpp", "fdtd_noalloc.cu", "fdtd_spectra.cu"]
+SOURCES = ["fdtd_solver.cu", "fdtd_input.cpp", "fdtd_capi.cpp", "fdtd_noalloc.cu", "fdtd_spectra.cu", "mlp.cu"]
 
 
 def nvcc() -> str:
@@ -41,7 +42,10 @@ def _stale(target: str, deps) -> bool:
 
 def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = False) -> str:
     os.makedirs(LIBDIR, exist_ok=True)
-    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(ROOT, "include", "fdtd_b200.h")]
+    inc = os.path.join(ROOT, "include")
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".hpp", ".cuh"))] + \
+        [os.path.join(inc, f) for f in os.listdir(inc)]
+    deps = [os.path.join(CSRC, f) for f in SOURCES] + headers
     if not force and not _stale(LIB, deps):
         return LIB
     objdir = os.path.join(LIBDIR, "obj")
@@ -49,13 +53,15 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
     objs = []
     for src in SOURCES:
         obj = os.path.join(objdir, os.path.splitext(src)[0] + ".o")
+        objs.append(obj)
+        if not force and not _stale(obj, [os.path.join(CSRC, src)] + headers):
+            continue
         cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-c", os.path.join(CSRC, src), "-o", obj]
         if ptxas_verbose and src.endswith(".cu"):
             cmd += ["-Xptxas", "-v"]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         subprocess.run(cmd, check=True)
-        objs.append(obj)
     cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)

@@ -7,7 +7,9 @@
 #include <vector>
 
 #include "../../include/fdtd_b200.h"
+#include "../../include/fdtd_surrogate.h"
 #include "fdtd_solver.hpp"
+#include "mlp.hpp"
 
 struct fdtd_solver {
     fdtd::Solver* s;
@@ -15,6 +17,10 @@ struct fdtd_solver {
 
 struct fdtd_ensemble {
     fdtd::Ensemble* e;
+};
+
+struct fdtd_net {
+    fdtd::mlp::Net* n;
 };
 
 namespace {
@@ -264,3 +270,95 @@ int fdtd_ensemble_last_device_ms(const fdtd_ensemble* e, double* ms) {
     *ms = e->e->last_device_ms();
     return FDTD_OK;
 }
+
+// ------------------------------------------------------------- surrogate
+extern "C" {
+
+int fdtd_tc_gemm(int device, int epilogue, int M, int N, int K, const void* A, const void* B, const float* bias,
+                 const void* mask, void* out, void* outT, void* stream) {
+    return guard([&] { fdtd::mlp::gemm(device, epilogue, M, N, K, A, B, bias, mask, out, outT, stream); });
+}
+
+int fdtd_net_create(int device, int n_in, int width, int hidden, int n_out, int batch, unsigned long long seed,
+                    fdtd_net** out) {
+    if (!out) return bad("null argument");
+    *out = nullptr;
+    return guard([&] {
+        auto* n = new fdtd::mlp::Net(device, n_in, width, hidden, n_out, batch, seed);
+        *out = new fdtd_net{n};
+    });
+}
+
+int fdtd_net_destroy(fdtd_net* h) {
+    if (!h) return FDTD_OK;
+    const int rc = guard([&] { delete h->n; });
+    delete h;
+    return rc;
+}
+
+int fdtd_net_n_params(const fdtd_net* h, int* n) {
+    if (!h || !n) return bad("null argument");
+    *n = h->n->n_params();
+    return FDTD_OK;
+}
+
+int fdtd_net_get_params(const fdtd_net* h, float* out) {
+    if (!h || !out) return bad("null argument");
+    return guard([&] { h->n->get_params(out); });
+}
+
+int fdtd_net_set_params(fdtd_net* h, const float* in) {
+    if (!h || !in) return bad("null argument");
+    return guard([&] { h->n->set_params(in); });
+}
+
+int fdtd_net_set_data(fdtd_net* h, const float* X, const float* T, int n) {
+    if (!h || !X || !T) return bad("null argument");
+    return guard([&] { h->n->set_data(X, T, n); });
+}
+
+int fdtd_net_get_normalization(const fdtd_net* h, float* im, float* is, float* om, float* os) {
+    if (!h || !im || !is || !om || !os) return bad("null argument");
+    return guard([&] { h->n->get_normalization(im, is, om, os); });
+}
+
+int fdtd_net_set_normalization(fdtd_net* h, const float* im, const float* is, const float* om, const float* os) {
+    if (!h || !im || !is || !om || !os) return bad("null argument");
+    return guard([&] { h->n->set_normalization(im, is, om, os); });
+}
+
+int fdtd_net_train(fdtd_net* h, int steps, float lr, float lr_final, unsigned long long seed, int report,
+                   double* loss) {
+    if (!h) return bad("null argument");
+    return guard([&] {
+        const double l = h->n->train(steps, lr, lr_final, seed, report);
+        if (loss) *loss = l;
+    });
+}
+
+int fdtd_net_gradients(fdtd_net* h, float* grad, double* loss) {
+    if (!h || !grad) return bad("null argument");
+    return guard([&] {
+        const double l = h->n->gradients(grad);
+        if (loss) *loss = l;
+    });
+}
+
+int fdtd_net_predict(fdtd_net* h, const float* X, int n, float* Y) {
+    if (!h || (n > 0 && (!X || !Y))) return bad("null argument");
+    return guard([&] { h->n->predict(X, n, Y); });
+}
+
+int fdtd_net_predict_device(fdtd_net* h, const float* X, int n, float* Y, void* stream) {
+    if (!h || (n > 0 && (!X || !Y))) return bad("null argument");
+    return guard([&] { h->n->predict_device(X, n, Y, stream); });
+}
+
+int fdtd_net_info(const fdtd_net* h, long long* launches, double* last_ms) {
+    if (!h) return bad("null argument");
+    if (launches) *launches = h->n->launches();
+    if (last_ms) *last_ms = h->n->last_device_ms();
+    return FDTD_OK;
+}
+
+}  // extern "C"
