@@ -763,8 +763,17 @@ class SolverImpl final : public SolverImplBase {
     // rows, W = 1 with wind)
     size_t march_smem_bytes(const MarchTiling& t) const {
         const size_t row = static_cast<size_t>(NJP_) * sizeof(R);
-        const size_t n = t.rows_max + 1, W = wind_on_ ? 1 : 0;
-        return 128 + 2 * (t.rows_max + 1) * row + static_cast<size_t>(t.nstage) * (4 * n + 1 + 3 * W) * row;
+        const int W = wind_on_ ? 1 : 0;
+        // staged rows of the largest block: the kernel's clamped stencil rows
+        // iclo .. ichi (u one more, v w p W more), as k_march computes them
+        int stage_rows = 0;
+        for (int bx = 0; bx < t.nrb; ++bx) {
+            const int i0 = bx * t.TI, i1 = (bx == t.nrb - 1) ? NI_ : i0 + t.TI;
+            const int rlo = i0 > 0 ? i0 - 1 : 0;
+            const int iclo = std::min(std::max(rlo, 1), NI_ - 2), ichi = std::min(std::max(i1 - 1, 1), NI_ - 2);
+            stage_rows = std::max(stage_rows, (ichi + 2 - iclo) + 3 * (ichi + 1 + W - iclo));
+        }
+        return 128 + 2 * static_cast<size_t>(t.rows_max + 1) * row + static_cast<size_t>(t.nstage) * stage_rows * row;
     }
 
     // stages: staging-ring planes (0: the minimum; planes g-1 with wind, g and

@@ -1,0 +1,215 @@
+"""Training data of the surrogate: excess attenuation spectra from FDTD solves.
+
+A sample is one point of the 11-parameter space below. For each sample two
+2D solves (NI = 3, Front/Back rigid: calculation_2D.cpp:835-860) run on the
+device through the batched ensemble:
+
+- the ground solve: ZK porous ground with the sample's flow resistivity,
+  porosity, tortuosity and layer depth; a porous hill (circular segment of
+  the sample's height and half-width, made with the reference's sphere
+  inclusion, air.cpp:1019-1031, and its canopy parameters) half way to the
+  farthest receiver; and a downwind profile;
+- the free-field solve: the same source, receivers and grid with air below
+  the source as well and PML on every face, no hill and no wind.
+
+The eight receivers sit at the receiver height at ranges R (k+1)/8. Each
+receiver trace is zero-padded to 2^FFT_M points. Band levels come from the
+GPU FFT (the reference's transform, airpore::get_FFT_y1) in 17 base-2
+third-octave bands 50 Hz - 2 kHz. Excess attenuation = ground level -
+free-field level per band and receiver, in dB: 136 outputs in
+[receiver][band] order.
+
+Wind: the reference's logarithmic profile (method 5, b ln(z/0.1 + 1),
+air.cpp:175-177) is not usable here. Its strong shear near the ground makes
+the reference's scheme grow without bound within a few hundred to two
+thousand steps, even in a closed rigid box (u* = 0.1 .. 0.6, d = 0.05 m).
+The CPU oracle, bit-exact with the reference, shows the same growth. The
+samples therefore use the reference's linear profile instead: method 1,
+V = b z capped at 2.8 m, air.cpp:128-140, which stays bounded for b <= 1/s
+over 2400 steps. b is matched to the log law of the sample's u* and z0 at
+2.8 m: b = (u*/0.4) ln(2.8/z0 + 1) / 2.8, with u* <= 0.2 m/s and z0 in
+0.01 .. 0.1 m, so b <= 1/s. A solve whose final pressure field exceeds
+half the initial pulse amplitude anywhere (a stable run has spread and
+absorbed the pulse by then) is flagged as grown, and its excess attenuation
+is NaN.
+
+The spacing (d = 0.05 m, CFL 0.5), PML width and range interval are chosen
+so that one sample costs about 1e9 cell updates; the range stays below 45 m
+so that a row holds at most 1024 nodes (the marching kernel's limit).
+"""
+
+from __future__ import annotations
+
+import math
+import os
+import shutil
+import tempfile
+import time
+from typing import Dict, List, Optional, Tuple
+
+import numpy as np
+
+from . import Airpore, Ensemble, THIRD_OCTAVE_50_2K, band_levels
+from .casegen import PML, POROUS, RIGID, Case, uniform_axis
+
+PARAMS = ("log10_sigma", "porosity", "tortuosity", "layer_depth", "source_height", "receiver_height", "range",
+          "hill_height", "hill_halfwidth", "ustar", "z0")
+# sampling box of every input (uniform; sigma log-uniform through log10)
+RANGES: Dict[str, Tuple[float, float]] = {
+    "log10_sigma": (4.0, math.log10(2.0e6)),  # 10 .. 2000 kPa s / m^2
+    "porosity": (0.2, 0.6),
+    "tortuosity": (1.0, 2.5),
+    "layer_depth": (0.1, 0.5),  # m
+    "source_height": (0.1, 3.0),  # m
+    "receiver_height": (0.5, 2.5),  # m
+    "range": (5.0, 45.0),  # m, farthest receiver
+    "hill_height": (0.0, 2.0),  # m
+    "hill_halfwidth": (1.0, 5.0),  # m
+    "ustar": (0.0, 0.2),  # m/s
+    "z0": (0.01, 0.1),  # m
+}
+N_REC = 8
+BANDS = THIRD_OCTAVE_50_2K
+D = 0.05
+PML_N = 20
+C0, RHO0, GAMMA = 343.0, 1.2, 1.4
+DT = 0.5 * D / C0
+FFT_M = 14
+
+
+def draw(seed: int, n: int) -> np.ndarray:
+    """n seeded samples [n][11] uniform in RANGES."""
+    rng = np.random.default_rng(seed)
+    lo = np.array([RANGES[p][0] for p in PARAMS])
+    hi = np.array([RANGES[p][1] for p in PARAMS])
+    return lo + (hi - lo) * rng.random((n, len(PARAMS)))
+
+
+def _r(x: float) -> float:
+    return round(float(x), 9)
+
+
+def steps_for(x: np.ndarray) -> int:
+    """Time steps covering the longest arrival (ground-reflected ray to the
+    farthest receiver) plus 3 m of travel for the pulse and the ground."""
+    p = dict(zip(PARAMS, x))
+    r = math.hypot(p["range"], p["source_height"] + p["receiver_height"])
+    return int(math.ceil((r + 3.0) / (C0 * DT)))
+
+
+def wind_gradient(ustar: float, z0: float) -> float:
+    """b of the linear profile V = b z (z < 2.8 m) that equals the log law
+    (u*/0.4) ln(z/z0 + 1) at 2.8 m."""
+    return (ustar / 0.4) * math.log(2.8 / z0 + 1.0) / 2.8
+
+
+GROWN = 0.5  # Pa: half the 1 Pa initial pulse
+
+
+def grown(final_p: np.ndarray) -> bool:
+    """A final pressure field above half the initial pulse amplitude."""
+    return bool(np.max(np.abs(final_p)) > GROWN)
+
+
+def cases(x: np.ndarray, steps: int) -> Tuple[Case, Case, List[Tuple[float, float, float]]]:
+    """(ground case, free-field case, receivers) of one sample."""
+    p = dict(zip(PARAMS, x))
+    hs, hr, R = p["source_height"], p["receiver_height"], p["range"]
+    top = max(hs, hr, p["hill_height"]) + 2.0
+    y_src = (PML_N + 20) * D
+    nj = int(round((y_src + R + 1.0) / D)) + PML_N + 1
+    nk = int(round(top / D)) + PML_N + 1
+    X = uniform_axis(3, 0.0, D)
+    Y = [_r(v) for v in uniform_axis(nj, 0.0, D)]
+    xc = _r(X[1])
+    src = (xc, _r(y_src), _r(hs))
+    rec = [(xc, _r(y_src + R * (k + 1) / N_REC), _r(hr)) for k in range(N_REC)]
+    P0 = RHO0 * C0 * C0 / GAMMA
+    common = dict(X=X, Y=Y, gauss_width=6 * D, time_domain=steps, gamma=GAMMA, P0=P0, c0=C0, pml_y=(2.0, 1000.0, 0),
+                  source=src, receiver=rec[0], dt=DT)
+    layer = max(2, int(round(p["layer_depth"] / D)))
+    ground = Case(Z=[_r(v) for v in uniform_axis(nk, 0.0, D)], pml_nodes=(0, 0, PML_N, PML_N, 0, PML_N),
+                  bc=(PML, POROUS, PML, PML, RIGID, RIGID),
+                  pore=(math.sqrt(p["tortuosity"]), p["porosity"], 10.0 ** p["log10_sigma"]),
+                  velocity_coef=_r(wind_gradient(p["ustar"], p["z0"])), velocity_method=1,
+                  pore_Z=[_r(v) for v in uniform_axis(layer + 2, -layer * D, D)], pore_dxyz=(D, D, D), **common)
+    hc = int(round(p["hill_height"] / D))
+    if hc >= 2:
+        wc = int(round(p["hill_halfwidth"] / D))
+        h, w = hc * D, wc * D
+        rad = (w * w + h * h) / (2 * h)
+        jc = int(round((y_src + R / 2) / D))
+        jc = min(max(jc, wc + PML_N + 1), nj - PML_N - 2 - wc)
+        ground.curve = (1, 0.0, _r(rad), xc, _r(Y[jc]), _r(h - rad)) + (0.0,) * 7 + (0,)
+        ground.hill_box = (X[1], X[1], Y[jc - wc], Y[jc + wc], 0.0, _r(h))
+    below = int(round(2.0 / D)) + PML_N
+    free = Case(Z=[_r(v) for v in uniform_axis(nk + below, -below * D, D)],
+                pml_nodes=(0, 0, PML_N, PML_N, PML_N, PML_N), bc=(PML, PML, PML, PML, RIGID, RIGID), **common)
+    return ground, free, rec
+
+
+def levels(traces: np.ndarray, device: int = 0) -> np.ndarray:
+    """Band levels [N_REC][len(BANDS)] dB of receiver traces [N_REC][nt]."""
+    return band_levels(traces, FFT_M, DT, BANDS, device=device)
+
+
+def solve(xs: np.ndarray, device: int = 0, precision: str = "f32", batch: int = 256, workdir: Optional[str] = None,
+          log=None) -> np.ndarray:
+    """Excess attenuation [n][N_REC * len(BANDS)] of the samples xs [n][11]
+    (NaN rows: grown traces): ground and free-field solves of up to `batch`
+    samples per ensemble, the samples sorted by their step count so that a
+    batch shares its horizon."""
+    xs = np.atleast_2d(np.asarray(xs, dtype=np.float64))
+    steps = np.array([steps_for(x) for x in xs])
+    order = np.argsort(steps, kind="stable")
+    out = np.zeros((len(xs), N_REC * len(BANDS)))
+    own = workdir is None
+    root = tempfile.mkdtemp(prefix="ea_") if own else workdir
+    try:
+        for b0 in range(0, len(xs), batch):
+            idx = order[b0:b0 + batch]
+            horizon = int(steps[idx].max())
+            t0 = time.perf_counter()
+            members, meta = [], []
+            for i in idx:
+                g, f, rec = cases(xs[i], horizon)
+                for kind, c in (("g", g), ("f", f)):
+                    dcase = c.write(os.path.join(root, f"s{i}{kind}"))
+                    a = Airpore(dcase, precision, device=device)
+                    a.set_receivers(rec)
+                    a.reset(horizon)
+                    members.append(a)
+                    meta.append((i, kind))
+            t1 = time.perf_counter()
+            with Ensemble(members) as e:
+                e.advance(horizon)
+                dev_ms = e.last_device_ms()
+            traces, bad = {}, set()
+            for a, (i, kind) in zip(members, meta):
+                traces[(i, kind)] = a.receivers(0, int(steps[i])).T.copy()  # [N_REC][own steps]
+                if grown(a.field("p")):
+                    bad.add(i)
+                a.close()
+            for i in idx:
+                tg, tf = traces[(i, "g")], traces[(i, "f")]
+                out[i] = np.nan if i in bad else (levels(tg, device) - levels(tf, device)).ravel()
+            for i, kind in meta:
+                shutil.rmtree(os.path.join(root, f"s{i}{kind}"), ignore_errors=True)
+            if log:
+                log(f"batch {b0 // batch}: {len(idx)} samples, horizon {horizon}, setup {t1 - t0:.1f} s, "
+                    f"device {dev_ms / 1e3:.2f} s")
+    finally:
+        if own:
+            shutil.rmtree(root, ignore_errors=True)
+    return out
+
+
+def generate(seed: int, n: int, path: str, device: int = 0, batch: int = 256, log=print) -> Dict[str, np.ndarray]:
+    """Draw n samples from `seed`, solve them and save {X, EA, seed} to path."""
+    xs = draw(seed, n)
+    t0 = time.perf_counter()
+    ea = solve(xs, device=device, batch=batch, log=log)
+    data = {"X": xs.astype(np.float32), "EA": ea.astype(np.float32), "seed": np.array(seed),
+            "seconds": np.array(time.perf_counter() - t0)}
+    np.savez_compressed(path, **data)
+    return data
