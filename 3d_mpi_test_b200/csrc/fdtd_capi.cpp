@@ -327,11 +327,11 @@ int fdtd_net_set_normalization(fdtd_net* h, const float* im, const float* is, co
     return guard([&] { h->n->set_normalization(im, is, om, os); });
 }
 
-int fdtd_net_train(fdtd_net* h, int steps, float lr, float lr_final, unsigned long long seed, int report,
-                   double* loss) {
+int fdtd_net_train(fdtd_net* h, int steps, float lr, float lr_final, float weight_decay, unsigned long long seed,
+                   int report, double* loss) {
     if (!h) return bad("null argument");
     return guard([&] {
-        const double l = h->n->train(steps, lr, lr_final, seed, report);
+        const double l = h->n->train(steps, lr, lr_final, seed, report, weight_decay);
         if (loss) *loss = l;
     });
 }

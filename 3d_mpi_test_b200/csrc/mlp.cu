@@ -205,10 +205,11 @@ __global__ void k_bias_grad(const __nv_bfloat16* __restrict__ dZT, int N, int B,
     if (lane == 0) db[n] = s;
 }
 
-// Adam (Kingma & Ba 2015) with bias correction; step t = *step + 1 and the
-// learning rate lr[*step] are read from device memory
+// Adam (Kingma & Ba 2015) with bias correction and decoupled weight decay
+// wd (Loshchilov & Hutter 2019); step t = *step + 1 and the learning rate
+// lr[*step] are read from device memory
 __global__ void k_adam(float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m, float* __restrict__ v,
-                       size_t n, const float* __restrict__ lr, const int* __restrict__ step) {
+                       size_t n, const float* __restrict__ lr, const int* __restrict__ step, float wd) {
     const size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x;
     if (i >= n) return;
     constexpr float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
@@ -220,7 +221,7 @@ __global__ void k_adam(float* __restrict__ w, const float* __restrict__ g, float
     const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
     m[i] = mi;
     v[i] = vi;
-    w[i] -= lr[*step] * (mi * c1) / (sqrtf(vi * c2) + eps);
+    w[i] -= lr[*step] * ((mi * c1) / (sqrtf(vi * c2) + eps) + wd * w[i]);
 }
 
 // bf16 copies W [N][K] and W^T [K][N] of an FP32 master
@@ -451,7 +452,9 @@ class NetImpl {
         upload_norm(nrm);
     }
 
-    double train(int steps, float lr0, float lr1, uint64_t seed, int report) {
+    double train(int steps, float lr0, float lr1, uint64_t seed, int report, float wd) {
+        if (!(wd >= 0.0f)) bad("weight decay must be >= 0");
+        wd_ = wd;
         if (!n_data_) bad("set_data first");
         if (steps < 1) bad("steps must be positive");
         ck(cudaSetDevice(dev_), "cudaSetDevice");
@@ -683,9 +686,10 @@ class NetImpl {
             for (int l = 0; l < L_; ++l) {
                 const size_t nw = static_cast<size_t>(Np_[l]) * Kp_[l];
                 k_adam<<<static_cast<unsigned>((nw + 255) / 256), 256, 0, s_>>>(
-                    W_[l].as<float>(), dW_[l].as<float>(), mW_[l].as<float>(), vW_[l].as<float>(), nw, lr_.as<float>(), step);
+                    W_[l].as<float>(), dW_[l].as<float>(), mW_[l].as<float>(), vW_[l].as<float>(), nw, lr_.as<float>(), step,
+                    wd_);
                 k_adam<<<(Np_[l] + 255) / 256, 256, 0, s_>>>(b_[l].as<float>(), db_[l].as<float>(), mb_[l].as<float>(),
-                                                              vb_[l].as<float>(), Np_[l], lr_.as<float>(), step);
+                                                              vb_[l].as<float>(), Np_[l], lr_.as<float>(), step, 0.0f);
                 ck(cudaGetLastError(), "adam");
                 n += 2;
             }
@@ -712,6 +716,7 @@ class NetImpl {
     cudaEvent_t e0_ = nullptr, e1_ = nullptr;
     cudaGraphExec_t graph_ = nullptr;
     int per_step_ = 0;
+    float wd_ = 0.0f;
     long long launches_ = 0;
     double last_ms_ = 0;
 };
@@ -727,8 +732,8 @@ void Net::get_normalization(float* a, float* b, float* c, float* d) const { impl
 void Net::set_normalization(const float* a, const float* b, const float* c, const float* d) {
     impl_->set_normalization(a, b, c, d);
 }
-double Net::train(int steps, float lr, float lr_final, uint64_t seed, int report) {
-    return impl_->train(steps, lr, lr_final, seed, report);
+double Net::train(int steps, float lr, float lr_final, uint64_t seed, int report, float weight_decay) {
+    return impl_->train(steps, lr, lr_final, seed, report, weight_decay);
 }
 double Net::gradients(float* grad) { return impl_->gradients(grad); }
 void Net::predict(const float* X, int n, float* Y) { impl_->predict(X, n, Y); }

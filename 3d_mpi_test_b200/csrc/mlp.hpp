@@ -38,9 +38,10 @@ class Net {
     void set_data(const float* X, const float* T, int n);
     void get_normalization(float* in_mean, float* in_std, float* out_mean, float* out_std) const;
     void set_normalization(const float* in_mean, const float* in_std, const float* out_mean, const float* out_std);
-    // Adam steps on shuffled minibatches; returns the mean loss (normalised
-    // MSE) of the last `report` steps
-    double train(int steps, float lr, float lr_final, uint64_t seed, int report);
+    // Adam steps on shuffled minibatches (decoupled weight decay on the
+    // weights); returns the mean loss (normalised MSE) of the last `report`
+    // steps
+    double train(int steps, float lr, float lr_final, uint64_t seed, int report, float weight_decay);
     // One forward + backward on the first `batch` rows of the data without
     // an update: loss and the gradients of every parameter (same order as
     // get_params)

@@ -36,7 +36,7 @@ def _declare(L) -> None:
         "fdtd_net_set_data": ([vp, _FP, _FP, i], i),
         "fdtd_net_get_normalization": ([vp, _FP, _FP, _FP, _FP], i),
         "fdtd_net_set_normalization": ([vp, _FP, _FP, _FP, _FP], i),
-        "fdtd_net_train": ([vp, i, f, f, ull, i, d], i),
+        "fdtd_net_train": ([vp, i, f, f, f, ull, i, d], i),
         "fdtd_net_gradients": ([vp, _FP, d], i),
         "fdtd_net_predict": ([vp, _FP, i, _FP], i),
         "fdtd_net_predict_device": ([vp, vp, i, vp, vp], i),
@@ -146,9 +146,11 @@ class Net:
         a, b, c, d = _f32(in_mean), _f32(in_std), _f32(out_mean), _f32(out_std)
         _check(self._L, self._L.fdtd_net_set_normalization(self._h, _fp(a), _fp(b), _fp(c), _fp(d)))
 
-    def train(self, steps: int, lr: float = 1e-3, lr_final: float = 1e-5, seed: int = 0, report: int = 100) -> float:
+    def train(self, steps: int, lr: float = 1e-3, lr_final: float = 1e-5, seed: int = 0, report: int = 100,
+              weight_decay: float = 0.0) -> float:
         loss = ctypes.c_double()
-        _check(self._L, self._L.fdtd_net_train(self._h, steps, lr, lr_final, seed, report, ctypes.byref(loss)))
+        _check(self._L, self._L.fdtd_net_train(self._h, steps, lr, lr_final, weight_decay, seed, report,
+                                               ctypes.byref(loss)))
         return loss.value
 
     def gradients(self) -> Tuple[float, np.ndarray]:
@@ -172,3 +174,84 @@ class Net:
         n, ms = ctypes.c_longlong(), ctypes.c_double()
         _check(self._L, self._L.fdtd_net_info(self._h, ctypes.byref(n), ctypes.byref(ms)))
         return {"launches": n.value, "last_device_ms": ms.value}
+
+
+class Surrogate:
+    """Ensemble of networks that answers excess-attenuation queries, with
+    the FDTD solver as its fallback.
+
+    Inputs: the 11 parameters of ``surrogate_data.PARAMS`` (flow
+    resistivity as log10, porosity, tortuosity, layer depth, source and
+    receiver heights, range, hill height and half-width, u*, z0). Outputs:
+    excess attenuation [n_rec][n_band] in dB (``surrogate_data`` layout).
+    Each member is trained on a bootstrap resample of the data from its own
+    initialisation. A query is answered by the FDTD solver instead of the
+    networks when it lies outside the training hull (the per-parameter
+    range of the training inputs) or when the members disagree: the root
+    mean square over the outputs of the standard deviation across members
+    exceeds ``tol_db``.
+    """
+
+    def __init__(self, members: int = 5, width: int = 512, hidden: int = 4, batch: int = 256, seed: int = 0,
+                 device: int = 0, lib_path: Optional[str] = None):
+        self.members, self.width, self.hidden, self.batch = members, width, hidden, batch
+        self.seed, self.device, self._lib_path = seed, device, lib_path
+        self.nets = []
+        self.lo = self.hi = None
+
+    def close(self) -> None:
+        for n in self.nets:
+            n.close()
+        self.nets = []
+
+    def fit(self, X, EA, steps: int = 6000, lr: float = 2e-3, lr_final: float = 2e-5,
+            weight_decay: float = 0.05) -> list:
+        """Trains every member; returns their final training losses (mean
+        squared error of the normalised outputs)."""
+        X = np.asarray(X, np.float32)
+        EA = np.asarray(EA, np.float32)
+        ok = np.isfinite(EA).all(axis=1) & np.isfinite(X).all(axis=1)
+        X, EA = X[ok], EA[ok]
+        self.lo, self.hi = X.min(axis=0), X.max(axis=0)
+        self.close()
+        losses = []
+        rng = np.random.default_rng(self.seed)
+        for m in range(self.members):
+            net = Net(X.shape[1], EA.shape[1], width=self.width, hidden=self.hidden, batch=self.batch,
+                      seed=self.seed * 1000 + m, device=self.device, lib_path=self._lib_path)
+            pick = rng.integers(0, len(X), len(X))  # bootstrap resample
+            net.set_data(X[pick], EA[pick])
+            losses.append(net.train(steps, lr=lr, lr_final=lr_final, seed=self.seed * 1000 + m, report=100,
+                                    weight_decay=weight_decay))
+            self.nets.append(net)
+        return losses
+
+    def in_hull(self, X) -> np.ndarray:
+        X = np.atleast_2d(np.asarray(X, np.float32))
+        return np.all((X >= self.lo) & (X <= self.hi), axis=1)
+
+    def predict(self, X) -> Tuple[np.ndarray, np.ndarray]:
+        """Member mean [n][outputs] and the disagreement [n] (root mean
+        square over the outputs of the standard deviation across members, dB)."""
+        ys = np.stack([n.predict(X) for n in self.nets])
+        return ys.mean(axis=0), np.sqrt(ys.var(axis=0).mean(axis=1))
+
+    def query(self, X, tol_db: float = 1.0, fdtd=None) -> Tuple[np.ndarray, np.ndarray]:
+        """Answers [n][outputs] and the source of each answer: 0 network,
+        1 FDTD (outside the hull), 2 FDTD (members disagree). ``fdtd`` maps
+        inputs [k][11] to excess attenuation [k][outputs]; the default runs
+        ``surrogate_data.solve``."""
+        X = np.atleast_2d(np.asarray(X, np.float32))
+        y, spread = self.predict(X)
+        src = np.zeros(len(X), np.int8)
+        src[spread > tol_db] = 2
+        src[~self.in_hull(X)] = 1
+        fall = np.nonzero(src)[0]
+        if len(fall):
+            if fdtd is None:
+                from .surrogate_data import solve
+
+                def fdtd(xs):
+                    return solve(xs, device=self.device)
+            y[fall] = fdtd(X[fall])
+        return y, src

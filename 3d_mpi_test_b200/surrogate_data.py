@@ -213,3 +213,31 @@ def generate(seed: int, n: int, path: str, device: int = 0, batch: int = 256, lo
             "seconds": np.array(time.perf_counter() - t0)}
     np.savez_compressed(path, **data)
     return data
+
+
+DATASET = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "ea_dataset.npz")
+DATASET_PARTS = ((2024, 5000), (2025, 10000))  # (seed, samples) of the committed dataset
+N_TRAIN = 13500  # the last 1500 samples of the committed dataset are held out
+
+
+def build_dataset(path: str = DATASET, device: int = 0, log=print) -> None:
+    """Regenerates the committed dataset: generate() for every part of
+    DATASET_PARTS, concatenated; X float32, EA float16 (0.06 dB at most)."""
+    parts = [generate(s, n, path + f".part{s}.npz", device=device, log=log) for s, n in DATASET_PARTS]
+    np.savez_compressed(path, X=np.concatenate([p["X"] for p in parts]).astype(np.float32),
+                        EA=np.concatenate([p["EA"] for p in parts]).astype(np.float16),
+                        seeds=np.array([s for s, _ in DATASET_PARTS]), counts=np.array([n for _, n in DATASET_PARTS]),
+                        seconds=np.array([float(p["seconds"]) for p in parts]))
+    for s, _ in DATASET_PARTS:
+        os.remove(path + f".part{s}.npz")
+
+
+def load_dataset(path: str = DATASET):
+    """(X_train, EA_train, X_test, EA_test) as float32; the first N_TRAIN
+    samples train, the rest are held out; rows of grown solves (NaN) are
+    dropped."""
+    d = np.load(path)
+    X, EA = d["X"].astype(np.float32), d["EA"].astype(np.float32)
+    ok = np.isfinite(EA).all(axis=1)
+    tr = np.arange(len(X)) < N_TRAIN
+    return X[ok & tr], EA[ok & tr], X[ok & ~tr], EA[ok & ~tr]

@@ -18,6 +18,12 @@ reference's MPI decomposition has no MPI here), aggregate throughput.
 Multi-GPU: replicas only -- each rank runs its own independent solve, no
 collective on the data path; value = all ranks' cell updates / max time.
 
+The domain line carries a ``surrogate`` section (skip with
+``--no-surrogate``; alone with ``--workload surrogate``): a 5-network bf16
+ensemble trained on the committed FDTD dataset, its held-out error and
+fallback rate, its inference throughput on 1 M queries in HBM against the
+bf16 tensor roofline, and the speed-up over the FDTD solves it replaces.
+
 ``--workload ensemble`` measures the batched ensemble instead: ``--members``
 independent FP32 solves drawn by casegen.ensemble_member (seed = rank),
 stepped by batched marching launches in a graph-captured loop, tile rule
@@ -308,6 +314,85 @@ def run_ensemble(args, rank, world, local_rank):
     }
 
 
+def bf16_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["bf16_tflops"]), "measured (burst cuBLAS bf16)"
+    return 1590.0, "fallback"
+
+
+def run_surrogate(queries: int = 1_000_000, members: int = 5, steps: int = 6000, device: int = 0) -> dict:
+    """The learned surrogate on this GPU: a `members`-network bf16 ensemble
+    trained on the committed FDTD dataset (3d_mpi_test_b200/data), its
+    held-out error and FDTD fallback rate, its inference throughput on
+    `queries` seeded queries resident in HBM (CUDA events), the end-to-end
+    rate from host arrays, and the time per query of the FDTD solves it
+    replaces (ground + free-field pair through the batched ensemble)."""
+    import numpy as np
+    import torch
+
+    sur = importlib.import_module("3d_mpi_test_b200.surrogate")
+    sd = importlib.import_module("3d_mpi_test_b200.surrogate_data")
+    Xtr, Etr, Xte, Ete = sd.load_dataset()
+    s = sur.Surrogate(members=members, seed=1)
+    t0 = time.perf_counter()
+    losses = s.fit(Xtr, Etr, steps=steps)
+    train_s = time.perf_counter() - t0
+    train_ms = sum(n.info()["last_device_ms"] for n in s.nets)
+    y, spread = s.predict(Xte)
+    err = np.abs(y - Ete)
+    kept = spread <= 1.0
+    per_band = err.reshape(len(Xte), sd.N_REC, len(sd.BANDS)).mean(axis=(0, 1))
+    # inference: queries resident in HBM, every member, CUDA events inside the library
+    Xq = sd.draw(99, queries).astype(np.float32)
+    xd = torch.from_numpy(Xq).cuda(device)
+    yd = torch.empty((queries, Etr.shape[1]), dtype=torch.float32, device=f"cuda:{device}")
+    for n in s.nets:
+        n.predict_device(xd.data_ptr(), 4096, yd.data_ptr())  # warm-up
+    l0 = sum(n.info()["launches"] for n in s.nets)
+    ms = 0.0
+    for n in s.nets:
+        n.predict_device(xd.data_ptr(), queries, yd.data_ptr())
+        ms += n.info()["last_device_ms"]
+    launches = sum(n.info()["launches"] for n in s.nets) - l0
+    width, K0, NO = 512, 64, 256  # padded GEMM shapes of one member
+    flop_padded = 2.0 * (K0 * width + 3 * width * width + width * NO)
+    flop_alg = 2.0 * (11 * width + 3 * width * width + width * Etr.shape[1])
+    peak, peak_kind = bf16_peak()
+    tflops = members * queries * flop_padded / (ms * 1e-3) / 1e12
+    # end to end from host arrays: H2D of the queries, D2H of the answers
+    t0 = time.perf_counter()
+    s.predict(Xq)
+    e2e_s = time.perf_counter() - t0
+    # the method without the network: an FDTD solve pair per query
+    nf = 16
+    t0 = time.perf_counter()
+    sd.solve(Xte[:nf])
+    fdtd_s = (time.perf_counter() - t0) / nf
+    s.close()
+    return {
+        "members": members, "layers": "11 -> 4 x 512 ReLU -> 136 (17 bands x 8 receivers), bf16 weights, FP32 accumulate",
+        "train": {"samples": int(len(Xtr)), "steps_per_member": steps, "batch": 256, "wall_s": round(train_s, 2),
+                  "device_ms": round(train_ms, 1), "final_loss_normalised": [round(float(v), 5) for v in losses]},
+        "held_out": {"samples": int(len(Xte)), "mae_db": round(float(err.mean()), 3),
+                     "rmse_db": round(float(np.sqrt((err ** 2).mean())), 3),
+                     "mae_db_per_band": [round(float(v), 2) for v in per_band],
+                     "fdtd_fallback_fraction_at_1db": round(float(1 - kept.mean()), 3),
+                     "mae_db_answered_by_network": round(float(err[kept].mean()), 3) if kept.any() else None},
+        "inference": {"queries": queries, "queries_per_s": round(queries / (ms * 1e-3), 1), "ms": round(ms, 3),
+                      "gpu_launches": int(launches),
+                      "roofline": {"bound": "tensor", "achieved": round(tflops, 1), "peak": peak, "unit": "TFLOP/s",
+                                   "frac": round(tflops / peak, 4), "peak_kind": peak_kind,
+                                   "flop_per_query_member_padded": flop_padded,
+                                   "flop_per_query_member_algorithmic": flop_alg}},
+        "e2e_queries_per_s": round(queries / e2e_s, 1),
+        "fdtd_s_per_query": round(fdtd_s, 5),
+        "speedup_vs_fdtd": round(fdtd_s / (e2e_s / queries), 1),
+    }
+
+
 def run_gpu(args, rank, world, local_rank):
     import numpy as np
     import torch
@@ -430,6 +515,8 @@ def run_gpu(args, rank, world, local_rank):
         "gpu_launches": int(f32["launches"]),
         "clocks": f32["clocks"],
     }
+    if world == 1 and not args.no_surrogate:
+        line["surrogate"] = run_surrogate(device=local_rank)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(case_dir_for_cpu(), cells)
     return line
@@ -477,7 +564,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tile", default="", help="rows,planes,threads,vector-width,ring-stages of the marching kernel (default: autotune)")
-    ap.add_argument("--workload", default="domain", choices=["domain", "ensemble"])
+    ap.add_argument("--workload", default="domain", choices=["domain", "ensemble", "surrogate"])
+    ap.add_argument("--no-surrogate", action="store_true", help="skip the surrogate section of the domain line")
     ap.add_argument("--members", type=int, default=256, help="ensemble members (--workload ensemble)")
     ap.add_argument("--check-members", type=int, default=-1, help="members checked against FP64 (-1: all)")
     ap.add_argument("--check-steps", type=int, default=200)
@@ -503,6 +591,8 @@ def main():
     try:
         if args.workload == "ensemble":
             line = run_ensemble(args, rank, world, local_rank)
+        elif args.workload == "surrogate":
+            line = {"workload": "surrogate", **run_surrogate(device=local_rank)} if rank == 0 else None
         else:
             line = run_gpu(args, rank, world, local_rank)
     finally:

@@ -55,10 +55,10 @@ int fdtd_net_set_normalization(fdtd_net *h, const float *in_mean, const float *i
                                const float *out_std);
 
 /* steps Adam updates on shuffled minibatches (cosine learning rate lr ->
- * lr_final, minibatch order from seed); *loss = mean normalised MSE of the
- * last `report` steps */
-int fdtd_net_train(fdtd_net *h, int steps, float lr, float lr_final, unsigned long long seed, int report,
-                   double *loss);
+ * lr_final, decoupled weight decay on the weights, minibatch order from
+ * seed); *loss = mean normalised MSE of the last `report` steps */
+int fdtd_net_train(fdtd_net *h, int steps, float lr, float lr_final, float weight_decay, unsigned long long seed,
+                   int report, double *loss);
 
 /* forward + backward on the first `batch` data rows without an update:
  * gradients of every parameter (fdtd_net_get_params order) and the loss */
