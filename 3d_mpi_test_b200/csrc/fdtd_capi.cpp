@@ -354,6 +354,18 @@ int fdtd_net_predict_device(fdtd_net* h, const float* X, int n, float* Y, void* 
     return guard([&] { h->n->predict_device(X, n, Y, stream); });
 }
 
+int fdtd_net_ensemble_predict(fdtd_net* const* nets, int members, const float* X, int n, float* mean, float* spread) {
+    if (!nets || members < 1 || (n > 0 && (!X || !mean || !spread))) return bad("bad ensemble arguments");
+    return guard([&] {
+        std::vector<fdtd::mlp::Net*> v;
+        for (int m = 0; m < members; ++m) {
+            if (!nets[m]) throw fdtd::SolverError{FDTD_ERR_ARG, "null ensemble member"};
+            v.push_back(nets[m]->n);
+        }
+        fdtd::mlp::ensemble_predict(v.data(), members, X, n, mean, spread);
+    });
+}
+
 int fdtd_net_info(const fdtd_net* h, long long* launches, double* last_ms) {
     if (!h) return bad("null argument");
     if (launches) *launches = h->n->launches();

@@ -237,6 +237,32 @@ __global__ void k_cast(const float* __restrict__ W, int N, int K, __nv_bfloat16*
 
 __global__ void k_next_step(int* step) { *step += 1; }
 
+// one warp per query: mean over `members` predictions Y [members][n][nout]
+// and the root mean square over the outputs of their standard deviation
+__global__ void k_ensemble_stats(const float* __restrict__ Y, int members, int n, int nout, float* __restrict__ mean,
+                                 float* __restrict__ spread) {
+    const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (row >= n) return;
+    const size_t plane = static_cast<size_t>(n) * nout;
+    float var = 0.0f;
+    for (int c = lane; c < nout; c += 32) {
+        const size_t o = static_cast<size_t>(row) * nout + c;
+        float s = 0.0f;
+        for (int m = 0; m < members; ++m) s += Y[m * plane + o];
+        const float mu = s / members;
+        float q = 0.0f;
+        for (int m = 0; m < members; ++m) {
+            const float d = Y[m * plane + o] - mu;
+            q += d * d;
+        }
+        mean[o] = mu;
+        var += q / members;
+    }
+    for (int k = 16; k > 0; k >>= 1) var += __shfl_xor_sync(0xffffffffu, var, k);
+    if (lane == 0) spread[row] = sqrtf(var / nout);
+}
+
 // denormalised outputs of the first `valid` rows: out [valid][nout]
 __global__ void k_denorm(const float* __restrict__ Y, int NO, int valid, int nout, const float* __restrict__ mean,
                          const float* __restrict__ sd, float* __restrict__ out) {
@@ -576,6 +602,9 @@ class NetImpl {
 
     long long launches() const { return launches_; }
     double last_ms() const { return last_ms_; }
+    int n_in() const { return nin_; }
+    int n_out() const { return nout_; }
+    int device() const { return dev_; }
 
    private:
     static constexpr int kChunk = 65536;  // inference rows per pass
@@ -741,6 +770,44 @@ void Net::predict_device(const float* X, int n, float* Y, void* stream) {
     impl_->predict_device(X, n, Y, static_cast<cudaStream_t>(stream));
 }
 long long Net::launches() const { return impl_->launches(); }
+int Net::n_in() const { return impl_->n_in(); }
+int Net::n_out() const { return impl_->n_out(); }
+int Net::device() const { return impl_->device(); }
+
+void ensemble_predict(Net* const* nets, int members, const float* X, int n, float* mean, float* spread) {
+    if (members < 1 || !nets || n < 0) bad("ensemble: need at least one network and n >= 0");
+    const int nin = nets[0]->n_in(), nout = nets[0]->n_out(), dev = nets[0]->device();
+    for (int m = 0; m < members; ++m)
+        if (!nets[m] || nets[m]->n_in() != nin || nets[m]->n_out() != nout || nets[m]->device() != dev)
+            bad("ensemble members must share inputs, outputs and device");
+    if (n == 0) return;
+    ck(cudaSetDevice(dev), "cudaSetDevice");
+    const int chunk = std::min(n, 1 << 18);
+    Buf xd(sizeof(float) * static_cast<size_t>(chunk) * nin), yd(sizeof(float) * static_cast<size_t>(chunk) * nout * members),
+        md(sizeof(float) * static_cast<size_t>(chunk) * nout), sd(sizeof(float) * chunk);
+    cudaStream_t s;
+    ck(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
+    try {
+        for (int r0 = 0; r0 < n; r0 += chunk) {
+            const int c = std::min(chunk, n - r0);
+            ck(cudaMemcpyAsync(xd.p, X + static_cast<size_t>(r0) * nin, sizeof(float) * c * nin, cudaMemcpyHostToDevice,
+                               s), "inputs");
+            for (int m = 0; m < members; ++m)
+                nets[m]->predict_device(xd.as<float>(), c, yd.as<float>() + static_cast<size_t>(m) * c * nout, s);
+            k_ensemble_stats<<<(c + 7) / 8, 256, 0, s>>>(yd.as<float>(), members, c, nout, md.as<float>(), sd.as<float>());
+            ck(cudaGetLastError(), "ensemble statistics");
+            ck(cudaMemcpyAsync(mean + static_cast<size_t>(r0) * nout, md.p, sizeof(float) * c * nout,
+                               cudaMemcpyDeviceToHost, s), "outputs");
+            ck(cudaMemcpyAsync(spread + r0, sd.p, sizeof(float) * c, cudaMemcpyDeviceToHost, s), "outputs");
+            ck(cudaStreamSynchronize(s), "ensemble");
+        }
+    } catch (...) {
+        cudaStreamSynchronize(s);
+        cudaStreamDestroy(s);
+        throw;
+    }
+    cudaStreamDestroy(s);
+}
 double Net::last_device_ms() const { return impl_->last_ms(); }
 
 }  // namespace mlp

@@ -52,10 +52,20 @@ class Net {
     void predict_device(const float* X, int n, float* Y, void* stream);
     long long launches() const;
     double last_device_ms() const;
+    int n_in() const;
+    int n_out() const;
+    int device() const;
 
    private:
     std::unique_ptr<NetImpl> impl_;
 };
+
+// Answer of an ensemble of networks with the same inputs and outputs on one
+// device, for host inputs X [n][n_in]: the members' mean [n][n_out] and
+// their disagreement [n] (root mean square over the outputs of the standard
+// deviation across members), host buffers. The reduction runs on the
+// device, so only the mean and the disagreement cross back to the host.
+void ensemble_predict(Net* const* nets, int members, const float* X, int n, float* mean, float* spread);
 
 }  // namespace mlp
 }  // namespace fdtd

@@ -38,7 +38,7 @@ namespace mlp {
 
 constexpr int kTileM = 128;  // rows per CTA (one tcgen05.mma M)
 constexpr int kTileK = 64;   // K elements per stage: 128 bytes of bf16, one swizzle atom row
-constexpr int kStages = 4;
+constexpr int kStages = 3;  // 3 stages (99 KB) let two CTAs share an SM: one's epilogue overlaps the other's MMAs
 constexpr long long kSpin = 1LL << 24;
 
 enum Epilogue : int {
@@ -160,7 +160,7 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
 }
 
 template <int BN, int EPI>
-__global__ void __launch_bounds__(128, 1)
+__global__ void __launch_bounds__(128, 2)
     k_gemm_tn(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, const GemmArgs g) {
     static_assert(BN == 64 || BN == 128 || BN == 256, "tile width");
     extern __shared__ unsigned char smem_raw[];

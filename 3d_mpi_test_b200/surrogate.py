@@ -41,6 +41,7 @@ def _declare(L) -> None:
         "fdtd_net_predict": ([vp, _FP, i, _FP], i),
         "fdtd_net_predict_device": ([vp, vp, i, vp, vp], i),
         "fdtd_net_info": ([vp, ll, d], i),
+        "fdtd_net_ensemble_predict": ([ctypes.POINTER(vp), i, _FP, i, _FP, _FP], i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -233,8 +234,17 @@ class Surrogate:
     def predict(self, X) -> Tuple[np.ndarray, np.ndarray]:
         """Member mean [n][outputs] and the disagreement [n] (root mean
         square over the outputs of the standard deviation across members, dB)."""
-        ys = np.stack([n.predict(X) for n in self.nets])
-        return ys.mean(axis=0), np.sqrt(ys.var(axis=0).mean(axis=1))
+        if not self.nets or not isinstance(self.nets[0], Net):  # stand-in members (tests)
+            ys = np.stack([n.predict(X) for n in self.nets])
+            return ys.mean(axis=0), np.sqrt(ys.var(axis=0).mean(axis=1))
+        X = _f32(np.atleast_2d(X))
+        net0 = self.nets[0]
+        mean = np.empty((X.shape[0], net0.n_out), np.float32)
+        spread = np.empty(X.shape[0], np.float32)
+        arr = (ctypes.c_void_p * len(self.nets))(*[n._h.value for n in self.nets])
+        _check(net0._L, net0._L.fdtd_net_ensemble_predict(arr, len(self.nets), _fp(X), X.shape[0], _fp(mean),
+                                                          _fp(spread)))
+        return mean, spread
 
     def query(self, X, tol_db: float = 1.0, fdtd=None) -> Tuple[np.ndarray, np.ndarray]:
         """Answers [n][outputs] and the source of each answer: 0 network,

@@ -69,6 +69,13 @@ int fdtd_net_predict(fdtd_net *h, const float *X, int n, float *Y);
 /* the same on device buffers, on a cudaStream_t (synchronises it) */
 int fdtd_net_predict_device(fdtd_net *h, const float *X, int n, float *Y, void *stream);
 
+/* answer of an ensemble of networks (same n_in, n_out and device): the
+ * members' mean [n][n_out] and their disagreement [n] -- the root mean
+ * square over the outputs of the standard deviation across members --
+ * for host inputs X [n][n_in]; the reduction runs on the device */
+int fdtd_net_ensemble_predict(fdtd_net *const *nets, int members, const float *X, int n, float *mean,
+                              float *spread);
+
 /* kernel launches so far and device milliseconds of the last train /
  * predict call */
 int fdtd_net_info(const fdtd_net *h, long long *launches, double *last_ms);

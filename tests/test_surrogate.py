@@ -121,3 +121,12 @@ def test_network_answers_faster_than_fdtd(trained):
     s.predict(Xq)
     net_per_query = (time.perf_counter() - t0) / len(Xq)
     assert fdtd_per_query / net_per_query > 1000, (fdtd_per_query, net_per_query)
+
+
+@pytest.mark.gpu
+def test_device_ensemble_reduction_matches_members(trained):
+    s, _, Xte, _ = trained
+    mean, spread = s.predict(Xte[:300])
+    ys = np.stack([n.predict(Xte[:300]) for n in s.nets]).astype(np.float64)
+    np.testing.assert_allclose(mean, ys.mean(axis=0), rtol=0, atol=1e-4)
+    np.testing.assert_allclose(spread, np.sqrt(ys.var(axis=0).mean(axis=1)), rtol=1e-4, atol=1e-4)
