@@ -516,7 +516,7 @@ def run_gpu(args, rank, world, local_rank):
         "clocks": f32["clocks"],
     }
     if world == 1 and not args.no_surrogate:
-        line["surrogate"] = run_surrogate(device=local_rank)
+        line["surrogate"] = run_surrogate(args.sur_queries, steps=args.sur_train_steps, device=local_rank)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(case_dir_for_cpu(), cells)
     return line
@@ -566,6 +566,8 @@ def main():
     ap.add_argument("--tile", default="", help="rows,planes,threads,vector-width,ring-stages of the marching kernel (default: autotune)")
     ap.add_argument("--workload", default="domain", choices=["domain", "ensemble", "surrogate"])
     ap.add_argument("--no-surrogate", action="store_true", help="skip the surrogate section of the domain line")
+    ap.add_argument("--sur-queries", type=int, default=1_000_000, help="surrogate inference queries")
+    ap.add_argument("--sur-train-steps", type=int, default=6000, help="training steps per surrogate member")
     ap.add_argument("--members", type=int, default=256, help="ensemble members (--workload ensemble)")
     ap.add_argument("--check-members", type=int, default=-1, help="members checked against FP64 (-1: all)")
     ap.add_argument("--check-steps", type=int, default=200)
@@ -592,7 +594,8 @@ def main():
         if args.workload == "ensemble":
             line = run_ensemble(args, rank, world, local_rank)
         elif args.workload == "surrogate":
-            line = {"workload": "surrogate", **run_surrogate(device=local_rank)} if rank == 0 else None
+            line = {"workload": "surrogate", **run_surrogate(args.sur_queries, steps=args.sur_train_steps,
+                                                              device=local_rank)} if rank == 0 else None
         else:
             line = run_gpu(args, rank, world, local_rank)
     finally:
