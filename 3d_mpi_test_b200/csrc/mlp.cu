@@ -70,9 +70,8 @@ CUtensorMap bf16_map(const void* base, int rows, int cols, int box_rows) {
 // one GEMM with fixed operands, ready to launch (also inside a graph)
 struct Plan {
     CUtensorMap a, b;
-    GemmArgs g;
+    GemmArgs g;  // g.M may be lowered (to a multiple of 128) before a launch
     int bn = 128, epi = 0;
-    dim3 grid;
 };
 
 template <int BN, int EPI>
@@ -118,19 +117,31 @@ Plan make_plan(int epi, int M, int N, int K, const void* A, const void* B, const
     p.b = bf16_map(B, N, K, p.bn);
     p.g = GemmArgs{M, N, K, bias, static_cast<const __nv_bfloat16*>(mask), ldm, out, ldo,
                    static_cast<__nv_bfloat16*>(outT), ldt, status};
-    p.grid = dim3(M / kTileM, N / p.bn, 1);
     return p;
 }
 
+int sm_count() {
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        ck(cudaGetDevice(&dev), "cudaGetDevice");
+        ck(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev), "SM count");
+    }
+    return n;
+}
+
+// persistent launch: one CTA per SM, at most one per tile
 template <int BN>
 void launch_bn(const Plan& p, cudaStream_t s) {
     const size_t smem = gemm_smem_bytes<BN>();
+    const int tiles = (p.g.M / kTileM) * (p.g.N / BN);
+    const dim3 grid(std::min(tiles, sm_count())), blk(kGemmThreads);
     switch (p.epi) {
-        case kEpiF32: k_gemm_tn<BN, kEpiF32><<<p.grid, 128, smem, s>>>(p.a, p.b, p.g); break;
-        case kEpiBiasReluT: k_gemm_tn<BN, kEpiBiasReluT><<<p.grid, 128, smem, s>>>(p.a, p.b, p.g); break;
-        case kEpiBiasF32: k_gemm_tn<BN, kEpiBiasF32><<<p.grid, 128, smem, s>>>(p.a, p.b, p.g); break;
-        case kEpiReluGradT: k_gemm_tn<BN, kEpiReluGradT><<<p.grid, 128, smem, s>>>(p.a, p.b, p.g); break;
-        default: k_gemm_tn<BN, kEpiBiasRelu><<<p.grid, 128, smem, s>>>(p.a, p.b, p.g); break;
+        case kEpiF32: k_gemm_tn<BN, kEpiF32><<<grid, blk, smem, s>>>(p.a, p.b, p.g); break;
+        case kEpiBiasReluT: k_gemm_tn<BN, kEpiBiasReluT><<<grid, blk, smem, s>>>(p.a, p.b, p.g); break;
+        case kEpiBiasF32: k_gemm_tn<BN, kEpiBiasF32><<<grid, blk, smem, s>>>(p.a, p.b, p.g); break;
+        case kEpiReluGradT: k_gemm_tn<BN, kEpiReluGradT><<<grid, blk, smem, s>>>(p.a, p.b, p.g); break;
+        default: k_gemm_tn<BN, kEpiBiasRelu><<<grid, blk, smem, s>>>(p.a, p.b, p.g); break;
     }
     ck(cudaGetLastError(), "GEMM launch");
 }
@@ -582,7 +593,7 @@ class NetImpl {
             ++launches_;
             for (int l = 0; l < L_; ++l) {
                 Plan p = infer_[l];
-                p.grid.x = rows / kTileM;
+                p.g.M = rows;
                 launch(p, s);
                 ++launches_;
             }

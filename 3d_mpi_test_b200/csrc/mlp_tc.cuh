@@ -8,19 +8,20 @@
 // stores, optionally also the transposed bf16 result that the backward pass
 // reads as its next operand).
 //
-// One CTA computes a 128 x BN tile with 128 threads:
+// A persistent CTA of 192 threads per SM walks 128 x BN output tiles:
 //   - warp 0, one lane: TMA producer. Each K block of 64 elements of A
-//     (128 rows) and B (BN rows) lands in a shared-memory stage through
-//     cp.async.bulk.tensor with the 128-byte swizzle, completing on the
-//     stage's "full" mbarrier;
+//     (128 rows) and B (BN rows) lands in a shared-memory stage (a 4-stage
+//     ring) through cp.async.bulk.tensor with the 128-byte swizzle,
+//     completing on the stage's "full" mbarrier;
 //   - warp 1, one lane: MMA issuer. Four tcgen05.mma (K = 16 each) per stage
 //     read both operands from shared memory through matrix descriptors and
-//     accumulate into a 128 x BN FP32 tile in tensor memory; tcgen05.commit
-//     frees the stage ("empty" mbarrier) once they complete, and a last
-//     commit signals "done";
-//   - all four warps: epilogue. Warp w owns accumulator rows 32w .. 32w+31
-//     (tensor-memory lanes), reads them with tcgen05.ld and stores.
-// Tensor memory (BN columns) is allocated and released by warp 0. Every
+//     accumulate into one of two 128 x BN FP32 tiles in tensor memory;
+//     tcgen05.commit frees the stage ("empty") once they complete and hands
+//     the finished accumulator to the epilogue;
+//   - warps 2..5: epilogue. Each reads its quarter of the accumulator rows
+//     with tcgen05.ld, stores, and hands the accumulator back, while the MMA
+//     warp already fills the other one.
+// Tensor memory (2 BN columns) is allocated and released by warp 1. Every
 // mbarrier wait is bounded; a wait that runs out sets bit 0 of *status and
 // the kernel finishes without hanging.
 //
@@ -38,7 +39,8 @@ namespace mlp {
 
 constexpr int kTileM = 128;  // rows per CTA (one tcgen05.mma M)
 constexpr int kTileK = 64;   // K elements per stage: 128 bytes of bf16, one swizzle atom row
-constexpr int kStages = 3;  // 3 stages (99 KB) let two CTAs share an SM: one's epilogue overlaps the other's MMAs
+constexpr int kStages = 4;
+constexpr int kGemmThreads = 192;  // warp 0 TMA, warp 1 MMA, warps 2..5 epilogue
 constexpr long long kSpin = 1LL << 24;
 
 enum Epilogue : int {
@@ -62,8 +64,8 @@ struct GemmArgs {
 };
 
 // shared memory: stages of A (128 x 64 bf16 = 16 KB) and B (BN x 64 bf16),
-// 1024-byte aligned for the 128-byte swizzle, then the mbarriers and the
-// tensor-memory address slot
+// 1024-byte aligned for the 128-byte swizzle, then the mbarriers (stage
+// full / empty, accumulator full / empty) and the tensor-memory address slot
 template <int BN>
 constexpr size_t gemm_smem_bytes() {
     return 1024 + kStages * (kTileM * kTileK * 2 + BN * kTileK * 2) + 256;
@@ -159,10 +161,69 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
     for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
 }
 
+// Epilogue of one accumulator tile row: this thread's row m of the tile
+// starting at column n0, read from tensor memory at taddr (the warp's lane
+// quarter, the tile's first column).
 template <int BN, int EPI>
-__global__ void __launch_bounds__(128, 2)
+__device__ __forceinline__ void epilogue_row(const GemmArgs& g, uint32_t taddr, int m, int n0) {
+#pragma unroll 1
+    for (int c = 0; c < BN; c += 16) {
+        float v[16];
+        tmem_ld16(taddr + c, v);
+        const int n = n0 + c;
+        if constexpr (EPI == kEpiF32 || EPI == kEpiBiasF32) {
+            if constexpr (EPI == kEpiBiasF32) {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) v[j] += g.bias[n + j];
+            }
+            float4* o = reinterpret_cast<float4*>(static_cast<float*>(g.out) + static_cast<size_t>(m) * g.ldo + n);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) o[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+        } else {
+            if constexpr (EPI == kEpiBiasReluT || EPI == kEpiBiasRelu) {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) v[j] = fmaxf(v[j] + g.bias[n + j], 0.0f);
+            } else {  // ReLU gradient: pass where the forward activation was positive
+                const uint4* mk = reinterpret_cast<const uint4*>(g.mask + static_cast<size_t>(m) * g.ldm + n);
+                const uint4 q0 = mk[0], q1 = mk[1];
+                const __nv_bfloat16* h0 = reinterpret_cast<const __nv_bfloat16*>(&q0);
+                const __nv_bfloat16* h1 = reinterpret_cast<const __nv_bfloat16*>(&q1);
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    if (!(__bfloat162float(h0[j]) > 0.0f)) v[j] = 0.0f;
+                    if (!(__bfloat162float(h1[j]) > 0.0f)) v[8 + j] = 0.0f;
+                }
+            }
+            __nv_bfloat16 b[16];
+#pragma unroll
+            for (int j = 0; j < 16; ++j) b[j] = __float2bfloat16_rn(v[j]);
+            uint4* o = reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(g.out) + static_cast<size_t>(m) * g.ldo + n);
+            o[0] = *reinterpret_cast<const uint4*>(&b[0]);
+            o[1] = *reinterpret_cast<const uint4*>(&b[8]);
+            if constexpr (EPI == kEpiBiasReluT || EPI == kEpiReluGradT) {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) g.outT[static_cast<size_t>(n + j) * g.ldt + m] = b[j];
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ void bar_arrive(uint64_t* b) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(su32(b)) : "memory");
+}
+
+// Persistent GEMM: CTA b computes tiles b, b + gridDim.x, ... (tile t =
+// row block t / (N / BN), column block t % (N / BN), so the column blocks of
+// one row block run together and share that block of A in L2). Six warps:
+// warp 0 (one lane) loads stages with TMA, warp 1 (one lane) issues the
+// MMAs, warps 2..5 run the epilogue. Two accumulators in tensor memory
+// (2 BN columns) let the epilogue of one tile overlap the MMAs of the next:
+// "tfull[a]" (MMA commit) hands accumulator a to the epilogue warps,
+// "tempty[a]" (one arrival per epilogue warp) hands it back.
+template <int BN, int EPI>
+__global__ void __launch_bounds__(kGemmThreads, 1)
     k_gemm_tn(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, const GemmArgs g) {
-    static_assert(BN == 64 || BN == 128 || BN == 256, "tile width");
+    static_assert(BN == 64 || BN == 128, "tile width");  // 128 x 256 tiles measured slower
     extern __shared__ unsigned char smem_raw[];
     unsigned char* smem =
         reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
@@ -171,25 +232,28 @@ __global__ void __launch_bounds__(128, 2)
     unsigned char* sB = smem + kStages * kABytes;
     uint64_t* full = reinterpret_cast<uint64_t*>(sB + kStages * kBBytes);
     uint64_t* empty = full + kStages;
-    uint64_t* done = empty + kStages;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+    uint64_t* tfull = empty + kStages;
+    uint64_t* tempty = tfull + 2;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 2);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.x * kTileM, n0 = blockIdx.y * BN;
-    const int nk = g.K / kTileK;
+    const int ntn = g.N / BN, ntiles = (g.M / kTileM) * ntn, nk = g.K / kTileK;
 
-    if (warp == 0) {
+    if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(tmem_slot)),
-                     "r"(BN)
+                     "r"(2 * BN)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
-    if (threadIdx.x == 32) {
+    if (threadIdx.x == 0) {
         for (int s = 0; s < kStages; ++s) {
             bar_init(&full[s], 1);
             bar_init(&empty[s], 1);
         }
-        bar_init(done, 1);
+        for (int a = 0; a < 2; ++a) {
+            bar_init(&tfull[a], 1);
+            bar_init(&tempty[a], 4);
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     tc_fence_before();
@@ -198,85 +262,68 @@ __global__ void __launch_bounds__(128, 2)
     const uint32_t tmem = *tmem_slot;
     bool ok = true;
 
-    if (warp == 0 && lane == 0) {  // TMA producer
-        for (int kb = 0; kb < nk && ok; ++kb) {
-            const int s = kb % kStages;
-            if (kb >= kStages) ok = bar_wait(&empty[s], ((kb / kStages) - 1) & 1);
-            if (!ok) break;
-            bar_expect_tx(&full[s], kABytes + kBBytes);
-            tma_load_2d(sA + s * kABytes, &mapA, kb * kTileK, m0, &full[s]);
-            tma_load_2d(sB + s * kBBytes, &mapB, kb * kTileK, n0, &full[s]);
-        }
-    } else if (warp == 1 && lane == 0) {  // MMA issuer
-        constexpr uint32_t idesc = idesc_bf16<BN>();
-        for (int kb = 0; kb < nk && ok; ++kb) {
-            const int s = kb % kStages;
-            ok = bar_wait(&full[s], (kb / kStages) & 1);
-            if (!ok) break;
-            tc_fence_after();
-            const uint64_t da = sw128_desc(su32(sA + s * kABytes)), db = sw128_desc(su32(sB + s * kBBytes));
-#pragma unroll
-            for (int kk = 0; kk < kTileK / 16; ++kk)  // +32 bytes per K = 16 step: +2 in the address field
-                mma_bf16(tmem, da + 2 * kk, db + 2 * kk, idesc, (kb | kk) != 0);
-            mma_commit(&empty[s]);
-        }
-        mma_commit(done);
-    }
-    __syncwarp();
-
-    // epilogue (tcgen05.ld is warp-collective: the decision is warp-uniform)
-    if (!bar_wait(done, 0)) ok = false;
-    ok = __all_sync(0xffffffffu, ok);
-    tc_fence_after();
-    const int row = warp * 32 + lane;  // accumulator row of this thread
-    const int m = m0 + row;
-    const uint32_t tbase = tmem + (static_cast<uint32_t>(warp * 32) << 16);
-    if (ok) {
-#pragma unroll 1
-        for (int c = 0; c < BN; c += 16) {
-            float v[16];
-            tmem_ld16(tbase + c, v);
-            const int n = n0 + c;
-            if constexpr (EPI == kEpiF32 || EPI == kEpiBiasF32) {
-                if constexpr (EPI == kEpiBiasF32) {
-#pragma unroll
-                    for (int j = 0; j < 16; ++j) v[j] += g.bias[n + j];
-                }
-                float4* o = reinterpret_cast<float4*>(static_cast<float*>(g.out) + static_cast<size_t>(m) * g.ldo + n);
-#pragma unroll
-                for (int j = 0; j < 4; ++j) o[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
-            } else {
-                if constexpr (EPI == kEpiBiasReluT || EPI == kEpiBiasRelu) {
-#pragma unroll
-                    for (int j = 0; j < 16; ++j) v[j] = fmaxf(v[j] + g.bias[n + j], 0.0f);
-                } else {  // ReLU gradient: pass where the forward activation was positive
-                    const uint4* mk = reinterpret_cast<const uint4*>(g.mask + static_cast<size_t>(m) * g.ldm + n);
-                    const uint4 q0 = mk[0], q1 = mk[1];
-                    const __nv_bfloat16* h0 = reinterpret_cast<const __nv_bfloat16*>(&q0);
-                    const __nv_bfloat16* h1 = reinterpret_cast<const __nv_bfloat16*>(&q1);
-#pragma unroll
-                    for (int j = 0; j < 8; ++j) {
-                        if (!(__bfloat162float(h0[j]) > 0.0f)) v[j] = 0.0f;
-                        if (!(__bfloat162float(h1[j]) > 0.0f)) v[8 + j] = 0.0f;
-                    }
-                }
-                __nv_bfloat16 b[16];
-#pragma unroll
-                for (int j = 0; j < 16; ++j) b[j] = __float2bfloat16_rn(v[j]);
-                uint4* o = reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(g.out) + static_cast<size_t>(m) * g.ldo + n);
-                o[0] = *reinterpret_cast<const uint4*>(&b[0]);
-                o[1] = *reinterpret_cast<const uint4*>(&b[8]);
-                if constexpr (EPI == kEpiBiasReluT || EPI == kEpiReluGradT) {
-#pragma unroll
-                    for (int j = 0; j < 16; ++j) g.outT[static_cast<size_t>(n + j) * g.ldt + m] = b[j];
+    if (warp == 0) {
+        if (lane == 0) {  // TMA producer
+            int kbg = 0;
+            for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+                const int m0 = (t / ntn) * kTileM, n0 = (t % ntn) * BN;
+                for (int kb = 0; kb < nk; ++kb, ++kbg) {
+                    const int s = kbg % kStages;
+                    if (kbg >= kStages && !(ok = bar_wait(&empty[s], ((kbg / kStages) - 1) & 1))) break;
+                    bar_expect_tx(&full[s], kABytes + kBBytes);
+                    tma_load_2d(sA + s * kABytes, &mapA, kb * kTileK, m0, &full[s]);
+                    tma_load_2d(sB + s * kBBytes, &mapB, kb * kTileK, n0, &full[s]);
                 }
             }
         }
+    } else if (warp == 1) {
+        if (lane == 0) {  // MMA issuer
+            constexpr uint32_t idesc = idesc_bf16<BN>();
+            int kbg = 0, it = 0;
+            for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++it) {
+                const int a = it & 1;
+                if (it >= 2 && !(ok = bar_wait(&tempty[a], ((it >> 1) - 1) & 1))) break;
+                tc_fence_after();
+                const uint32_t d = tmem + a * BN;
+                for (int kb = 0; kb < nk; ++kb, ++kbg) {
+                    const int s = kbg % kStages;
+                    if (!(ok = bar_wait(&full[s], (kbg / kStages) & 1))) break;
+                    tc_fence_after();
+                    const uint64_t da = sw128_desc(su32(sA + s * kABytes)), db = sw128_desc(su32(sB + s * kBBytes));
+#pragma unroll
+                    for (int kk = 0; kk < kTileK / 16; ++kk)  // +32 bytes per K = 16 step: +2 in the address field
+                        mma_bf16(d, da + 2 * kk, db + 2 * kk, idesc, (kb | kk) != 0);
+                    mma_commit(&empty[s]);
+                }
+                if (!ok) break;
+                mma_commit(&tfull[a]);
+            }
+        }
+    } else {  // epilogue warps: warp w reads tensor-memory lanes 32 (w % 4) .. + 31
+        const int quarter = warp & 3;
+        int it = 0;
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
+            const int a = it & 1;
+            const bool w = __all_sync(0xffffffffu, bar_wait(&tfull[a], (it >> 1) & 1));
+            if (!w) {
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+            const int m = (t / ntn) * kTileM + quarter * 32 + lane, n0 = (t % ntn) * BN;
+            epilogue_row<BN, EPI>(g, tmem + a * BN + (static_cast<uint32_t>(quarter * 32) << 16), m, n0);
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) bar_arrive(&tempty[a]);
+        }
     }
     if (!ok && lane == 0) atomicOr(g.status, 1);
+    __syncwarp();
     tc_fence_before();
     __syncthreads();
-    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN) : "memory");
+    tc_fence_after();
+    if (warp == 1)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * BN) : "memory");
 }
 
 }  // namespace mlp
