@@ -1726,6 +1726,23 @@ class EnsembleImpl final : public EnsembleImplBase {
         cudaEvent_t done = nullptr;
     };
 
+    // Estimated cost of block (bx, by): its cells, plus twice the cells of
+    // every PML slab it updates (a slab node costs about three plain ones)
+    static long long block_cost(const Dev<R>& d, const MarchTiling& tl, int bx, int by) {
+        const int i0 = bx * tl.TI, i1 = (bx == tl.nrb - 1) ? d.NI : i0 + tl.TI;
+        const int c0 = 1 + by * tl.GC, c1 = std::min(c0 + tl.GC, d.NG - 1);
+        auto overlap = [](int a0, int a1, int b0, int b1) { return std::max(0, std::min(a1, b1) - std::max(a0, b0)); };
+        const long long rows = i1 - i0, planes = c1 - c0, cols = d.NJ;
+        long long slab = 0;
+        for (int s = 0; s < 6; ++s) {
+            const Slab<R>& S = d.sl[s];
+            if (!S.ni) continue;
+            slab += static_cast<long long>(overlap(i0, i1, S.i0, S.i0 + S.ni)) *
+                    overlap(c0, c1, S.k0 + d.gOff, S.k0 + S.nk + d.gOff) * S.nj;
+        }
+        return (rows + 1) * cols * (planes + 2) + 2 * slab;
+    }
+
     void apply_tiling(int TI, int GC) {
         for (SolverImpl<R>* m : mem_) {
             try {
@@ -1787,13 +1804,9 @@ class EnsembleImpl final : public EnsembleImplBase {
                     g.threads = std::max(g.threads, m.threads);
                     g.smem = std::max(g.smem, m.smem);
                     const MarchTiling& tl = m.tile;
-                    const long long row = m.dev[0].NJP;
                     for (int by = 0; by < tl.nchunk; ++by)
-                        for (int bx = 0; bx < tl.nrb; ++bx) {
-                            const int rows = bx == tl.nrb - 1 ? m.dev[0].NI - bx * tl.TI : tl.TI;
-                            const int planes = std::min(tl.GC, m.dev[0].NG - 2 - by * tl.GC);
-                            blocks.push_back({static_cast<long long>(rows + 1) * row * (planes + 2), {a, bx, by}});
-                        }
+                        for (int bx = 0; bx < tl.nrb; ++bx)
+                            blocks.push_back({block_cost(m.dev[0], tl, bx, by), {a, bx, by}});
                 }
                 // longest blocks first: the short ones fill the last wave
                 std::stable_sort(blocks.begin(), blocks.end(),

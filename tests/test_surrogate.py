@@ -12,6 +12,8 @@ it (an FDTD solve per query): the answer time per query."""
 from __future__ import annotations
 
 import importlib
+import os
+import tempfile
 import time
 
 import numpy as np
@@ -130,3 +132,24 @@ def test_device_ensemble_reduction_matches_members(trained):
     ys = np.stack([n.predict(Xte[:300]) for n in s.nets]).astype(np.float64)
     np.testing.assert_allclose(mean, ys.mean(axis=0), rtol=0, atol=1e-4)
     np.testing.assert_allclose(spread, np.sqrt(ys.var(axis=0).mean(axis=1)), rtol=1e-4, atol=1e-4)
+
+
+def test_reference_log_wind_grows_and_linear_wind_stays_bounded():
+    """Why the dataset uses the linear wind profile: in a closed rigid box the
+    reference's logarithmic profile (method 5) grows without bound under its
+    own scheme, while its linear profile (method 1) stays bounded. Run with
+    the oracle, which is bit-exact with the reference."""
+    import oracle
+
+    cg = importlib.import_module("3d_mpi_test_b200.casegen")
+    peaks = {}
+    for method, coef in ((5, 1.5), (1, 1.0)):  # u* = 0.6 m/s; b = 1 / s
+        c = cg.Case(X=cg.uniform_axis(3, 0.0, 0.05), Y=cg.uniform_axis(120, 0.0, 0.05),
+                    Z=cg.uniform_axis(60, 0.0, 0.05), bc=(cg.RIGID,) * 6, time_domain=1500,
+                    gauss_width=0.3, gamma=1.4, P0=1.2 * 343.0 ** 2 / 1.4, c0=343.0, source=(0.05, 3.0, 1.0),
+                    receiver=(0.05, 4.0, 1.0), dt=0.5 * 0.05 / 343.0, velocity_coef=coef, velocity_method=method)
+        d = c.write(os.path.join(tempfile.mkdtemp(), f"w{method}"))
+        r = oracle.run_case(d, [(0.05, 4.0, 1.0)], 1500)["receivers"]
+        peaks[method] = (float(np.abs(r[:300]).max()), float(np.abs(r[-300:]).max()))
+    assert peaks[5][1] > 10 * peaks[5][0], peaks
+    assert peaks[1][1] < peaks[1][0], peaks
