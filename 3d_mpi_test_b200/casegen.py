@@ -348,3 +348,24 @@ def ensemble_member(seed: int, index: int, d: float = 0.1, pml: int = 10, layer:
                   tortuosity=tortuosity, source_height=src_h, hill_height=r_cells * d if r_cells >= 2 else 0.0,
                   ustar=ustar)
     return case, receivers, params
+
+
+def moving_window(ni=256, window=1024, nk=192, total=4096, d=0.05, pml=20, trail=11, ratio=0.05, steps=20000):
+    """The long-range workload's shape: a window of `window` range nodes
+    (Y/j) x `ni` transverse x `nk` height moving over `total` range nodes
+    with the reference's moving frame (calculation_2D.cpp:405-496,
+    air.cpp:2447-2730; lead = trail, frames of trail - 1 cells, the first
+    frame shortened by `ratio`), rigid ground, PML on the other five faces,
+    no wind, Gaussian pulse at 1.5 m, receivers every 5 m at 1.5 m height."""
+    c0, rho0, gamma = 343.0, 1.2, 1.4
+    case = Case(
+        X=uniform_axis(ni, 0.0, d), Y=uniform_axis(total, 0.0, d), Z=uniform_axis(nk, 0.0, d),
+        pml_nodes=(pml, pml, pml, pml, 0, pml), gauss_width=6 * d, bc=(PML, RIGID, PML, PML, PML, PML),
+        time_domain=steps, gamma=gamma, P0=rho0 * c0 * c0 / gamma, c0=c0, pml_y=(2.0, 1000.0, 0),
+        source=(round(ni // 2 * d, 9), round((pml + 20) * d, 9), 1.5),
+        receiver=(round(ni // 2 * d, 9), 5.0, 1.5), dt=0.5 * d / c0,
+        mf_jmax=window, mf_lead=trail, mf_trail=trail, mf_judge=1, mf_ratio=ratio, ijkmax=total,
+    )
+    xc = round(ni // 2 * d, 9)
+    receivers = [(xc, float(r), 1.5) for r in range(5, int(total * d) - 5, 5)][:20]
+    return case, receivers

@@ -314,6 +314,69 @@ def run_ensemble(args, rank, world, local_rank):
     }
 
 
+WINDOW_WORKLOAD = ("moving window 256 (i) x 1024 (j) x 192 (k) = 50.3 M nodes over a 4096-node range, "
+                   "frames of 10 cells, rigid ground, 20-node PML, no wind, FP32")
+
+
+def run_window(args, rank, world, local_rank):
+    """The long-range configuration's shape: a 50.3 M-node window moving
+    over the range (frame shifts inside the timed region)."""
+    import torch
+
+    pkg = importlib.import_module("3d_mpi_test_b200")
+    casegen = importlib.import_module("3d_mpi_test_b200.casegen")
+    replicas = importlib.import_module("3d_mpi_test_b200.replicas")
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist  # noqa: F811
+    group = replicas.ReplicaGroup(dist, "cuda")
+    tmp = tempfile.mkdtemp(prefix=f"bench_win_r{rank}_")
+    case, rec = casegen.moving_window()
+    d = case.write(os.path.join(tmp, "window"))
+    cells = case.NI * 1024 * case.NK
+    hbm_peak, peak_kind = peaks()
+    inner = args.inner
+    a = pkg.Airpore(d, "f32", device=local_rank)
+    a.set_receivers(rec)
+    a.reset((args.warmup + args.steps) * inner + 8)
+    for _ in range(args.warmup):
+        a.advance(inner)
+    group.barrier()
+    l0 = a.launch_count()
+    ms = 0.0
+    sampler = ClockSampler(local_rank)
+    with sampler:
+        for _ in range(args.steps):
+            a.advance(inner)  # 1.7 GB of FP32 state: far larger than L2
+            ms += a.last_device_ms()
+    torch.cuda.synchronize()
+    group.barrier()
+    launches = a.launch_count() - l0
+    steps_total = args.steps * inner
+    gcell = group.throughput(cells, steps_total, ms)
+    ms = group.max_over_ranks(ms)
+    slab = 2 * 21 * 1024 * 192 + 2 * 256 * 21 * 192 + 256 * 1024 * 21  # x1 x2 y1 y2 z2 storage nodes
+    bytes_step = cells * 8 * 4 + slab * 8 * 4
+    achieved = bytes_step / (ms * 1e-3 / steps_total) / 1e9
+    a.close()
+    shutil.rmtree(tmp, ignore_errors=True)
+    if rank != 0:
+        return None
+    return {
+        "metric": "Gcell-upd/s of the moving-window configuration (FP32)", "value": round(gcell, 3), "unit": UNIT,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded case generator)",
+        "config": {"workload": WINDOW_WORKLOAD, "inner_fb_steps_per_bench_step": inner, "cells_per_fb_step": cells,
+                   "frame_shifts_in_timed_region": int(steps_total // 20), "l2": "inputs larger than L2"},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
+                     "frac": round(achieved / hbm_peak, 4), "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_step": bytes_step},
+        "gpu_launches": int(launches), "clocks": sampler.summary(),
+    }
+
+
 def bf16_peak():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -564,7 +627,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tile", default="", help="rows,planes,threads,vector-width,ring-stages of the marching kernel (default: autotune)")
-    ap.add_argument("--workload", default="domain", choices=["domain", "ensemble", "surrogate"])
+    ap.add_argument("--workload", default="domain", choices=["domain", "ensemble", "surrogate", "window"])
     ap.add_argument("--no-surrogate", action="store_true", help="skip the surrogate section of the domain line")
     ap.add_argument("--sur-queries", type=int, default=1_000_000, help="surrogate inference queries")
     ap.add_argument("--sur-train-steps", type=int, default=6000, help="training steps per surrogate member")
@@ -593,6 +656,8 @@ def main():
     try:
         if args.workload == "ensemble":
             line = run_ensemble(args, rank, world, local_rank)
+        elif args.workload == "window":
+            line = run_window(args, rank, world, local_rank)
         elif args.workload == "surrogate":
             line = {"workload": "surrogate", **run_surrogate(args.sur_queries, steps=args.sur_train_steps,
                                                               device=local_rank)} if rank == 0 else None

@@ -174,6 +174,20 @@ def narrow_y():
     return c, [(0.3, 0.1, 0.25), (0.35, 0.15, 0.3)]
 
 
+def wide_2d():
+    """2D (NI = 3, Front/Back rigid) with 900 columns: the FP32 marching tile
+    fits shared memory only with its stage sized to the rows it stages;
+    porous ground, linear wind, PML."""
+    layer = 4
+    c = _base(ni=3, nj=900, nk=40, steps=30, bc=(PML, POROUS, PML, PML, RIGID, RIGID),
+              pml_nodes=(0, 0, 10, 10, 0, 10), pore=(math.sqrt(1.5), 0.4, 1.0e5), velocity_coef=0.8,
+              velocity_method=1)
+    c.pore_Z = uniform_axis(layer + 2, -layer * D, D)
+    c.pore_dxyz = (D, D, D)
+    c.source = (0.05, 20.0, 0.5)
+    return c, [(0.05, 20.5, 0.5), (0.05, 25.0, 1.0), (0.05, 40.0, 0.3)]
+
+
 ENS_SMALL = ((24, 36), (16, 20), (10, 13))  # NJ, NK, 3D NI ranges of the small ensemble members
 
 
@@ -195,5 +209,5 @@ CASES: Dict[str, Callable[[], Tuple[Case, List]]] = {
     for f in [pml_rigid, tdbc_east, porous_ground, porous_tdbc_fine_pore, south_pml_all_faces, front_only_pml,
               back_only_pml, all_rigid, wind_linear, wind_log, wind_vortex, hill(1), hill(2), hill(3), hill(4),
               hill(5), moving_frame, fb_v_p, delayed_y1, stretched, odd_columns_wind, odd_columns_porous, narrow_y,
-              ensemble_member_2d, ensemble_member_3d]
+              ensemble_member_2d, ensemble_member_3d, wide_2d]
 }
