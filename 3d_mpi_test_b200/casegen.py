@@ -206,8 +206,8 @@ def write_receivers(path: str, receivers: Sequence[Tuple[float, float, float]]) 
 
 
 # ---------------------------------------------------------------------- #
-# Named workloads.  BASELINE "x" (range) maps to reference Y/j, BASELINE "y"
-# (transverse) to X/i, "z" to Z/k.
+# Named workloads.  The range axis of a workload maps to the reference's
+# Y/j, the transverse axis to X/i and the height to Z/k.
 # ---------------------------------------------------------------------- #
 
 def plain_box(ni=48, nj=96, nk=48, d=0.05, steps=500, pml=10):
