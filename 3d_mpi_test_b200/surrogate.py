@@ -205,8 +205,8 @@ class Surrogate:
             n.close()
         self.nets = []
 
-    def fit(self, X, EA, steps: int = 6000, lr: float = 2e-3, lr_final: float = 2e-5,
-            weight_decay: float = 0.05) -> list:
+    def fit(self, X, EA, steps: int = 12000, lr: float = 2e-3, lr_final: float = 2e-5,
+            weight_decay: float = 0.1) -> list:
         """Trains every member; returns their final training losses (mean
         squared error of the normalised outputs)."""
         X = np.asarray(X, np.float32)

@@ -216,16 +216,18 @@ def generate(seed: int, n: int, path: str, device: int = 0, batch: int = 256, lo
 
 
 DATASET = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "ea_dataset.npz")
-DATASET_PARTS = ((2024, 5000), (2025, 10000))  # (seed, samples) of the committed dataset
-N_TRAIN = 13500  # the last 1500 samples of the committed dataset are held out
+DATASET_PARTS = ((2024, 5000), (2025, 10000), (2026, 15000))  # (seed, samples) of the committed dataset
+N_TRAIN = 28500  # the last 1500 samples of the committed dataset are held out
 
 
 def build_dataset(path: str = DATASET, device: int = 0, log=print) -> None:
     """Regenerates the committed dataset: generate() for every part of
-    DATASET_PARTS, concatenated; X float32, EA float16 (0.06 dB at most)."""
+    DATASET_PARTS, concatenated; X float32, excess attenuation as int16
+    hundredths of a dB (EA_cdb). The committed file's first two parts went
+    through float16 first (0.06 dB at most)."""
     parts = [generate(s, n, path + f".part{s}.npz", device=device, log=log) for s, n in DATASET_PARTS]
     np.savez_compressed(path, X=np.concatenate([p["X"] for p in parts]).astype(np.float32),
-                        EA=np.concatenate([p["EA"] for p in parts]).astype(np.float16),
+                        EA_cdb=np.round(np.concatenate([p["EA"] for p in parts]) * 100).astype(np.int16),
                         seeds=np.array([s for s, _ in DATASET_PARTS]), counts=np.array([n for _, n in DATASET_PARTS]),
                         seconds=np.array([float(p["seconds"]) for p in parts]))
     for s, _ in DATASET_PARTS:
@@ -237,7 +239,8 @@ def load_dataset(path: str = DATASET):
     samples train, the rest are held out; rows of grown solves (NaN) are
     dropped."""
     d = np.load(path)
-    X, EA = d["X"].astype(np.float32), d["EA"].astype(np.float32)
+    X = d["X"].astype(np.float32)
+    EA = d["EA_cdb"].astype(np.float32) / 100 if "EA_cdb" in d else d["EA"].astype(np.float32)
     ok = np.isfinite(EA).all(axis=1)
     tr = np.arange(len(X)) < N_TRAIN
     return X[ok & tr], EA[ok & tr], X[ok & ~tr], EA[ok & ~tr]

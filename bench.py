@@ -386,7 +386,7 @@ def bf16_peak():
     return 1590.0, "fallback"
 
 
-def run_surrogate(queries: int = 1_000_000, members: int = 5, steps: int = 6000, device: int = 0) -> dict:
+def run_surrogate(queries: int = 1_000_000, members: int = 5, steps: int = 12000, device: int = 0) -> dict:
     """The learned surrogate on this GPU: a `members`-network bf16 ensemble
     trained on the committed FDTD dataset (3d_mpi_test_b200/data), its
     held-out error and FDTD fallback rate, its inference throughput on
@@ -630,7 +630,7 @@ def main():
     ap.add_argument("--workload", default="domain", choices=["domain", "ensemble", "surrogate", "window"])
     ap.add_argument("--no-surrogate", action="store_true", help="skip the surrogate section of the domain line")
     ap.add_argument("--sur-queries", type=int, default=1_000_000, help="surrogate inference queries")
-    ap.add_argument("--sur-train-steps", type=int, default=6000, help="training steps per surrogate member")
+    ap.add_argument("--sur-train-steps", type=int, default=12000, help="training steps per surrogate member")
     ap.add_argument("--members", type=int, default=256, help="ensemble members (--workload ensemble)")
     ap.add_argument("--check-members", type=int, default=-1, help="members checked against FP64 (-1: all)")
     ap.add_argument("--check-steps", type=int, default=200)

@@ -105,7 +105,7 @@ def test_fdtd_fallback_matches_dataset(trained):
     np.testing.assert_allclose(y[0], direct[0], rtol=0, atol=1e-4)  # answers are float32
     # the fallback solver reproduces the dataset's own values
     again = sd.solve(Xte[1:3])
-    np.testing.assert_allclose(again, Ete[1:3], rtol=0, atol=0.07)  # the dataset stores float16
+    np.testing.assert_allclose(again, Ete[1:3], rtol=0, atol=0.01)  # the dataset stores 0.01 dB steps
 
 
 @pytest.mark.gpu
