@@ -40,7 +40,7 @@ EXPORTS = (
     "fdtd_fft", "fdtd_spectrum", "fdtd_band_levels", "fdtd_save_restart", "fdtd_load_restart",
     "fdtd_write_contour", "fdtd_get_receivers", "fdtd_set_wait_limit", "fdtd_ensemble_create",
     "fdtd_ensemble_destroy", "fdtd_ensemble_advance", "fdtd_ensemble_autotune", "fdtd_ensemble_info",
-    "fdtd_ensemble_last_device_ms",
+    "fdtd_ensemble_last_device_ms", "fdtd_ensemble_set_mode",
     # include/fdtd_surrogate.h (signatures in surrogate.py)
     "fdtd_tc_gemm", "fdtd_net_create", "fdtd_net_destroy", "fdtd_net_n_params", "fdtd_net_get_params",
     "fdtd_net_set_params", "fdtd_net_set_data", "fdtd_net_get_normalization", "fdtd_net_set_normalization",
@@ -105,6 +105,7 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
         "fdtd_ensemble_autotune": ([vp, i, ip], i),
         "fdtd_ensemble_info": ([vp, ctypes.POINTER(ctypes.c_longlong)], i),
         "fdtd_ensemble_last_device_ms": ([vp, dp], i),
+        "fdtd_ensemble_set_mode": ([vp, i], i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -295,7 +296,7 @@ class Ensemble:
     horizon (``reset``) and read-out, and must stay open while the ensemble
     is used."""
 
-    def __init__(self, members: Sequence[Airpore], lib_path: Optional[str] = None):
+    def __init__(self, members: Sequence[Airpore], lib_path: Optional[str] = None, mode: int = 1):
         if not members:
             raise FdtdError(FDTD_ERR_ARG, "an ensemble needs at least one member")
         self._L = members[0]._L if lib_path is None else load_library(lib_path)
@@ -303,6 +304,7 @@ class Ensemble:
         arr = (ctypes.c_void_p * len(members))(*[m._h.value for m in members])
         self._h = ctypes.c_void_p()
         self._check(self._L.fdtd_ensemble_create(arr, len(members), ctypes.byref(self._h)))
+        self._check(self._L.fdtd_ensemble_set_mode(self._h, mode))
 
     def _check(self, rc: int) -> None:
         if rc < 0:

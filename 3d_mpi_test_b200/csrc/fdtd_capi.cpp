@@ -265,6 +265,11 @@ int fdtd_ensemble_info(const fdtd_ensemble* e, long long* info) {
     });
 }
 
+int fdtd_ensemble_set_mode(fdtd_ensemble* e, int mode) {
+    if (!e) return bad("null argument");
+    return guard([&] { e->e->set_mode(mode); });
+}
+
 int fdtd_ensemble_last_device_ms(const fdtd_ensemble* e, double* ms) {
     if (!e || !ms) return bad("null argument");
     *ms = e->e->last_device_ms();

@@ -98,6 +98,9 @@ class Ensemble {
     long long launch_count() const;
     // {launch groups, blocks per step}
     std::array<long long, 2> shape() const;
+    // 0: one batched launch per group per step; 1 (default): every member's
+    // own marching launch, members spread over several streams
+    void set_mode(int mode);
 
    private:
     std::unique_ptr<EnsembleImplBase> impl_;

@@ -238,7 +238,7 @@ def run_ensemble(args, rank, world, local_rank):
         a.set_receivers(rec)
         a.reset(horizon)
         mem.append(a)
-    ens = pkg.Ensemble(mem)
+    ens = pkg.Ensemble(mem, mode=args.ens_mode)
     tile = ens.autotune(3)
     for a in mem:
         a.reset(horizon)
@@ -304,6 +304,8 @@ def run_ensemble(args, rank, world, local_rank):
         "config": {"workload": ENS_WORKLOAD, "members": args.members, "cells_per_fb_step": cells,
                    "inner_fb_steps_per_bench_step": inner, "l2": "inputs larger than L2",
                    "tile_rows_planes": list(tile), "launch_groups": info["groups"],
+                   "launch_mode": ["one batched launch per group per step",
+                                   "each member's own launch, 16 streams"][args.ens_mode],
                    "blocks_per_fb_step": info["blocks_per_step"], "setup_s": round(setup_s, 1),
                    "parallelism": f"replicas x{world}" if world > 1 else "one device"},
         "check": {"members": nchk, "steps": args.check_steps, "max_rel_l2_receivers_vs_fp64": max(errs),
@@ -634,6 +636,7 @@ def main():
     ap.add_argument("--members", type=int, default=256, help="ensemble members (--workload ensemble)")
     ap.add_argument("--check-members", type=int, default=-1, help="members checked against FP64 (-1: all)")
     ap.add_argument("--check-steps", type=int, default=200)
+    ap.add_argument("--ens-mode", type=int, default=1, choices=[0, 1], help="ensemble launch mode")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

@@ -150,10 +150,13 @@ int fdtd_get_receivers(fdtd_solver *h, int first_step, int nsteps, double *out);
 int fdtd_set_wait_limit(fdtd_solver *h, long long polls);
 
 /* Ensembles: independent handles of one precision on one device stepped
- * together. Each step is one launch of the batched marching kernel per
- * group of members (same kernel form and block size class) over a work
- * list of (member, row block, plane chunk), heaviest blocks first; groups
- * run as parallel chains and the time loop is captured in a CUDA graph.
+ * together, the time loop captured in a CUDA graph. By default (mode 1,
+ * fdtd_ensemble_set_mode) each step launches every member's marching
+ * kernel, the members spread over up to 16 streams. In mode 0 each step is
+ * one launch of the batched marching kernel per group of members (same
+ * kernel form and block size class) over a work list of (member, row
+ * block, plane chunk), heaviest blocks first, the groups as parallel
+ * chains.
  * Members must use the fused FB_p_v pass (FDTD_ERR_UNSUPPORTED otherwise)
  * and no moving frame; they keep their receivers, horizon and read-out, and
  * must outlive the ensemble. fdtd_ensemble_advance takes min(nsteps, the
@@ -171,6 +174,11 @@ int fdtd_ensemble_advance(fdtd_ensemble *e, int nsteps, int *taken);
 int fdtd_ensemble_autotune(fdtd_ensemble *e, int nsteps, int *best);
 int fdtd_ensemble_info(const fdtd_ensemble *e, long long *info);
 int fdtd_ensemble_last_device_ms(const fdtd_ensemble *e, double *ms);
+/* mode 0: one batched launch per group per step, members' parameters read
+ * from a table in global memory; 1 (default): every member's own marching
+ * launch (parameters in the constant bank), the members spread over up to
+ * 16 streams in the captured step graph. FDTD_ERR_ARG for other values. */
+int fdtd_ensemble_set_mode(fdtd_ensemble *e, int mode);
 
 /* Pressure contour of the current state (airpore::get_data_contour,
  * airpore.cpp:1014-1056; calculation_2D::mpi_send_data and operator<<,

@@ -91,9 +91,10 @@ def test_ensemble_argument_checks():
 
 # ------------------------------------------------------------------ GPU
 @pytest.mark.gpu
-@pytest.mark.parametrize("precision,tile", [("f32", None), ("f64", None), ("f32", (2, 3, 48, 2, 5)),
-                                            ("f64", (8, 7, 1000, 0, 0))])
-def test_batch_equals_single_solves(precision, tile, tmp_path):
+@pytest.mark.parametrize("precision,tile,mode", [("f32", None, 0), ("f64", None, 0), ("f32", (2, 3, 48, 2, 5), 0),
+                                                 ("f64", (8, 7, 1000, 0, 0), 0), ("f32", None, 1),
+                                                 ("f64", (3, 5, 32, 2, 5), 1)])
+def test_batch_equals_single_solves(precision, tile, mode, tmp_path):
     steps = 37  # a graph of 16 steps twice plus 5 single launches
     ms = _members(tmp_path, 6, steps)
     mem = []
@@ -104,11 +105,12 @@ def test_batch_equals_single_solves(precision, tile, tmp_path):
         if tile:
             a.set_tiling(*tile)
         mem.append(a)
-    with pkg.Ensemble(mem) as e:
+    with pkg.Ensemble(mem, mode=mode) as e:
         assert e.advance(7) == 7
         assert e.advance(steps) == steps - 7  # capped at the members' horizon
         info = e.info()
-        assert info["launches"] == steps * info["groups"] and info["blocks_per_step"] >= 6
+        per_step = info["groups"] if mode == 0 else len(mem)  # mode 1: each member's own launch
+        assert info["launches"] == steps * per_step and info["blocks_per_step"] >= 6
     tol = 1e-10 if precision == "f64" else 1e-4
     same = 1e-13 if precision == "f64" else 1e-5  # batch vs single: rounding only
     for (d, rec, _), a in zip(ms, mem):
