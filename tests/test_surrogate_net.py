@@ -68,8 +68,10 @@ def _bf(t):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("M,N,K", [(128, 64, 64), (256, 128, 128), (384, 192, 320), (128, 512, 512),
-                                   (1024, 256, 576)])
+                                   (1024, 256, 576), (8192, 512, 512), (32768, 512, 64), (20480, 192, 128)])
 def test_tc_gemm_matches_numpy(M, N, K):
+    """Small and large products: from one tile per CTA up to several tiles
+    per persistent CTA (both tensor-memory accumulators, wrapped phases)."""
     import torch
 
     rng = np.random.default_rng(M + N + K)
@@ -160,3 +162,18 @@ def test_training_lowers_loss_and_predictions_match_oracle():
         assert np.array_equal(yd.cpu().numpy(), Y)
         info = net.info()
         assert info["launches"] > 600 and info["last_device_ms"] > 0
+
+
+@pytest.mark.gpu
+def test_inference_across_chunks_matches_single_rows():
+    """Queries spanning several inference passes (65,536 rows each) and a
+    ragged last pass give the same answers as the same rows on their own."""
+    X, T = _data(2048, 11, 136, 4)
+    with sur.Net(11, 136, width=512, hidden=4, batch=256, seed=9) as net:
+        net.set_data(X, T)
+        net.train(50, lr=1e-3, lr_final=1e-3)
+        Xq = np.tile(X, (70000 // len(X) + 1, 1))[:70000] + np.linspace(0, 1, 70000, dtype=np.float32)[:, None]
+        Y = net.predict(Xq)
+        for r0 in (0, 65530, 69990):
+            np.testing.assert_array_equal(net.predict(Xq[r0:r0 + 10]), Y[r0:r0 + 10])
+        assert net.predict(np.zeros((0, 11), np.float32)).shape == (0, 136)
