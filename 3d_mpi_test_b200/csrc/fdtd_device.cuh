@@ -332,7 +332,10 @@ __device__ __forceinline__ void wind_dp(const Dev<R>& d, int j, int k, R ax, R a
 //   pim pjm pkm  p_n(i-1), p_n(j-1), p_n(g-1) (read with wind only)
 // Columns outside 1..NJ-2 (faces, row padding) get values the caller
 // discards; every read for them stays in bounds.
-template <typename R, bool WIND, int N>
+// XF: the rarer features (porous inclusions, vectors with columns of both y
+// layers) are compiled in; a kernel built without them is used only for
+// domains that have none
+template <typename R, bool WIND, int N, bool XF = true>
 __device__ __forceinline__ Arr<R, N> p_vec(const Dev<R>& d, const PlaneC<R>& pc, const RowC<R>& rc, int i, int jb,
                                            const Arr<R, N>& ay, int ysp, const Arr<R, N>& u0, const Arr<R, N>& v0,
                                            const Arr<R, N>& w0, const Arr<R, N>& pn, const Arr<R, N>& ui,
@@ -361,7 +364,7 @@ __device__ __forceinline__ Arr<R, N> p_vec(const Dev<R>& d, const PlaneC<R>& pc,
     }
     const int ysv = y_common<N>(ysp);
     if (rc.xs | ysv | pc.zs) {
-        if (ysv != 3) {
+        if (!XF || ysv != 3) {
             pml_dp_v<R, N>(d, i, jb, pc.k, rc.xs, ysp, ysv, pc.zs, rc.ax, ay, pc.az, gu, gv, gw, pn, rc.X, pc.Z, dp);
         } else {  // both y layers within N columns (very narrow grids): column by column
 #pragma unroll
@@ -376,7 +379,7 @@ __device__ __forceinline__ Arr<R, N> p_vec(const Dev<R>& d, const PlaneC<R>& pc,
     }
 #pragma unroll
     for (int e = 0; e < N; ++e) out.e[e] = pn.e[e] + dp.e[e];
-    if (rc.inmask) {
+    if (XF && rc.inmask) {
 #pragma unroll
         for (int e = 0; e < N; ++e) {
             const int mv = mask_at(d, i, jb + e, pc.k);
@@ -529,7 +532,7 @@ struct Vel {
 // (air.cpp:1476-1949); pore: porous::cal_fuvw (porous.cpp:58-104);
 // accumulation: calculation_2D::Cal_velocity (calculation_2D.cpp:548-579).
 // Column conventions as p_vec.
-template <typename R, bool WIND, int N>
+template <typename R, bool WIND, int N, bool XF = true>
 __device__ __forceinline__ Vel<R, N> vel_vec(const Dev<R>& d, const PlaneC<R>& pc, const RowC<R>& rc, int i, int jb,
                                              const Arr<R, N>& ay, int ysp, const Arr<R, N>& u0, const Arr<R, N>& v0,
                                              const Arr<R, N>& w0, const Arr<R, N>& p0, const Arr<R, N>& pim,
@@ -573,7 +576,7 @@ __device__ __forceinline__ Vel<R, N> vel_vec(const Dev<R>& d, const PlaneC<R>& p
     }
     const int ysv = y_common<N>(ysp);
     if (rc.xs | ysv | pc.zs) {
-        if (ysv != 3) {
+        if (!XF || ysv != 3) {
             pml_dvel_v<R, N>(d, i, jb, pc.k, rc.xs, ysp, ysv, pc.zs, ax, ay, az, u0, v0, w0, gpX, gpY, gpZ, p0, pim,
                              pjm, pkm, qp_old, rc.X, pc.Z, du, dv, dw);
         } else {  // both y layers within N columns (very narrow grids): column by column
@@ -596,7 +599,7 @@ __device__ __forceinline__ Vel<R, N> vel_vec(const Dev<R>& d, const PlaneC<R>& p
         r.v.e[e] = v0.e[e] + dv.e[e];
         r.w.e[e] = w0.e[e] + dw.e[e];
     }
-    if (rc.inmask) {
+    if (XF && rc.inmask) {
 #pragma unroll
         for (int e = 0; e < N; ++e) {
             const int mv = mask_at(d, i, jb + e, pc.k);

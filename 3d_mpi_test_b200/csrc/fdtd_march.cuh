@@ -92,7 +92,7 @@ __device__ __forceinline__ void march_bookkeeping(const Dev<R>& d, int par, int 
 // 1..NJ-2 are kept; column 0 repeats column 1 (west face copy,
 // calculation_2D.cpp:650-660); columns >= NJ-1 are 0 -- the east face is
 // extrapolated where it is used.
-template <typename R, bool WIND, int VW>
+template <typename R, bool WIND, int VW, bool XF>
 __device__ __forceinline__ Arr<R, VW> march_p(const Dev<R>& d, const PlaneC<R>& pc, const RowC<R>& rc, const R* rg,
                                           const MarchGeo& G, int oq, int on, int om, int ic, int jb,
                                           const Arr<R, VW>& ay, int ysp) {
@@ -114,7 +114,7 @@ __device__ __forceinline__ Arr<R, VW> march_p(const Dev<R>& d, const PlaneC<R>& 
 #pragma unroll
         for (int e = 0; e < V; ++e) pjm.e[e] = e > 0 ? pn.e[e > 0 ? e - 1 : 0] : pj0;
     }
-    Arr<R, VW> out = p_vec<R, WIND, VW>(d, pc, rc, ic, jb, ay, ysp, u0, v0, w0, pn, ui, vj, wk, pim, pjm, pkm);
+    Arr<R, VW> out = p_vec<R, WIND, VW, XF>(d, pc, rc, ic, jb, ay, ysp, u0, v0, w0, pn, ui, vj, wk, pim, pjm, pkm);
 #pragma unroll
     for (int e = 0; e < V; ++e)
         if (jb + e < 1 || jb + e > NJ - 2) out.e[e] = R(0);
@@ -194,7 +194,7 @@ __device__ __forceinline__ void march_slabs(const Dev<R>& d, int i, int jb, int 
 // Emit output row i of plane q: new velocity at the clamped stencil row ii
 // from the shared-memory pressure, face resolution, outputs, slabs, TDBC
 // state, and the face planes 0 / NG-1 next to it.
-template <typename R, bool WIND, int VW>
+template <typename R, bool WIND, int VW, bool XF>
 __device__ __forceinline__ void march_emit(const Dev<R>& d, const PlaneC<R>& pc, const R* rg, const R* pb,
                                            const MarchGeo& G, int oq, int on, int slot, int q, int i, int jb,
                                            const Arr<R, VW>& ay, int ysp, int ysm1, int ystore, R& bad) {
@@ -230,7 +230,7 @@ __device__ __forceinline__ void march_emit(const Dev<R>& d, const PlaneC<R>& pc,
             nb.wj.e[e] = e + 1 < V ? w0.e[e1] : wn;
         }
     }
-    const Vel<R, VW> r = vel_vec<R, WIND, VW>(d, pc, rc, ii, jb, ay, ysp, u0, v0, w0, P0, Pi, Pj, Pk, nb, true);
+    const Vel<R, VW> r = vel_vec<R, WIND, VW, XF>(d, pc, rc, ii, jb, ay, ysp, u0, v0, w0, P0, Pi, Pj, Pk, nb, true);
     Arr<R, VW> fu{}, fv{}, fw{};
 #pragma unroll
     for (int e = 0; e < V; ++e)
@@ -277,7 +277,7 @@ __device__ __forceinline__ void march_emit(const Dev<R>& d, const PlaneC<R>& pc,
         for (int e = 0; e < V; ++e)
             if (e == eE) pv.e[e] = pE;
     }
-    const bool tdE = hasE && d.tdbc && !pc.pore;
+    const bool tdE = XF && hasE && d.tdbc && !pc.pore;
     if (tdE) {
         const R vt = static_cast<R>(tdbc_v(d, ii, pc.k, static_cast<double>(pEs)));
 #pragma unroll
@@ -292,7 +292,7 @@ __device__ __forceinline__ void march_emit(const Dev<R>& d, const PlaneC<R>& pc,
     stn<R, VW>(d.v_out + go, fv);
     stn<R, VW>(d.w_out + go, fw);
     if (q >= d.gOff) march_slabs<R, VW>(d, i, jb, pc.k, ystore, pv, fu, fv, fw);
-    if (hasE && d.tdbc && q >= d.gOff) psi_update(d, i, pc.k, static_cast<double>(pE));
+    if (XF && hasE && d.tdbc && q >= d.gOff) psi_update(d, i, pc.k, static_cast<double>(pE));
     const Arr<R, VW> zero{};
     if (q == 1) {  // south face plane: p, u, v of plane 1, w = 0
         const size_t g0 = static_cast<size_t>(i) * pitch + jb;
@@ -302,7 +302,7 @@ __device__ __forceinline__ void march_emit(const Dev<R>& d, const PlaneC<R>& pc,
         stn<R, VW>(d.w_out + g0, zero);
         if (0 >= d.gOff) {
             march_slabs<R, VW>(d, i, jb, -d.gOff, ystore, pv, fu, fv, zero);
-            if (hasE && d.tdbc) psi_update(d, i, -d.gOff, static_cast<double>(pE));
+            if (XF && hasE && d.tdbc) psi_update(d, i, -d.gOff, static_cast<double>(pE));
         }
     }
     if (q == NG - 2) {  // north face plane: p, u, v of plane NG-2 (east: TDBC on the face row), w = 0
@@ -320,7 +320,7 @@ __device__ __forceinline__ void march_emit(const Dev<R>& d, const PlaneC<R>& pc,
         stn<R, VW>(d.v_out + gT, vT);
         stn<R, VW>(d.w_out + gT, zero);
         march_slabs<R, VW>(d, i, jb, kT, ystore, pv, fu, vT, zero);
-        if (hasE && d.tdbc) psi_update(d, i, kT, static_cast<double>(pE));
+        if (XF && hasE && d.tdbc) psi_update(d, i, kT, static_cast<double>(pE));
     }
 }
 
@@ -328,7 +328,7 @@ __device__ __forceinline__ void march_emit(const Dev<R>& d, const PlaneC<R>& pc,
 // may have more threads than the tile's trows thread rows (batched launches
 // over domains of different widths): the extra threads only take part in
 // the block barriers.
-template <typename R, bool WIND, int VW>
+template <typename R, bool WIND, int VW, bool XF>
 __device__ __forceinline__ void march_block(const Dev<R>& d, const MarchTiling& t, int par, int bx, int by) {
     static_assert(VW >= 2 && VW * sizeof(R) <= 16, "a thread owns 2..16 bytes of columns");
     constexpr int V = VW;
@@ -464,7 +464,7 @@ __device__ __forceinline__ void march_block(const Dev<R>& d, const MarchTiling& 
         for (int i = rlo + tr; i < i1; i += m) {
             const int ic = i < 1 ? 1 : (i > NI - 2 ? NI - 2 : i);
             const RowC<R> rc = row_c(d, pc, ic);
-            stn<R, VW>(pb + G.prow(slot, i) + jb, march_p<R, WIND, VW>(d, pc, rc, rg, G, oq, on, om, ic, jb, ay, ys));
+            stn<R, VW>(pb + G.prow(slot, i) + jb, march_p<R, WIND, VW, XF>(d, pc, rc, rg, G, oq, on, om, ic, jb, ay, ys));
         }
         __syncthreads();
         if (q == 1) {  // plane 0 (south face) pressure is plane 1's
@@ -474,7 +474,7 @@ __device__ __forceinline__ void march_block(const Dev<R>& d, const MarchTiling& 
         // phase 2: velocity, outputs, slabs, TDBC of rows i0 .. i1-1
         if (q >= c0)
             for (int i = i0 + tr; i < i1; i += m)
-                march_emit<R, WIND, VW>(d, pc, rg, pb, G, oq, on, slot, q, i, jb, ay, ys, ysm1, ystore, bad);
+                march_emit<R, WIND, VW, XF>(d, pc, rg, pb, G, oq, on, slot, q, i, jb, ay, ys, ysm1, ystore, bad);
         __syncthreads();
     }
     if (!(bad == R(0))) atomicOr(d.status, 1);
@@ -486,9 +486,12 @@ __device__ __forceinline__ void march_block(const Dev<R>& d, const MarchTiling& 
     }
 }
 
-template <typename R, bool WIND, int VW>
+// XF: porous inclusions, the east TDBC and vectors with columns of both y
+// layers compiled in (the host picks the form without them for domains
+// that have none: fewer registers and instructions)
+template <typename R, bool WIND, int VW, bool XF>
 __global__ void __launch_bounds__(256) k_march(__grid_constant__ const Dev<R> d, const MarchTiling t, int par) {
-    march_block<R, WIND, VW>(d, t, par, blockIdx.x, blockIdx.y);
+    march_block<R, WIND, VW, XF>(d, t, par, blockIdx.x, blockIdx.y);
 }
 
 // One block of a batched launch over independent domains (an ensemble of
@@ -509,12 +512,12 @@ struct BatchEntry {
 // entries [2][nmem]: phase 0 holds every member at the parity of the first
 // step of the sequence, phase 1 at the other one; step s of a sequence
 // passes phase s & 1.
-template <typename R, bool WIND, int VW>
+template <typename R, bool WIND, int VW, bool XF>
 __global__ void __launch_bounds__(256) k_march_batch(const BatchWork* __restrict__ work,
                                                      const BatchEntry<R>* __restrict__ entries, int nmem, int phase) {
     const BatchWork w = work[blockIdx.x];
     const BatchEntry<R>& e = entries[phase * nmem + w.member];
-    march_block<R, WIND, VW>(e.d, e.t, e.par, w.bx, w.by);
+    march_block<R, WIND, VW, XF>(e.d, e.t, e.par, w.bx, w.by);
 }
 
 }  // namespace fdtd

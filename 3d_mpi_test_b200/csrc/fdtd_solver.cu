@@ -528,6 +528,11 @@ class SolverImpl final : public SolverImplBase {
             upload(d_ayP_, air_.fy);
         }
         build_pml_y(N);
+        const bool xf = needs_xf();
+        if (xf != xf_) {
+            xf_ = xf;
+            graph_dirty_ = true;
+        }
         upload(d_sy_[0], sy_); upload(d_sy_[1], fy_); upload(d_sy_[2], gy_);
         h2d(d_sdy_, sdy_.data(), NJ_);
         if (wind_on_) {
@@ -819,25 +824,47 @@ class SolverImpl final : public SolverImplBase {
         graph_dirty_ = true;
     }
 
+    template <bool XF>
+    static const void* march_kernel(int VW, bool wind) {
+        if constexpr (sizeof(R) == 4) {
+            if (VW == 4) return wind ? reinterpret_cast<const void*>(k_march<R, true, 4, XF>)
+                                     : reinterpret_cast<const void*>(k_march<R, false, 4, XF>);
+        }
+        return wind ? reinterpret_cast<const void*>(k_march<R, true, 2, XF>)
+                    : reinterpret_cast<const void*>(k_march<R, false, 2, XF>);
+    }
+
     template <typename F>
     static void for_march_kernels(F f) {
-        f(reinterpret_cast<const void*>(k_march<R, true, 2>));
-        f(reinterpret_cast<const void*>(k_march<R, false, 2>));
-        if constexpr (sizeof(R) == 4) {
-            f(reinterpret_cast<const void*>(k_march<R, true, 4>));
-            f(reinterpret_cast<const void*>(k_march<R, false, 4>));
+        for (int VW : {2, 4}) {
+            if (VW > kVecMax) continue;
+            for (bool w : {true, false}) {
+                f(march_kernel<true>(VW, w));
+                f(march_kernel<false>(VW, w));
+            }
         }
+    }
+
+    // the kernel form this domain launches: XF (inclusion mask, east TDBC,
+    // vectors with both y layers) only when the domain has one of them
+    bool needs_xf() const {
+        if (mask_on_ || tdbc_) return true;
+        for (int VW : {2, 4})
+            for (int jb = 0; jb < NJ_; jb += VW) {
+                int c = 0;
+                for (int e = 0; e < VW && jb + e < NJ_; ++e) {
+                    const int s = sdy_[jb + e];
+                    if (s) c = (c == 0 || c == s) ? s : 3;
+                }
+                if (c == 3) return true;
+            }
+        return false;
     }
 
     // resident blocks per SM of the marching kernel for a block shape
     int march_occupancy(int VW, int threads, size_t smem) const {
         int n = 0;
-        const void* k = reinterpret_cast<const void*>(k_march<R, false, 2>);
-        if constexpr (sizeof(R) == 4) {
-            if (VW == 4) k = wind_on_ ? reinterpret_cast<const void*>(k_march<R, true, 4>)
-                                      : reinterpret_cast<const void*>(k_march<R, false, 4>);
-        }
-        if (VW == 2 && wind_on_) k = reinterpret_cast<const void*>(k_march<R, true, 2>);
+        const void* k = xf_ ? march_kernel<true>(VW, wind_on_) : march_kernel<false>(VW, wind_on_);
         if (smem > 48 * 1024)
             FDTD_CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSmemMax)));
         FDTD_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, threads, smem));
@@ -848,21 +875,25 @@ class SolverImpl final : public SolverImplBase {
 
     // one fused step at parity par on stream s (also an ensemble's stream)
     void launch_fused_on(int par, cudaStream_t s) {
-        const dim3 grd(tiling_.nrb, tiling_.nchunk, 1), blk(fused_threads_, 1, 1);
         const Dev<R> d = params_fused(par);
+        if (xf_) launch_march<true>(d, par, s);
+        else launch_march<false>(d, par, s);
+        FDTD_CK(cudaGetLastError());
+        ++launches_;
+    }
+
+    template <bool XF>
+    void launch_march(const Dev<R>& d, int par, cudaStream_t s) {
+        const dim3 grd(tiling_.nrb, tiling_.nchunk, 1), blk(fused_threads_, 1, 1);
         if constexpr (sizeof(R) == 4) {
             if (tiling_.VW == 4) {
-                if (wind_on_) k_march<R, true, 4><<<grd, blk, fused_smem_, s>>>(d, tiling_, par);
-                else k_march<R, false, 4><<<grd, blk, fused_smem_, s>>>(d, tiling_, par);
-                FDTD_CK(cudaGetLastError());
-                ++launches_;
+                if (wind_on_) k_march<R, true, 4, XF><<<grd, blk, fused_smem_, s>>>(d, tiling_, par);
+                else k_march<R, false, 4, XF><<<grd, blk, fused_smem_, s>>>(d, tiling_, par);
                 return;
             }
         }
-        if (wind_on_) k_march<R, true, 2><<<grd, blk, fused_smem_, s>>>(d, tiling_, par);
-        else k_march<R, false, 2><<<grd, blk, fused_smem_, s>>>(d, tiling_, par);
-        FDTD_CK(cudaGetLastError());
-        ++launches_;
+        if (wind_on_) k_march<R, true, 2, XF><<<grd, blk, fused_smem_, s>>>(d, tiling_, par);
+        else k_march<R, false, 2, XF><<<grd, blk, fused_smem_, s>>>(d, tiling_, par);
     }
 
     void enqueue_step(int par) {
@@ -1456,6 +1487,7 @@ class SolverImpl final : public SolverImplBase {
         int threads;
         size_t smem;
         bool wind;
+        bool xf;
         int par;
     };
     int device() const { return device_; }
@@ -1485,6 +1517,7 @@ class SolverImpl final : public SolverImplBase {
         v.threads = fused_threads_;
         v.smem = fused_smem_;
         v.wind = wind_on_;
+        v.xf = xf_;
         v.par = par_;
         return v;
     }
@@ -1550,6 +1583,7 @@ class SolverImpl final : public SolverImplBase {
     cudaGraphExec_t graph_exec_ = nullptr;
     bool graph_dirty_ = true;
     bool fused_ = false;
+    bool xf_ = true;  // marching kernel with the rarer features compiled in
     MarchTiling tiling_{};
     int fused_threads_ = 0;
     size_t fused_smem_ = 0;
@@ -1737,7 +1771,7 @@ class EnsembleImpl final : public EnsembleImplBase {
     }
 
     struct Group {
-        bool wind = false;
+        bool wind = false, xf = true;
         int VW = 0, threads = 0;
         size_t smem = 0;
         std::vector<int> members;  // indices into mem_
@@ -1795,9 +1829,9 @@ class EnsembleImpl final : public EnsembleImplBase {
         // share a launch with 256-thread blocks
         auto key_of = [&](size_t i) {
             const int cls = (v[i].threads + 63) / 64;
-            return std::array<int, 3>{v[i].wind ? 1 : 0, v[i].tile.VW, cls};
+            return std::array<int, 4>{v[i].wind ? 1 : 0, v[i].tile.VW, cls, v[i].xf ? 1 : 0};
         };
-        std::vector<std::array<int, 3>> keys;
+        std::vector<std::array<int, 4>> keys;
         std::vector<int> gi(mem_.size());
         for (size_t i = 0; i < mem_.size(); ++i) {
             const auto k = key_of(i);
@@ -1826,6 +1860,7 @@ class EnsembleImpl final : public EnsembleImplBase {
                 Group& g = groups_[k];
                 g.wind = keys[k][0] != 0;
                 g.VW = keys[k][1];
+                g.xf = keys[k][3] != 0;
                 struct Costed { long long cost; BatchWork w; };
                 std::vector<Costed> blocks;
                 for (int a = 0; a < static_cast<int>(g.members.size()); ++a) {
@@ -1868,29 +1903,36 @@ class EnsembleImpl final : public EnsembleImplBase {
         }
     }
 
-    static const void* kernel(const Group& g) {
+    template <bool XF>
+    static const void* kernel_xf(const Group& g) {
         if constexpr (sizeof(R) == 4) {
             if (g.VW == 4)
-                return g.wind ? reinterpret_cast<const void*>(k_march_batch<R, true, 4>)
-                              : reinterpret_cast<const void*>(k_march_batch<R, false, 4>);
+                return g.wind ? reinterpret_cast<const void*>(k_march_batch<R, true, 4, XF>)
+                              : reinterpret_cast<const void*>(k_march_batch<R, false, 4, XF>);
         }
-        return g.wind ? reinterpret_cast<const void*>(k_march_batch<R, true, 2>)
-                      : reinterpret_cast<const void*>(k_march_batch<R, false, 2>);
+        return g.wind ? reinterpret_cast<const void*>(k_march_batch<R, true, 2, XF>)
+                      : reinterpret_cast<const void*>(k_march_batch<R, false, 2, XF>);
     }
+    static const void* kernel(const Group& g) { return g.xf ? kernel_xf<true>(g) : kernel_xf<false>(g); }
 
-    void launch(const Group& g, int phase) {
+    template <bool XF>
+    void launch_xf(const Group& g, int phase) {
         const dim3 grd(static_cast<unsigned>(g.work.size())), blk(g.threads);
         const int nm = static_cast<int>(g.members.size());
         if constexpr (sizeof(R) == 4) {
             if (g.VW == 4) {
-                if (g.wind) k_march_batch<R, true, 4><<<grd, blk, g.smem, g.stream>>>(g.d_work, g.d_entries, nm, phase);
-                else k_march_batch<R, false, 4><<<grd, blk, g.smem, g.stream>>>(g.d_work, g.d_entries, nm, phase);
-                FDTD_CK(cudaGetLastError());
+                if (g.wind) k_march_batch<R, true, 4, XF><<<grd, blk, g.smem, g.stream>>>(g.d_work, g.d_entries, nm, phase);
+                else k_march_batch<R, false, 4, XF><<<grd, blk, g.smem, g.stream>>>(g.d_work, g.d_entries, nm, phase);
                 return;
             }
         }
-        if (g.wind) k_march_batch<R, true, 2><<<grd, blk, g.smem, g.stream>>>(g.d_work, g.d_entries, nm, phase);
-        else k_march_batch<R, false, 2><<<grd, blk, g.smem, g.stream>>>(g.d_work, g.d_entries, nm, phase);
+        if (g.wind) k_march_batch<R, true, 2, XF><<<grd, blk, g.smem, g.stream>>>(g.d_work, g.d_entries, nm, phase);
+        else k_march_batch<R, false, 2, XF><<<grd, blk, g.smem, g.stream>>>(g.d_work, g.d_entries, nm, phase);
+    }
+
+    void launch(const Group& g, int phase) {
+        if (g.xf) launch_xf<true>(g, phase);
+        else launch_xf<false>(g, phase);
         FDTD_CK(cudaGetLastError());
     }
 
