@@ -528,11 +528,7 @@ class SolverImpl final : public SolverImplBase {
             upload(d_ayP_, air_.fy);
         }
         build_pml_y(N);
-        const bool xf = needs_xf();
-        if (xf != xf_) {
-            xf_ = xf;
-            graph_dirty_ = true;
-        }
+        if (fused_) update_xf();
         upload(d_sy_[0], sy_); upload(d_sy_[1], fy_); upload(d_sy_[2], gy_);
         h2d(d_sdy_, sdy_.data(), NJ_);
         if (wind_on_) {
@@ -822,6 +818,15 @@ class SolverImpl final : public SolverImplBase {
         fused_threads_ = t.trows * nvec;
         fused_smem_ = smem;
         graph_dirty_ = true;
+        if (!sdy_.empty()) update_xf();
+    }
+
+    void update_xf() {
+        const bool xf = needs_xf(tiling_.VW);
+        if (xf != xf_) {
+            xf_ = xf;
+            graph_dirty_ = true;
+        }
     }
 
     template <bool XF>
@@ -845,26 +850,26 @@ class SolverImpl final : public SolverImplBase {
         }
     }
 
-    // the kernel form this domain launches: XF (inclusion mask, east TDBC,
-    // vectors with both y layers) only when the domain has one of them
-    bool needs_xf() const {
-        if (mask_on_ || tdbc_) return true;
-        for (int VW : {2, 4})
-            for (int jb = 0; jb < NJ_; jb += VW) {
-                int c = 0;
-                for (int e = 0; e < VW && jb + e < NJ_; ++e) {
-                    const int s = sdy_[jb + e];
-                    if (s) c = (c == 0 || c == s) ? s : 3;
-                }
-                if (c == 3) return true;
+    // the kernel form this domain launches with column vectors of VW: XF
+    // (inclusion mask, east TDBC, vectors with both y layers, an east column
+    // that starts a vector) only when the domain has one of them
+    bool needs_xf(int VW) const {
+        if (mask_on_ || tdbc_ || (!east_scalar<R, false>() && (NJ_ - 1) % VW == 0)) return true;
+        for (int jb = 0; jb < NJ_; jb += VW) {
+            int c = 0;
+            for (int e = 0; e < VW && jb + e < NJ_; ++e) {
+                const int s = sdy_[jb + e];
+                if (s) c = (c == 0 || c == s) ? s : 3;
             }
+            if (c == 3) return true;
+        }
         return false;
     }
 
     // resident blocks per SM of the marching kernel for a block shape
     int march_occupancy(int VW, int threads, size_t smem) const {
         int n = 0;
-        const void* k = xf_ ? march_kernel<true>(VW, wind_on_) : march_kernel<false>(VW, wind_on_);
+        const void* k = needs_xf(VW) ? march_kernel<true>(VW, wind_on_) : march_kernel<false>(VW, wind_on_);
         if (smem > 48 * 1024)
             FDTD_CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSmemMax)));
         FDTD_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, threads, smem));
