@@ -371,6 +371,29 @@ int fdtd_net_ensemble_predict(fdtd_net* const* nets, int members, const float* X
     });
 }
 
+int fdtd_ray_features(const float* P, int n, int n_par, int col_hs, int col_hr, int col_range, int n_rec, float* F,
+                      void* stream) {
+    if (n < 0 || (n > 0 && (!P || !F))) return bad("bad ray-feature arguments");
+    return guard([&] {
+        fdtd::mlp::ray_features(fdtd::mlp::RayFeatures{n_par, col_hs, col_hr, col_range, n_rec}, P, n, F, stream);
+    });
+}
+
+int fdtd_net_ensemble_predict_rays(fdtd_net* const* nets, int members, const float* P, int n, int n_par, int col_hs,
+                                   int col_hr, int col_range, int n_rec, float* mean, float* spread) {
+    if (!nets || members < 1 || (n > 0 && (!P || !mean || !spread))) return bad("bad ensemble arguments");
+    return guard([&] {
+        std::vector<fdtd::mlp::Net*> v;
+        for (int m = 0; m < members; ++m) {
+            if (!nets[m]) throw fdtd::SolverError{FDTD_ERR_ARG, "null ensemble member"};
+            v.push_back(nets[m]->n);
+        }
+        fdtd::mlp::ensemble_predict_rays(v.data(), members,
+                                         fdtd::mlp::RayFeatures{n_par, col_hs, col_hr, col_range, n_rec}, P, n, mean,
+                                         spread);
+    });
+}
+
 int fdtd_net_info(const fdtd_net* h, long long* launches, double* last_ms) {
     if (!h) return bad("null argument");
     if (launches) *launches = h->n->launches();

@@ -248,6 +248,29 @@ __global__ void k_cast(const float* __restrict__ W, int N, int K, __nv_bfloat16*
 
 __global__ void k_next_step(int* step) { *step += 1; }
 
+// one thread per output element of F [n][np + 2 nrec] (RayFeatures in
+// mlp.hpp); d2 - d1 is formed as 4 hs hr / (d1 + d2), free of cancellation
+__global__ void k_ray_features(const float* __restrict__ P, long long n, int np, int chs, int chr, int crange,
+                               int nrec, float* __restrict__ F) {
+    const int nf = np + 2 * nrec;
+    const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= n * nf) return;
+    const long long r = t / nf;
+    const int c = static_cast<int>(t - r * nf);
+    const float* p = P + r * np;
+    float v;
+    if (c < np) {
+        v = p[c];
+    } else {
+        const int k = (c - np) % nrec;
+        const float hs = p[chs], hr = p[chr];
+        const float rk = p[crange] * static_cast<float>(k + 1) / static_cast<float>(nrec);
+        const float a = rk * rk + (hs - hr) * (hs - hr), b = rk * rk + (hs + hr) * (hs + hr);
+        v = (c - np < nrec) ? logf(4.0f * hs * hr) - logf(sqrtf(a) + sqrtf(b)) : 10.0f * log10f(b / a);
+    }
+    F[t] = v;
+}
+
 // one warp per query: mean over `members` predictions Y [members][n][nout]
 // and the root mean square over the outputs of their standard deviation
 __global__ void k_ensemble_stats(const float* __restrict__ Y, int members, int n, int nout, float* __restrict__ mean,
@@ -785,24 +808,54 @@ int Net::n_in() const { return impl_->n_in(); }
 int Net::n_out() const { return impl_->n_out(); }
 int Net::device() const { return impl_->device(); }
 
-void ensemble_predict(Net* const* nets, int members, const float* X, int n, float* mean, float* spread) {
+void RayFeatures::validate() const {
+    if (n_par < 1 || n_rec < 1 || col_hs < 0 || col_hs >= n_par || col_hr < 0 || col_hr >= n_par || col_range < 0 ||
+        col_range >= n_par)
+        bad("ray features: need n_par, n_rec >= 1 and the height and range columns inside the row");
+}
+
+static void launch_ray_features(const RayFeatures& g, const float* P, int n, float* F, cudaStream_t s) {
+    const long long total = static_cast<long long>(n) * g.n_out();
+    if (total == 0) return;
+    k_ray_features<<<static_cast<unsigned>((total + 255) / 256), 256, 0, s>>>(P, n, g.n_par, g.col_hs, g.col_hr,
+                                                                              g.col_range, g.n_rec, F);
+    ck(cudaGetLastError(), "ray features");
+}
+
+void ray_features(const RayFeatures& g, const float* P, int n, float* F, void* stream) {
+    g.validate();
+    if (n < 0) bad("ray features: n >= 0");
+    launch_ray_features(g, P, n, F, static_cast<cudaStream_t>(stream));
+}
+
+// mean and disagreement of the members over host rows X [n][nx]; with g,
+// X holds query rows and the networks read their ray features
+static void ensemble_run(Net* const* nets, int members, const RayFeatures* g, const float* X, int n, float* mean,
+                         float* spread) {
     if (members < 1 || !nets || n < 0) bad("ensemble: need at least one network and n >= 0");
     const int nin = nets[0]->n_in(), nout = nets[0]->n_out(), dev = nets[0]->device();
     for (int m = 0; m < members; ++m)
         if (!nets[m] || nets[m]->n_in() != nin || nets[m]->n_out() != nout || nets[m]->device() != dev)
             bad("ensemble members must share inputs, outputs and device");
+    if (g) {
+        g->validate();
+        if (g->n_out() != nin) bad("ensemble: the networks' inputs are not the query rows' ray features");
+    }
+    const int nx = g ? g->n_par : nin;
     if (n == 0) return;
     ck(cudaSetDevice(dev), "cudaSetDevice");
     const int chunk = std::min(n, 1 << 18);
     Buf xd(sizeof(float) * static_cast<size_t>(chunk) * nin), yd(sizeof(float) * static_cast<size_t>(chunk) * nout * members),
-        md(sizeof(float) * static_cast<size_t>(chunk) * nout), sd(sizeof(float) * chunk);
+        md(sizeof(float) * static_cast<size_t>(chunk) * nout), sd(sizeof(float) * chunk),
+        pd(g ? sizeof(float) * static_cast<size_t>(chunk) * nx : 0);
     cudaStream_t s;
     ck(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
     try {
         for (int r0 = 0; r0 < n; r0 += chunk) {
             const int c = std::min(chunk, n - r0);
-            ck(cudaMemcpyAsync(xd.p, X + static_cast<size_t>(r0) * nin, sizeof(float) * c * nin, cudaMemcpyHostToDevice,
-                               s), "inputs");
+            ck(cudaMemcpyAsync(g ? pd.p : xd.p, X + static_cast<size_t>(r0) * nx, sizeof(float) * c * nx,
+                               cudaMemcpyHostToDevice, s), "inputs");
+            if (g) launch_ray_features(*g, pd.as<float>(), c, xd.as<float>(), s);
             for (int m = 0; m < members; ++m)
                 nets[m]->predict_device(xd.as<float>(), c, yd.as<float>() + static_cast<size_t>(m) * c * nout, s);
             k_ensemble_stats<<<(c + 7) / 8, 256, 0, s>>>(yd.as<float>(), members, c, nout, md.as<float>(), sd.as<float>());
@@ -818,6 +871,15 @@ void ensemble_predict(Net* const* nets, int members, const float* X, int n, floa
         throw;
     }
     cudaStreamDestroy(s);
+}
+
+void ensemble_predict(Net* const* nets, int members, const float* X, int n, float* mean, float* spread) {
+    ensemble_run(nets, members, nullptr, X, n, mean, spread);
+}
+
+void ensemble_predict_rays(Net* const* nets, int members, const RayFeatures& g, const float* P, int n, float* mean,
+                           float* spread) {
+    ensemble_run(nets, members, &g, P, n, mean, spread);
 }
 double Net::last_device_ms() const { return impl_->last_ms(); }
 

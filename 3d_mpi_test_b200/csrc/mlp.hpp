@@ -67,5 +67,25 @@ class Net {
 // device, so only the mean and the disagreement cross back to the host.
 void ensemble_predict(Net* const* nets, int members, const float* X, int n, float* mean, float* spread);
 
+// Ray-geometry inputs of excess-attenuation queries. A query row P [n_par]
+// holds the source height, receiver height and farthest range at columns
+// col_hs, col_hr, col_range; its network input row is P followed, per
+// receiver k < n_rec at range r_k = range (k + 1) / n_rec, by
+// ln(d2 - d1) and then, for every k, 20 log10(d2 / d1), with the direct
+// and ground-reflected path lengths d1 = |(r_k, hs - hr)| and
+// d2 = |(r_k, hs + hr)| (flat-ground image source).
+struct RayFeatures {
+    int n_par, col_hs, col_hr, col_range, n_rec;
+    int n_out() const { return n_par + 2 * n_rec; }
+    void validate() const;
+};
+// F [n][g.n_out()] from P [n][g.n_par], device buffers, on a stream
+void ray_features(const RayFeatures& g, const float* P, int n, float* F, void* stream);
+// ensemble_predict of host query rows P [n][g.n_par]: the rows cross to the
+// device as they are and the networks (n_in == g.n_out()) read their ray
+// features, formed there
+void ensemble_predict_rays(Net* const* nets, int members, const RayFeatures& g, const float* P, int n, float* mean,
+                           float* spread);
+
 }  // namespace mlp
 }  // namespace fdtd

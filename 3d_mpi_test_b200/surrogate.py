@@ -15,6 +15,10 @@ from typing import Optional, Tuple
 import numpy as np
 
 from . import FDTD_ERR_ARG, FdtdError, load_library
+from .surrogate_data import N_REC, PARAMS, features
+
+# query-row geometry of the ray features: (n_par, col_hs, col_hr, col_range, n_rec)
+RAYS = (len(PARAMS), PARAMS.index("source_height"), PARAMS.index("receiver_height"), PARAMS.index("range"), N_REC)
 
 EPI_F32, EPI_BIAS_RELU_T, EPI_BIAS_F32, EPI_RELU_GRAD_T, EPI_BIAS_RELU = 0, 1, 2, 3, 4
 
@@ -42,6 +46,8 @@ def _declare(L) -> None:
         "fdtd_net_predict_device": ([vp, vp, i, vp, vp], i),
         "fdtd_net_info": ([vp, ll, d], i),
         "fdtd_net_ensemble_predict": ([ctypes.POINTER(vp), i, _FP, i, _FP, _FP], i),
+        "fdtd_ray_features": ([vp, i, i, i, i, i, i, vp, vp], i),
+        "fdtd_net_ensemble_predict_rays": ([ctypes.POINTER(vp), i, _FP, i, i, i, i, i, i, _FP, _FP], i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -67,6 +73,13 @@ def _f32(a) -> np.ndarray:
 
 def _fp(a: np.ndarray):
     return a.ctypes.data_as(_FP)
+
+
+def ray_features(P_ptr: int, n: int, F_ptr: int, stream: int = 0, lib_path: Optional[str] = None) -> None:
+    """Network inputs F [n][27] (device) of query rows P [n][11] (device):
+    ``surrogate_data.features`` formed on the device, on a stream."""
+    L = _lib(lib_path)
+    _check(L, L.fdtd_ray_features(P_ptr, n, *RAYS, F_ptr, stream))
 
 
 def tc_gemm(epilogue: int, A, B, out, bias=None, mask=None, outT=None, device: int = 0,
@@ -183,8 +196,10 @@ class Surrogate:
 
     Inputs: the 11 parameters of ``surrogate_data.PARAMS`` (flow
     resistivity as log10, porosity, tortuosity, layer depth, source and
-    receiver heights, range, hill height and half-width, u*, z0). Outputs:
-    excess attenuation [n_rec][n_band] in dB (``surrogate_data`` layout).
+    receiver heights, range, hill height and half-width, u*, z0); the
+    networks see them with the receivers' ray geometry appended
+    (``surrogate_data.features``, 27 inputs). Outputs: excess attenuation
+    [n_rec][n_band] in dB (``surrogate_data`` layout).
     Each member is trained on a bootstrap resample of the data from its own
     initialisation. A query is answered by the FDTD solver instead of the
     networks when it lies outside the training hull (the per-parameter
@@ -214,14 +229,15 @@ class Surrogate:
         ok = np.isfinite(EA).all(axis=1) & np.isfinite(X).all(axis=1)
         X, EA = X[ok], EA[ok]
         self.lo, self.hi = X.min(axis=0), X.max(axis=0)
+        F = features(X)
         self.close()
         losses = []
         rng = np.random.default_rng(self.seed)
         for m in range(self.members):
-            net = Net(X.shape[1], EA.shape[1], width=self.width, hidden=self.hidden, batch=self.batch,
+            net = Net(F.shape[1], EA.shape[1], width=self.width, hidden=self.hidden, batch=self.batch,
                       seed=self.seed * 1000 + m, device=self.device, lib_path=self._lib_path)
             pick = rng.integers(0, len(X), len(X))  # bootstrap resample
-            net.set_data(X[pick], EA[pick])
+            net.set_data(F[pick], EA[pick])
             losses.append(net.train(steps, lr=lr, lr_final=lr_final, seed=self.seed * 1000 + m, report=100,
                                     weight_decay=weight_decay))
             self.nets.append(net)
@@ -233,17 +249,20 @@ class Surrogate:
 
     def predict(self, X) -> Tuple[np.ndarray, np.ndarray]:
         """Member mean [n][outputs] and the disagreement [n] (root mean
-        square over the outputs of the standard deviation across members, dB)."""
-        if not self.nets or not isinstance(self.nets[0], Net):  # stand-in members (tests)
+        square over the outputs of the standard deviation across members, dB)
+        of the parameter rows X [n][11]."""
+        if not self.nets or not isinstance(self.nets[0], Net):  # stand-in members (tests) see the parameters
             ys = np.stack([n.predict(X) for n in self.nets])
             return ys.mean(axis=0), np.sqrt(ys.var(axis=0).mean(axis=1))
         X = _f32(np.atleast_2d(X))
+        if X.shape[1] != len(PARAMS):
+            raise FdtdError(FDTD_ERR_ARG, f"queries need {len(PARAMS)} parameters per row")
         net0 = self.nets[0]
         mean = np.empty((X.shape[0], net0.n_out), np.float32)
         spread = np.empty(X.shape[0], np.float32)
         arr = (ctypes.c_void_p * len(self.nets))(*[n._h.value for n in self.nets])
-        _check(net0._L, net0._L.fdtd_net_ensemble_predict(arr, len(self.nets), _fp(X), X.shape[0], _fp(mean),
-                                                          _fp(spread)))
+        _check(net0._L, net0._L.fdtd_net_ensemble_predict_rays(arr, len(self.nets), _fp(X), X.shape[0], *RAYS,
+                                                               _fp(mean), _fp(spread)))
         return mean, spread
 
     def query(self, X, tol_db: float = 1.0, fdtd=None) -> Tuple[np.ndarray, np.ndarray]:

@@ -410,24 +410,34 @@ def run_surrogate(queries: int = 1_000_000, members: int = 5, steps: int = 12000
     err = np.abs(y - Ete)
     kept = spread <= 1.0
     per_band = err.reshape(len(Xte), sd.N_REC, len(sd.BANDS)).mean(axis=(0, 1))
-    # inference: queries resident in HBM, every member, CUDA events inside the library
+    # inference: query rows resident in HBM; the ray-feature kernel (CUDA
+    # events on its stream) and every member (CUDA events inside the library)
     Xq = sd.draw(99, queries).astype(np.float32)
-    xd = torch.from_numpy(Xq).cuda(device)
+    pq = torch.from_numpy(Xq).cuda(device)
+    xd = torch.empty((queries, sd.N_FEATURES), dtype=torch.float32, device=f"cuda:{device}")
     yd = torch.empty((queries, Etr.shape[1]), dtype=torch.float32, device=f"cuda:{device}")
+    st = torch.cuda.current_stream(device)
+    sur.ray_features(pq.data_ptr(), 4096, xd.data_ptr(), st.cuda_stream)  # warm-up
     for n in s.nets:
         n.predict_device(xd.data_ptr(), 4096, yd.data_ptr())  # warm-up
     l0 = sum(n.info()["launches"] for n in s.nets)
-    ms = 0.0
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(device)
+    ev0.record(st)
+    sur.ray_features(pq.data_ptr(), queries, xd.data_ptr(), st.cuda_stream)
+    ev1.record(st)
+    torch.cuda.synchronize(device)
+    ms = ev0.elapsed_time(ev1)
     for n in s.nets:
         n.predict_device(xd.data_ptr(), queries, yd.data_ptr())
         ms += n.info()["last_device_ms"]
-    launches = sum(n.info()["launches"] for n in s.nets) - l0
+    launches = sum(n.info()["launches"] for n in s.nets) - l0 + 1  # + the ray-feature kernel
     width, K0, NO = 512, 64, 256  # padded GEMM shapes of one member
     flop_padded = 2.0 * (K0 * width + 3 * width * width + width * NO)
-    flop_alg = 2.0 * (11 * width + 3 * width * width + width * Etr.shape[1])
+    flop_alg = 2.0 * (sd.N_FEATURES * width + 3 * width * width + width * Etr.shape[1])
     peak, peak_kind = bf16_peak()
     tflops = members * queries * flop_padded / (ms * 1e-3) / 1e12
-    # end to end from host arrays: H2D of the queries, D2H of the answers
+    # end to end from host parameter arrays: features, H2D of the inputs, D2H of the answers
     t0 = time.perf_counter()
     s.predict(Xq)
     e2e_s = time.perf_counter() - t0
@@ -438,7 +448,8 @@ def run_surrogate(queries: int = 1_000_000, members: int = 5, steps: int = 12000
     fdtd_s = (time.perf_counter() - t0) / nf
     s.close()
     return {
-        "members": members, "layers": "11 -> 4 x 512 ReLU -> 136 (17 bands x 8 receivers), bf16 weights, FP32 accumulate",
+        "members": members, "layers": "11 parameters + 16 ray-geometry features -> 4 x 512 ReLU -> 136 (17 bands x 8 receivers), "
+                                    "bf16 weights, FP32 accumulate",
         "train": {"samples": int(len(Xtr)), "steps_per_member": steps, "batch": 256, "wall_s": round(train_s, 2),
                   "device_ms": round(train_ms, 1), "final_loss_normalised": [round(float(v), 5) for v in losses]},
         "held_out": {"samples": int(len(Xte)), "mae_db": round(float(err.mean()), 3),

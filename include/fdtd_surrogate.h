@@ -76,6 +76,23 @@ int fdtd_net_predict_device(fdtd_net *h, const float *X, int n, float *Y, void *
 int fdtd_net_ensemble_predict(fdtd_net *const *nets, int members, const float *X, int n, float *mean,
                               float *spread);
 
+/* Ray-geometry network inputs of excess-attenuation queries, formed on the
+ * device. A query row P [n_par] holds the source height, the receiver
+ * height and the farthest range at columns col_hs, col_hr, col_range. Its
+ * network input row [n_par + 2 n_rec] is P, then ln(d2 - d1) for every
+ * receiver k < n_rec at range r_k = range (k + 1) / n_rec, then
+ * 20 log10(d2 / d1) for every k, with d1 = |(r_k, hs - hr)| the direct and
+ * d2 = |(r_k, hs + hr)| the ground-reflected path (flat-ground image
+ * source). F [n][n_par + 2 n_rec] from P [n][n_par], device buffers, on a
+ * cudaStream_t (not synchronised). */
+int fdtd_ray_features(const float *P, int n, int n_par, int col_hs, int col_hr, int col_range, int n_rec, float *F,
+                      void *stream);
+/* fdtd_net_ensemble_predict of host query rows P [n][n_par]: the rows cross
+ * to the device as they are and the members (n_in = n_par + 2 n_rec) read
+ * their ray features, formed there */
+int fdtd_net_ensemble_predict_rays(fdtd_net *const *nets, int members, const float *P, int n, int n_par, int col_hs,
+                                   int col_hr, int col_range, int n_rec, float *mean, float *spread);
+
 /* kernel launches so far and device milliseconds of the last train /
  * predict call */
 int fdtd_net_info(const fdtd_net *h, long long *launches, double *last_ms);

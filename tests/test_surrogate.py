@@ -125,11 +125,31 @@ def test_network_answers_faster_than_fdtd(trained):
     assert fdtd_per_query / net_per_query > 1000, (fdtd_per_query, net_per_query)
 
 
+def _device_features(X):
+    import torch
+
+    P = torch.from_numpy(np.ascontiguousarray(X, np.float32)).cuda()
+    F = torch.empty((len(X), sd.N_FEATURES), dtype=torch.float32, device="cuda")
+    sur.ray_features(P.data_ptr(), len(X), F.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    return F.cpu().numpy()
+
+
+@pytest.mark.gpu
+def test_ray_features_on_device_match_host():
+    X = sd.draw(5, 20000).astype(np.float32)
+    F = _device_features(X)
+    H = sd.features(X)
+    assert F.shape == H.shape == (len(X), 27)
+    np.testing.assert_array_equal(F[:, :11], X)
+    np.testing.assert_allclose(F[:, 11:], H[:, 11:], rtol=1e-5, atol=2e-5)
+
+
 @pytest.mark.gpu
 def test_device_ensemble_reduction_matches_members(trained):
     s, _, Xte, _ = trained
     mean, spread = s.predict(Xte[:300])
-    ys = np.stack([n.predict(Xte[:300]) for n in s.nets]).astype(np.float64)
+    ys = np.stack([n.predict(_device_features(Xte[:300])) for n in s.nets]).astype(np.float64)
     np.testing.assert_allclose(mean, ys.mean(axis=0), rtol=0, atol=1e-4)
     np.testing.assert_allclose(spread, np.sqrt(ys.var(axis=0).mean(axis=1)), rtol=1e-4, atol=1e-4)
 
