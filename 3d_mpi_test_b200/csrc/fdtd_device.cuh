@@ -240,7 +240,10 @@ __device__ __forceinline__ Arr<R, 1> el(const Arr<R, N>& a, int e) {
 // added to dp in the reference's order. x and z layers are uniform over the
 // columns; the y layer is per column (ysp), all active columns on side ysv
 // (1 or 2). Columns outside the y layer take zero y coefficients, which
-// adds exact zeros; their slab reads stay inside the padded slab row.
+// adds exact zeros; their slab reads stay inside the padded slab row. The
+// reference multiplies every term by dt last; here dt (and gamma P0 or the
+// averaging factor) is folded into the layer coefficients first, which
+// changes only the last bits of the rounding.
 template <typename R, int N>
 __device__ __forceinline__ void pml_dp_v(const Dev<R>& d, int i, int jb, int k, int xs, int ysp, int ysv, int zs,
                                          R ax, const Arr<R, N>& ay, R az, const Arr<R, N>& gu, const Arr<R, N>& gv,
@@ -248,7 +251,8 @@ __device__ __forceinline__ void pml_dp_v(const Dev<R>& d, int i, int jb, int k, 
                                          const PmlC<R>& Z, Arr<R, N>& dp) {
     const R gP0 = d.gP0, dt = d.dt;
     const int NJ = d.NJ;
-    Arr<R, N> dQux{}, dQvx{}, dQwx{}, QpX{}, dQvy{}, dQwy{}, QpY{};
+    const R xS = X.s * dt, xF = X.f * gP0 * dt, zS = Z.s * dt, zF = Z.f * gP0 * dt;
+    Arr<R, N> dQux{}, dQvx{}, dQwx{}, QpX{}, dQvy{}, dQwy{}, QpY{}, yS{};
     PmlC<R> Y[N];
     if (xs) {
         const Slab<R>& S = d.sl[xs - 1];
@@ -264,7 +268,7 @@ __device__ __forceinline__ void pml_dp_v(const Dev<R>& d, int i, int jb, int k, 
             dQux.e[e] = ax * (u1.e[e] - u0.e[e]);
             dQvx.e[e] = ay.e[e] * (v1 - v0.e[e]);
             dQwx.e[e] = az * (w1.e[e] - w0.e[e]);
-            dp.e[e] += X.f * gP0 * gu.e[e] * dt - X.s * (pn.e[e] + gP0 * (dQvx.e[e] + dQwx.e[e])) * dt;
+            dp.e[e] += xF * gu.e[e] - xS * (pn.e[e] + gP0 * (dQvx.e[e] + dQwx.e[e]));
         }
     }
     sched_fence();
@@ -283,9 +287,10 @@ __device__ __forceinline__ void pml_dp_v(const Dev<R>& d, int i, int jb, int k, 
             const R dQuy = ax * (u1.e[e] - u0.e[e]);
             dQvy.e[e] = ay.e[e] * (v1 - v0.e[e]);
             dQwy.e[e] = az * (w1.e[e] - w0.e[e]);
-            dp.e[e] += Y[e].f * gP0 * gv.e[e] * dt - Y[e].s * (pn.e[e] + gP0 * (dQuy + dQwy.e[e])) * dt;
+            yS.e[e] = Y[e].s * dt;
+            dp.e[e] += (Y[e].f * gP0 * dt) * gv.e[e] - yS.e[e] * (pn.e[e] + gP0 * (dQuy + dQwy.e[e]));
             if (xs)
-                dp.e[e] += -(QpX.e[e] * X.s * Y[e].s + gP0 * (X.g * Y[e].s * dQux.e[e] + Y[e].g * X.s * dQvx.e[e])) * dt;
+                dp.e[e] -= QpX.e[e] * (X.s * yS.e[e]) + gP0 * ((X.g * yS.e[e]) * dQux.e[e] + (Y[e].g * xS) * dQvx.e[e]);
         }
     }
     sched_fence();
@@ -300,12 +305,11 @@ __device__ __forceinline__ void pml_dp_v(const Dev<R>& d, int i, int jb, int k, 
             const R v1 = e + 1 < N ? v0.e[e + 1 < N ? e + 1 : 0] : vn;
             const R dQuz = ax * (u1.e[e] - u0.e[e]);
             const R dQvz = ay.e[e] * (v1 - v0.e[e]);
-            dp.e[e] += Z.f * gP0 * gw.e[e] * dt - Z.s * (pn.e[e] + gP0 * (dQuz + dQvz)) * dt;
-            if (xs)
-                dp.e[e] += -(QpX.e[e] * X.s * Z.s + gP0 * (X.g * Z.s * dQux.e[e] + Z.g * X.s * dQwx.e[e])) * dt;
+            dp.e[e] += zF * gw.e[e] - zS * (pn.e[e] + gP0 * (dQuz + dQvz));
+            if (xs) dp.e[e] -= QpX.e[e] * (X.s * zS) + gP0 * ((X.g * zS) * dQux.e[e] + (Z.g * xS) * dQwx.e[e]);
             if (ysv)
-                dp.e[e] +=
-                    -(QpY.e[e] * Y[e].s * Z.s + gP0 * (Y[e].g * Z.s * dQvy.e[e] + Z.g * Y[e].s * dQwy.e[e])) * dt;
+                dp.e[e] -=
+                    QpY.e[e] * (Y[e].s * zS) + gP0 * ((Y[e].g * zS) * dQvy.e[e] + (Z.g * yS.e[e]) * dQwy.e[e]);
         }
     }
 }
@@ -392,7 +396,8 @@ __device__ __forceinline__ Arr<R, N> p_vec(const Dev<R>& d, const PlaneC<R>& pc,
 
 // -------------------------------------------------- velocity increment parts
 // PML part of the air velocity increment of N columns (air::cal_fuvw,
-// air.cpp:1476-1949); same column conventions as pml_dp_v. p0, pim, pjm,
+// air.cpp:1476-1949); same column conventions and folding of dt as
+// pml_dp_v. p0, pim, pjm,
 // pkm: the scheme's pressure at the nodes and at i-1, j-1, g-1. qp_old: the
 // slabs' Qp buffers still hold the values from before this step's pressure
 // update (single-pass form), so the advanced Qp is formed here as
@@ -406,6 +411,7 @@ __device__ __forceinline__ void pml_dvel_v(const Dev<R>& d, int i, int jb, int k
                                            const PmlC<R>& X, const PmlC<R>& Z, Arr<R, N>& du, Arr<R, N>& dv,
                                            Arr<R, N>& dw) {
     const R A = d.Aav, dt = d.dt;
+    const R xS = X.s * dt, zS = Z.s * dt;
     // backward differences of the slab's Qp advanced to this step
     auto bq = [&](const Slab<R>& S, int q, Arr<R, N>& bx, Arr<R, N>& by, Arr<R, N>& bz) {
         const R* Q = S.rd[3];
@@ -426,7 +432,7 @@ __device__ __forceinline__ void pml_dvel_v(const Dev<R>& d, int i, int jb, int k
         }
     };
     Arr<R, N> bxX{}, byX{}, bzX{}, bxY{}, byY{}, bzY{};
-    Arr<R, N> QuX{}, QvX{}, QwX{}, QuY{}, QvY{}, QwY{};
+    Arr<R, N> QuX{}, QvX{}, QwX{}, QuY{}, QvY{}, QwY{}, yS{};
     PmlC<R> Y[N];
     if (xs) {
         const Slab<R>& S = d.sl[xs - 1];
@@ -439,9 +445,9 @@ __device__ __forceinline__ void pml_dvel_v(const Dev<R>& d, int i, int jb, int k
         }
 #pragma unroll
         for (int e = 0; e < N; ++e) {
-            du.e[e] += -X.s * u0.e[e] * dt + X.f * (A * gpX.e[e]) * dt;
-            dv.e[e] += -X.s * (v0.e[e] + A * byX.e[e]) * dt;
-            dw.e[e] += -X.s * (w0.e[e] + A * bzX.e[e]) * dt;
+            du.e[e] += (X.f * A * dt) * gpX.e[e] - xS * u0.e[e];
+            dv.e[e] -= xS * (v0.e[e] + A * byX.e[e]);
+            dw.e[e] -= xS * (w0.e[e] + A * bzX.e[e]);
         }
     }
     sched_fence();
@@ -457,13 +463,15 @@ __device__ __forceinline__ void pml_dvel_v(const Dev<R>& d, int i, int jb, int k
 #pragma unroll
         for (int e = 0; e < N; ++e) {
             Y[e] = pml_y(d, (ysp >> (2 * e)) & 3, jb + e);
-            du.e[e] += -Y[e].s * (u0.e[e] + A * bxY.e[e]) * dt;
-            dv.e[e] += Y[e].f * A * gpY.e[e] * dt - Y[e].s * v0.e[e] * dt;
-            dw.e[e] += -Y[e].s * (w0.e[e] + A * bzY.e[e]) * dt;
+            yS.e[e] = Y[e].s * dt;
+            du.e[e] -= yS.e[e] * (u0.e[e] + A * bxY.e[e]);
+            dv.e[e] += (Y[e].f * A * dt) * gpY.e[e] - yS.e[e] * v0.e[e];
+            dw.e[e] -= yS.e[e] * (w0.e[e] + A * bzY.e[e]);
             if (xs) {
-                du.e[e] += -(QuX.e[e] * X.s * Y[e].s + X.g * Y[e].s * A * bxX.e[e]) * dt;
-                dv.e[e] += -(QvX.e[e] * X.s * Y[e].s + Y[e].g * X.s * A * byX.e[e]) * dt;
-                dw.e[e] += -QwX.e[e] * X.s * Y[e].s * dt;
+                const R cXY = X.s * yS.e[e];
+                du.e[e] -= QuX.e[e] * cXY + (X.g * yS.e[e] * A) * bxX.e[e];
+                dv.e[e] -= QvX.e[e] * cXY + (Y[e].g * xS * A) * byX.e[e];
+                dw.e[e] -= QwX.e[e] * cXY;
             }
         }
     }
@@ -475,18 +483,20 @@ __device__ __forceinline__ void pml_dvel_v(const Dev<R>& d, int i, int jb, int k
         bq(S, q, bxZ, byZ, bzZ);
 #pragma unroll
         for (int e = 0; e < N; ++e) {
-            du.e[e] += -Z.s * (u0.e[e] + A * bxZ.e[e]) * dt;
-            dv.e[e] += -Z.s * (v0.e[e] + A * byZ.e[e]) * dt;
-            dw.e[e] += Z.f * A * gpZ.e[e] * dt - Z.s * w0.e[e] * dt;
+            du.e[e] -= zS * (u0.e[e] + A * bxZ.e[e]);
+            dv.e[e] -= zS * (v0.e[e] + A * byZ.e[e]);
+            dw.e[e] += (Z.f * A * dt) * gpZ.e[e] - zS * w0.e[e];
             if (xs) {
-                du.e[e] += -(QuX.e[e] * X.s * Z.s + X.g * Z.s * A * bxX.e[e]) * dt;
-                dv.e[e] += -QvX.e[e] * X.s * Z.s * dt;
-                dw.e[e] += -(QwX.e[e] * X.s * Z.s + Z.g * X.s * A * bzX.e[e]) * dt;
+                const R cXZ = X.s * zS;
+                du.e[e] -= QuX.e[e] * cXZ + (X.g * zS * A) * bxX.e[e];
+                dv.e[e] -= QvX.e[e] * cXZ;
+                dw.e[e] -= QwX.e[e] * cXZ + (Z.g * xS * A) * bzX.e[e];
             }
             if (ysv) {
-                du.e[e] += -QuY.e[e] * Y[e].s * Z.s * dt;
-                dv.e[e] += -(QvY.e[e] * Y[e].s * Z.s + Y[e].g * Z.s * A * byY.e[e]) * dt;
-                dw.e[e] += -(QwY.e[e] * Y[e].s * Z.s + Z.g * Y[e].s * A * bzY.e[e]) * dt;
+                const R cYZ = Y[e].s * zS;
+                du.e[e] -= QuY.e[e] * cYZ;
+                dv.e[e] -= QvY.e[e] * cYZ + (Y[e].g * zS * A) * byY.e[e];
+                dw.e[e] -= QwY.e[e] * cYZ + (Z.g * yS.e[e] * A) * bzY.e[e];
             }
         }
     }
