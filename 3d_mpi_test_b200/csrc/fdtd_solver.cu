@@ -144,7 +144,7 @@ class SolverImpl final : public SolverImplBase {
         FDTD_CK(cudaSetDevice(device_));
         cudaDeviceProp prop{};
         FDTD_CK(cudaGetDeviceProperties(&prop, device_));
-        if (prop.major != 10) fail(-3, "this build targets sm_100a (B200); device is sm_" + std::to_string(prop.major) +
+        if (prop.major != 10) fail(-3, "the library is compiled for sm_100a (B200) only; device is sm_" + std::to_string(prop.major) +
                                            std::to_string(prop.minor));
         validate_and_build_geometry();
         // every transfer below is ordered on this stream, so host uploads at
