@@ -47,6 +47,20 @@ def test_dataset_shape():
     assert np.all(Xtr >= lo - 1e-6) and np.all(Xtr <= hi + 1e-6)
 
 
+def test_ray_features_follow_the_image_source_geometry():
+    X = sd.draw(3, 500)
+    F = sd.features(X)
+    assert F.shape == (500, sd.N_FEATURES) and sd.N_FEATURES == 27
+    np.testing.assert_array_equal(F[:, :11], X.astype(np.float32))
+    hs, hr = X[:, sd.PARAMS.index("source_height")], X[:, sd.PARAMS.index("receiver_height")]
+    R = X[:, sd.PARAMS.index("range")]
+    for k in range(sd.N_REC):
+        r = R * (k + 1) / sd.N_REC
+        d1, d2 = np.hypot(r, hs - hr), np.hypot(r, hs + hr)  # direct and ground-reflected paths
+        np.testing.assert_allclose(F[:, 11 + k], np.log(d2 - d1), rtol=1e-5, atol=1e-5)
+        np.testing.assert_allclose(F[:, 11 + sd.N_REC + k], 20 * np.log10(d2 / d1), rtol=1e-5, atol=1e-5)
+
+
 def test_query_routing_with_stand_in_members():
     s = sur.Surrogate(members=3)
     s.lo, s.hi = np.zeros(11, np.float32), np.ones(11, np.float32)
