@@ -73,6 +73,19 @@ def test_null_arguments(lib):
     assert lib.fdtd_state_elems(None) == 0
 
 
+def test_ray_feature_arguments_are_checked_before_any_device_work(lib):
+    fn = lib.fdtd_ray_features
+    fn.argtypes = [ctypes.c_void_p] + [ctypes.c_int] * 6 + [ctypes.c_void_p, ctypes.c_void_p]
+    fn.restype = ctypes.c_int
+    buf = ctypes.c_void_p(16)  # never dereferenced: every call below is rejected first
+    assert fn(None, 1, 11, 4, 5, 6, 8, buf, None) == pkg.FDTD_ERR_ARG  # null rows
+    assert fn(buf, -1, 11, 4, 5, 6, 8, buf, None) == pkg.FDTD_ERR_ARG  # negative count
+    assert fn(buf, 1, 11, 4, 5, 11, 8, buf, None) == pkg.FDTD_ERR_ARG  # range column outside the row
+    assert fn(buf, 1, 11, 4, 5, 6, 0, buf, None) == pkg.FDTD_ERR_ARG  # no receivers
+    assert b"ray features" in lib.fdtd_last_error()
+    assert fn(None, 0, 11, 4, 5, 6, 8, None, None) == pkg.FDTD_OK  # nothing to do
+
+
 def test_package_fails_loudly_without_library(tmp_path):
     with pytest.raises(pkg.FdtdError) as e:
         pkg.load_library(str(tmp_path / "libfdtd_b200.so"))
