@@ -96,6 +96,7 @@ struct Dev {
     int nrec;
     const long long* rec_node;  // unified index or -1 (outside window / not strictly interior)
     double* rec_out;            // [step][nrec]
+    int rec_steps;              // steps rec_out holds; a step at or past it records nothing
     int* counters;              // step counters (see k_pressure)
     int* status;                // bit 0: non-finite pressure seen; bit 1: staged-copy timeout
     long long wait_spin;        // polls of a staged-copy wait before it reports a timeout
@@ -735,7 +736,7 @@ __global__ void __launch_bounds__(256) k_pressure(__grid_constant__ const Dev<R>
     const int g = blockIdx.z;
     if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0) {
         const int t = threadIdx.y * blockDim.x + threadIdx.x;
-        if (t < d.nrec) {
+        if (t < d.nrec && step < d.rec_steps) {
             const long long n = d.rec_node[t];
             double val = 0.0;
             if (n >= 0) val = static_cast<double>(d.pold[n]);

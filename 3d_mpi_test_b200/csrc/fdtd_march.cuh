@@ -84,7 +84,7 @@ template <typename R>
 __device__ __forceinline__ void march_bookkeeping(const Dev<R>& d, int par, int step, bool first_block) {
     if (first_block) {
         const int tt = threadIdx.x;
-        for (int r = tt; r < d.nrec; r += blockDim.x) {  // blocks may be narrower than the receiver list
+        for (int r = tt; r < d.nrec && step < d.rec_steps; r += blockDim.x) {  // blocks may be narrower than the receiver list
             const long long n = d.rec_node[r];
             double val = 0.0;
             if (n >= 0) val = static_cast<double>(d.pold[n]);

@@ -164,6 +164,24 @@ extern "C" int fdtd_fb_step_noalloc(int precision, int NI, int NJ, int NK, const
         return fail(FDTD_ERR_ARG, "fdtd_fb_step_noalloc: each axis is limited to 4096 nodes (fixed 128 KiB scratch)");
     if (!(dt > 0) || !(dx > 0) || !(dy > 0) || !(dz > 0) || !(gamma > 0) || !(P0 > 0) || !(c0 > 0))
         return fail(FDTD_ERR_ARG, "non-positive physical parameter");
+    if (precision == FDTD_F64 || precision == FDTD_F32) {
+        // face nodes read their inward neighbour and the velocity pass reads
+        // the old pressure, so an output that shares memory with any input
+        // (or another output) would be read after other threads wrote it
+        const size_t bytes = static_cast<size_t>(NI) * NJ * NK * (precision == FDTD_F64 ? 8 : 4);
+        const void* in[4] = {u_in, v_in, w_in, p_in};
+        const void* out[4] = {u_out, v_out, w_out, p_out};
+        auto overlap = [bytes](const void* a, const void* b) {
+            const uintptr_t x = reinterpret_cast<uintptr_t>(a), y = reinterpret_cast<uintptr_t>(b);
+            return x < y + bytes && y < x + bytes;
+        };
+        for (int o = 0; o < 4; ++o) {
+            for (int q = 0; q < 4; ++q)
+                if (overlap(out[o], in[q])) return fail(FDTD_ERR_ARG, "output buffer overlaps an input buffer");
+            for (int q = o + 1; q < 4; ++q)
+                if (overlap(out[o], out[q])) return fail(FDTD_ERR_ARG, "two output buffers overlap");
+        }
+    }
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (precision == FDTD_F64)
         return step<double>(NI, NJ, NK, X, Y, Z, dx, dy, dz, dt, gamma, P0, c0, u_in, v_in, w_in, p_in, u_out, v_out,

@@ -714,6 +714,7 @@ class SolverImpl final : public SolverImplBase {
         d.nrec = static_cast<int>(rec_idx_.size());
         d.rec_node = d_rec_node_;
         d.rec_out = d_rec_out_;
+        d.rec_steps = static_cast<int>(rec_cap_ / std::max<size_t>(rec_idx_.size(), 1));
         d.counters = d_counters_;
         d.status = d_status_;
         d.wait_spin = wait_spin_;
@@ -1051,6 +1052,9 @@ class SolverImpl final : public SolverImplBase {
     void step_pressure() override {
         FDTD_CK(cudaSetDevice(device_));
         if (in.scheme != FB_P_V) fail(-2, "half steps are exposed for FB_p_v only");
+        // the receiver buffer holds horizon_ steps: a half step past it would
+        // sample into memory the handle does not own
+        if (steps_ >= horizon_) fail(-6, "half step past the horizon set by reset(); call reset first");
         if (!frame_started_) {
             mf_limit_ = frame_limit();
             upload_frame(mf_count_);
@@ -1469,7 +1473,7 @@ class SolverImpl final : public SolverImplBase {
     // taken, [nsteps][n_receivers]
     void get_receivers(int first_step, int nsteps, double* out) override {
         FDTD_CK(cudaSetDevice(device_));
-        if (first_step < 0 || nsteps < 0 || first_step + nsteps > steps_)
+        if (first_step < 0 || nsteps < 0 || first_step > steps_ || nsteps > steps_ - first_step)
             fail(-5, "receiver range outside the steps taken so far");
         if (rec_idx_.empty() || nsteps == 0) return;
         d2h(out, d_rec_out_ + static_cast<size_t>(first_step) * rec_idx_.size(),

@@ -248,8 +248,10 @@ int fdtd_band_levels(int device, const double *traces, int nrec, int nt, int fft
  * (larger grids return FDTD_ERR_ARG). The first call on a device resolves
  * that array's device address (make it before any stream capture). All
  * calls share the array and reset it themselves; calls that overlap on the
- * GPU race and must be serialised by the caller. Synchronises the stream
- * before returning; FDTD_ERR_NONFINITE if the new pressure is not finite. */
+ * GPU race and must be serialised by the caller. The four output buffers
+ * must not overlap each other or any input buffer (FDTD_ERR_ARG otherwise:
+ * the step cannot run in place). Synchronises the stream before returning;
+ * FDTD_ERR_NONFINITE if the new pressure is not finite. */
 int fdtd_fb_step_noalloc(int precision, int NI, int NJ, int NK, const double *X, const double *Y,
                          const double *Z, double dx, double dy, double dz, double dt, double gamma,
                          double P0, double c0, const void *u_in, const void *v_in, const void *w_in,

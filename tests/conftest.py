@@ -20,11 +20,13 @@ def ref_harness():
     import refio
 
     if not os.path.exists(refio.REF_HARNESS):
-        ref_src = "/root/reference/3D_MPI_TEST"
+        import importlib
+
+        ref_src = importlib.import_module("__graft_entry__").reference_src()
         if os.path.isdir(ref_src):
             import subprocess
 
-            subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True,
+            subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), f"REF={ref_src}", "ref"], check=True,
                            stdout=subprocess.DEVNULL)
         else:
             pytest.skip("reference build oracle/_ref/ref_harness not present")

@@ -90,3 +90,27 @@ def test_package_fails_loudly_without_library(tmp_path):
     with pytest.raises(pkg.FdtdError) as e:
         pkg.load_library(str(tmp_path / "libfdtd_b200.so"))
     assert e.value.code == pkg.FDTD_ERR_CUDA
+
+
+def test_noalloc_rejects_overlapping_buffers_before_any_device_work(lib):
+    # the step cannot run in place: every output must be disjoint from every
+    # input and from the other outputs; the check comes before any CUDA call
+    import numpy as np
+
+    fn = lib.fdtd_fb_step_noalloc
+    NI, NJ, NK = 4, 8, 4
+    X, Y, Z = (np.arange(n, dtype=np.float64) * 0.05 for n in (NI, NJ, NK))
+    dp = ctypes.POINTER(ctypes.c_double)
+    nb = NI * NJ * NK * 8
+    base = 1 << 40  # never dereferenced: every call below is rejected first
+    bufs = [ctypes.c_void_p(base + q * 4 * nb) for q in range(8)]  # disjoint address ranges
+
+    def call(u_o, v_o, w_o, p_o):
+        return fn(0, NI, NJ, NK, X.ctypes.data_as(dp), Y.ctypes.data_as(dp), Z.ctypes.data_as(dp), 0.05, 0.05,
+                  0.05, 1e-5, 1.4, 1e5, 343.0, bufs[0], bufs[1], bufs[2], bufs[3], u_o, v_o, w_o, p_o, None)
+
+    assert call(bufs[0], bufs[5], bufs[6], bufs[7]) == pkg.FDTD_ERR_ARG  # u in place
+    assert b"overlaps an input" in lib.fdtd_last_error()
+    assert call(bufs[4], bufs[5], bufs[6], ctypes.c_void_p(base + 3 * 4 * nb + 8)) == pkg.FDTD_ERR_ARG
+    assert call(bufs[4], bufs[4], bufs[6], bufs[7]) == pkg.FDTD_ERR_ARG  # two outputs share memory
+    assert b"two output buffers" in lib.fdtd_last_error()

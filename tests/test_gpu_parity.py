@@ -224,3 +224,27 @@ def test_fused_and_two_pass_agree(case_dirs):
         b.get_output(4)
         p1 = b.field("p")
     assert rel_l2(p1, p2) <= 1e-13
+
+
+def test_half_step_past_horizon_is_state_error(case_dirs):
+    """Cal_pressure samples receivers into a buffer of `horizon` steps, so a
+    half step at the horizon is refused before any launch and the handle
+    stays usable."""
+    d, rec, _ = case_dirs["pml_rigid"]
+    with pkg.Airpore(d, "f64") as a:
+        a.set_receivers(rec)
+        a.reset(2)
+        for _ in range(2):
+            a.Cal_pressure()
+            a.Cal_velocity()
+        launches = a.launch_count()
+        with pytest.raises(pkg.FdtdError) as e:
+            a.Cal_pressure()
+        assert e.value.code == pkg.FDTD_ERR_STATE
+        assert a.launch_count() == launches
+        with pytest.raises(pkg.FdtdError) as e:
+            a.receivers(1, 2)  # steps 1..2 are not all taken: only 0 and 1 are
+        assert e.value.code == pkg.FDTD_ERR_ARG
+        assert a.receivers(0, 2).shape == (2, len(rec))
+        a.reset(2)
+        a.Cal_pressure()  # usable again after a reset
