@@ -540,6 +540,9 @@ def run_gpu(args, rank, world, local_rank):
         results[prec] = {"gcell": gcell, "ms_per_bench_step": dev_ms / args.steps, "wall_s": wall, "tile": tile,
                          "launches": launches, "achieved_gbs": achieved, "bytes_per_step": ab["bytes_per_step"],
                          "clocks": sampler.summary() if sampler else None}
+        # the error statement: receiver p(t) over the workload's full 4000
+        # steps from t = 0, this precision's path with the tuned tile
+        results["trace_" + prec] = a.get_output(case.time_domain).T.copy()
         # end to end through the public API with host buffers (FP32 headline only)
         if prec == "f32":
             n = a.state_elems()
@@ -568,6 +571,7 @@ def run_gpu(args, rank, world, local_rank):
             "kernel": "k_march (one launch = one FB step of the whole domain), FP32",
             "tile_rows_planes_threads_width_stages": list(f32["tile"]),
             "algorithmic_bytes_per_step": f32["bytes_per_step"]}
+    fp32_error = fp32_error_statement(results["trace_f32"], results["trace_f64"], case.dt, local_rank)
     prof = os.path.join(ROOT, "profiles", "traffic.txt")
     if os.path.exists(prof):
         with open(prof) as fh:
@@ -586,6 +590,7 @@ def run_gpu(args, rank, world, local_rank):
                  "achieved_gbs": round(f64["achieved_gbs"], 1),
                  "frac": round(f64["achieved_gbs"] / hbm_peak, 4),
                  "fp32_speedup": round(f32["gcell"] / f64["gcell"], 3)},
+        "fp32_error": fp32_error,
         "roofline": roof,
         "e2e": {k: (round(v, 3) if isinstance(v, float) else v) for k, v in results["e2e"].items()},
         "gpu_launches": int(f32["launches"]),
@@ -596,6 +601,28 @@ def run_gpu(args, rank, world, local_rank):
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(case_dir_for_cpu(), cells)
     return line
+
+
+def fp32_error_statement(tr32, tr64, dt: float, device: int) -> dict:
+    """FP32 against FP64 on the device for the same workload: relative L2
+    of every receiver's p(t) over the whole run, and the band-level error
+    per third-octave band (50 Hz - 2 kHz) from the receivers' spectra."""
+    import numpy as np
+
+    pkg = importlib.import_module("3d_mpi_test_b200")
+    nt = tr64.shape[1]
+    fft_m = max(1, int(np.ceil(np.log2(nt))))
+    l32 = pkg.band_levels(tr32, fft_m, dt, device=device)
+    l64 = pkg.band_levels(tr64, fft_m, dt, device=device)
+    db = np.abs(l32 - l64)
+    per_rec = [float(np.linalg.norm(a - b) / np.linalg.norm(b)) for a, b in zip(tr32, tr64)]
+    return {"steps": int(nt), "receivers": int(tr64.shape[0]),
+            "rel_l2_receivers": float(np.linalg.norm(tr32 - tr64) / np.linalg.norm(tr64)),
+            "rel_l2_worst_receiver": max(per_rec),
+            "band_db_error_max": float(db.max()), "band_db_error_mean": float(db.mean()),
+            "band_db_error_max_per_band": [round(float(v), 7) for v in db.max(axis=0)],
+            "bands_hz": [round(f, 1) for f in pkg.THIRD_OCTAVE_50_2K], "fft_m": fft_m,
+            "within_1e-4": bool(float(np.linalg.norm(tr32 - tr64) / np.linalg.norm(tr64)) <= 1e-4)}
 
 
 def case_dir_for_cpu():
