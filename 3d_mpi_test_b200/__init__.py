@@ -40,7 +40,7 @@ EXPORTS = (
     "fdtd_fft", "fdtd_spectrum", "fdtd_band_levels", "fdtd_save_restart", "fdtd_load_restart",
     "fdtd_write_contour", "fdtd_get_receivers", "fdtd_set_wait_limit", "fdtd_ensemble_create",
     "fdtd_ensemble_destroy", "fdtd_ensemble_advance", "fdtd_ensemble_autotune", "fdtd_ensemble_info",
-    "fdtd_ensemble_last_device_ms", "fdtd_ensemble_set_mode",
+    "fdtd_ensemble_last_device_ms", "fdtd_ensemble_set_mode", "fdtd_set_tile_shape", "fdtd_get_tile_shape",
     # include/fdtd_surrogate.h (signatures in surrogate.py)
     "fdtd_tc_gemm", "fdtd_net_create", "fdtd_net_destroy", "fdtd_net_n_params", "fdtd_net_get_params",
     "fdtd_net_set_params", "fdtd_net_set_data", "fdtd_net_get_normalization", "fdtd_net_set_normalization",
@@ -91,6 +91,8 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
         "fdtd_fb_step_noalloc": ([i, i, i, i, dp, dp, dp] + [ctypes.c_double] * 7 + [vp] * 9, i),
         "fdtd_set_tiling": ([vp, i, i, i, i, i], i),
         "fdtd_autotune": ([vp, i, ip], i),
+        "fdtd_set_tile_shape": ([vp, i, i, i, i, i], i),
+        "fdtd_get_tile_shape": ([vp, ip], i),
         "fdtd_fft": ([i, dp, i, i, i, dp, dp], i),
         "fdtd_spectrum": ([i, dp, i, i, i, ctypes.c_longlong, ctypes.c_longlong, dp], i),
         "fdtd_band_levels": ([i, dp, i, i, i, ctypes.c_double, i, dp, dp], i),
@@ -262,6 +264,18 @@ class Airpore:
         (0: the minimum)."""
         self._check(self._L.fdtd_set_tiling(self._h, rows_per_block, planes_per_block, threads_per_block,
                                             vector_width, ring_stages))
+
+    def set_tile_shape(self, kind: int, rows: int, vectors: int, planes: int, ring_stages: int = 4) -> None:
+        """Largest tile of the tiled kernel for kind 0 (full tiles: PML,
+        faces, TDBC) or 1 (lean interior tiles): rows, 16-byte column vectors
+        and planes per tile, TMA ring stages; selects the tiled kernel."""
+        self._check(self._L.fdtd_set_tile_shape(self._h, kind, rows, vectors, planes, ring_stages))
+
+    def tile_shape(self) -> dict:
+        out = (ctypes.c_int * 13)()
+        self._check(self._L.fdtd_get_tile_shape(self._h, out))
+        keys = ("rows", "vectors", "planes", "stages", "threads", "tiles")
+        return {"full": dict(zip(keys, out[0:6])), "lean": dict(zip(keys, out[6:12])), "tiled": bool(out[12])}
 
     def autotune(self, nsteps: int = 20) -> Tuple[int, int, int, int, int]:
         best = (ctypes.c_int * 5)()

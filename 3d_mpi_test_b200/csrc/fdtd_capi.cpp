@@ -157,6 +157,19 @@ int fdtd_set_tiling(fdtd_solver* h, int rows_per_block, int planes_per_block, in
     return guard([&] { h->s->set_tiling(rows_per_block, planes_per_block, threads_per_block, vector_width, ring_stages); });
 }
 
+int fdtd_set_tile_shape(fdtd_solver* h, int kind, int rows, int vectors, int planes, int ring_stages) {
+    if (!h) return bad("null handle");
+    return guard([&] { h->s->set_tile_shape(kind, rows, vectors, planes, ring_stages); });
+}
+
+int fdtd_get_tile_shape(const fdtd_solver* h, int* out) {
+    if (!h || !out) return bad("null argument");
+    return guard([&] {
+        const auto t = h->s->tile_shape();
+        for (int q = 0; q < 13; ++q) out[q] = t[q];
+    });
+}
+
 int fdtd_autotune(fdtd_solver* h, int nsteps, int* best) {
     if (!h || !best || nsteps <= 0) return bad("bad autotune arguments");
     return guard([&] {

@@ -340,7 +340,9 @@ __device__ __forceinline__ void wind_dp(const Dev<R>& d, int j, int k, R ax, R a
 // XF: the rarer features (porous inclusions, vectors with columns of both y
 // layers) are compiled in; a kernel built without them is used only for
 // domains that have none
-template <typename R, bool WIND, int N, bool XF = true>
+// PML: the PML terms are compiled in (a kernel built without them runs only
+// tiles that hold no PML node)
+template <typename R, bool WIND, int N, bool XF = true, bool PML = true>
 __device__ __forceinline__ Arr<R, N> p_vec(const Dev<R>& d, const PlaneC<R>& pc, const RowC<R>& rc, int i, int jb,
                                            const Arr<R, N>& ay, int ysp, const Arr<R, N>& u0, const Arr<R, N>& v0,
                                            const Arr<R, N>& w0, const Arr<R, N>& pn, const Arr<R, N>& ui,
@@ -368,7 +370,7 @@ __device__ __forceinline__ Arr<R, N> p_vec(const Dev<R>& d, const PlaneC<R>& pc,
                 wind_dp(d, jb + e, pc.k, rc.ax, ay.e[e], pc.az, pn.e[e], pim.e[e], pjm.e[e], pkm.e[e], dp.e[e]);
     }
     const int ysv = y_common<N>(ysp);
-    if (rc.xs | ysv | pc.zs) {
+    if (PML && (rc.xs | ysv | pc.zs)) {
         if (!XF || ysv != 3) {
             pml_dp_v<R, N>(d, i, jb, pc.k, rc.xs, ysp, ysv, pc.zs, rc.ax, ay, pc.az, gu, gv, gw, pn, rc.X, pc.Z, dp);
         } else {  // both y layers within N columns (very narrow grids): column by column
@@ -543,7 +545,7 @@ struct Vel {
 // (air.cpp:1476-1949); pore: porous::cal_fuvw (porous.cpp:58-104);
 // accumulation: calculation_2D::Cal_velocity (calculation_2D.cpp:548-579).
 // Column conventions as p_vec.
-template <typename R, bool WIND, int N, bool XF = true>
+template <typename R, bool WIND, int N, bool XF = true, bool PML = true>
 __device__ __forceinline__ Vel<R, N> vel_vec(const Dev<R>& d, const PlaneC<R>& pc, const RowC<R>& rc, int i, int jb,
                                              const Arr<R, N>& ay, int ysp, const Arr<R, N>& u0, const Arr<R, N>& v0,
                                              const Arr<R, N>& w0, const Arr<R, N>& p0, const Arr<R, N>& pim,
@@ -586,7 +588,7 @@ __device__ __forceinline__ Vel<R, N> vel_vec(const Dev<R>& d, const PlaneC<R>& p
                           du.e[e], dv.e[e], dw.e[e]);
     }
     const int ysv = y_common<N>(ysp);
-    if (rc.xs | ysv | pc.zs) {
+    if (PML && (rc.xs | ysv | pc.zs)) {
         if (!XF || ysv != 3) {
             pml_dvel_v<R, N>(d, i, jb, pc.k, rc.xs, ysp, ysv, pc.zs, ax, ay, az, u0, v0, w0, gpX, gpY, gpZ, p0, pim,
                              pjm, pkm, qp_old, rc.X, pc.Z, du, dv, dw);

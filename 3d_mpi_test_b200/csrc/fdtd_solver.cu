@@ -19,6 +19,7 @@
 
 #include "fdtd_device.cuh"
 #include "fdtd_march.cuh"
+#include "fdtd_tile.cuh"
 
 namespace fdtd {
 
@@ -94,6 +95,43 @@ bool wind_at(int method, double b, double y, double z, double& U, double& V, dou
     }
 }
 
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn tensor_map_encoder() {
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        FDTD_CK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+        if (q != cudaDriverEntryPointSuccess || !p) fail(-3, "cuTensorMapEncodeTiled is unavailable");
+        fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    return fn;
+}
+
+// split [a, b) into ceil((b - a) / T) near-equal pieces
+void split_even(int a, int b, int T, std::vector<std::array<int, 2>>& out) {
+    const int L = b - a;
+    if (L <= 0) return;
+    const int n = (L + T - 1) / T;
+    for (int q = 0; q < n; ++q)
+        out.push_back({a + static_cast<int>(static_cast<long long>(L) * q / n),
+                       a + static_cast<int>(static_cast<long long>(L) * (q + 1) / n)});
+}
+
+// consecutive segments between the sorted, de-duplicated cut points in [lo, hi]
+std::vector<std::array<int, 2>> segments(std::vector<int> cuts, int lo, int hi) {
+    std::vector<int> c;
+    for (int x : cuts) c.push_back(std::min(std::max(x, lo), hi));
+    std::sort(c.begin(), c.end());
+    c.erase(std::unique(c.begin(), c.end()), c.end());
+    std::vector<std::array<int, 2>> out;
+    for (size_t q = 0; q + 1 < c.size(); ++q) out.push_back({c[q], c[q + 1]});
+    return out;
+}
+
 template <typename T>
 T* dalloc(size_t n) {
     T* p = nullptr;
@@ -132,6 +170,8 @@ class SolverImplBase {
     virtual std::array<int, 5> autotune(int nsteps) = 0;
     virtual void get_receivers(int first_step, int nsteps, double* out) = 0;
     virtual void set_wait_limit(long long polls) = 0;
+    virtual void set_tile_shape_api(int kind, int TI, int TV, int GC, int ns) = 0;
+    virtual std::array<int, 13> tile_shape() const = 0;
 };
 
 template <typename R>
@@ -155,14 +195,26 @@ class SolverImpl final : public SolverImplBase {
         FDTD_CK(cudaEventCreate(&ev1_));
         allocate();
         FDTD_CK(cudaDeviceSynchronize());
-        // FB_p_v runs as one marching pass per step when a 2-row tile fits
-        // (one thread per 16-byte column vector, at most 512 per row);
-        // FB_v_p and larger rows keep the two passes
+        // FB_p_v runs as one pass per step: the tiled kernel (any row
+        // width) by default; the row marching kernel where a 2-row tile of
+        // it fits (one thread per 16-byte column vector, at most 256 per
+        // row) is kept for the batched ensemble and as a selectable
+        // alternative. FB_v_p keeps the two passes.
         const int nvec = NJP_ / kVecMax;
-        fused_ = (in.scheme == FB_P_V) && nvec <= kMarchThreads && march_smem_bytes(make_tiling(2, 16, 1, kVecMax, 0)) <= kSmemMax;
-        if (fused_) {  // 4-row tiles where they fit shared memory, else 2-row
+        fused_ = in.scheme == FB_P_V;
+        old_ok_ = fused_ && nvec <= kMarchThreads && march_smem_bytes(make_tiling(2, 16, 1, kVecMax, 0)) <= kSmemMax;
+        if (old_ok_) {  // 4-row tiles where they fit shared memory, else 2-row
             const int TI = march_smem_bytes(make_tiling(4, 16, 256 / nvec, kVecMax, 0)) <= kSmemMax ? 4 : 2;
             set_tiling(TI, 16, 256, 0, 0);
+        }
+        if (fused_) {
+            FDTD_CK(cudaStreamCreateWithFlags(&stream2_, cudaStreamNonBlocking));
+            FDTD_CK(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming));
+            FDTD_CK(cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming));
+            tcfg_[0] = default_tile(false);
+            tcfg_[1] = default_tile(true);
+            tile_on_ = true;
+            build_tiles();
         }
         reset(in.time_domain);
     }
@@ -172,6 +224,10 @@ class SolverImpl final : public SolverImplBase {
         if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
         for (void* p : allocs_) cudaFree(p);
         if (d_rec_out_) cudaFree(d_rec_out_);
+        if (d_tiles_) cudaFree(d_tiles_);
+        if (ev_fork_) cudaEventDestroy(ev_fork_);
+        if (ev_join_) cudaEventDestroy(ev_join_);
+        if (stream2_) cudaStreamDestroy(stream2_);
         if (ev0_) cudaEventDestroy(ev0_);
         if (ev1_) cudaEventDestroy(ev1_);
         if (stream_) cudaStreamDestroy(stream_);
@@ -823,7 +879,7 @@ class SolverImpl final : public SolverImplBase {
     }
 
     void update_xf() {
-        const bool xf = needs_xf(tiling_.VW);
+        const bool xf = needs_xf(tile_on_ ? kVecMax : tiling_.VW);
         if (xf != xf_) {
             xf_ = xf;
             graph_dirty_ = true;
@@ -877,15 +933,37 @@ class SolverImpl final : public SolverImplBase {
         return n;
     }
 
-    void launch_fused(int par) { launch_fused_on(par, stream_); }
+    // one fused step at parity par on the handle's stream; tiled form: the
+    // lean tiles run on a second stream, forked from and joined to it, so
+    // both launches share the device
+    void launch_fused(int par) {
+        if (tile_on_ && ntile_[1] && ntile_[0]) {
+            FDTD_CK(cudaEventRecord(ev_fork_, stream_));
+            FDTD_CK(cudaStreamWaitEvent(stream2_, ev_fork_, 0));
+            launch_tiles(par, stream_, stream2_);
+            FDTD_CK(cudaEventRecord(ev_join_, stream2_));
+            FDTD_CK(cudaStreamWaitEvent(stream_, ev_join_, 0));
+        } else {
+            launch_fused_on(par, stream_);
+        }
+    }
 
-    // one fused step at parity par on stream s (also an ensemble's stream)
-    void launch_fused_on(int par, cudaStream_t s) {
+    // one fused step at parity par on stream s (also an ensemble's stream);
+    // returns the kernels launched
+    int launch_fused_on(int par, cudaStream_t s) {
+        if (tile_on_) return launch_tiles(par, s, s);
+        if (!old_ok_) fail(-2, "rows too wide for the row marching kernel");
         const Dev<R> d = params_fused(par);
         if (xf_) launch_march<true>(d, par, s);
         else launch_march<false>(d, par, s);
         FDTD_CK(cudaGetLastError());
         ++launches_;
+        return 1;
+    }
+
+    int launches_per_step() const {
+        if (in.scheme == FB_P_V && fused_) return tile_on_ ? (ntile_[0] ? 1 : 0) + (ntile_[1] ? 1 : 0) : 1;
+        return 2;
     }
 
     template <bool XF>
@@ -937,7 +1015,7 @@ class SolverImpl final : public SolverImplBase {
             ensure_graph();
             while (n >= kGraphSteps) {
                 FDTD_CK(cudaGraphLaunch(graph_exec_, stream_));
-                launches_ += 2 * kGraphSteps;
+                launches_ += static_cast<long long>(launches_per_step()) * kGraphSteps;
                 n -= kGraphSteps;
                 steps_ += kGraphSteps;
             }
@@ -1413,7 +1491,266 @@ class SolverImpl final : public SolverImplBase {
     void set_tiling_api(int TI, int GC, int nt, int vw, int stages) override {
         FDTD_CK(cudaSetDevice(device_));
         if (!fused_) fail(-2, "tiling applies to the fused FB_p_v pass only");
+        if (!old_ok_) fail(-2, "rows too wide for the row marching kernel");
         set_tiling(TI, GC, nt, vw, stages);
+        tile_on_ = false;  // the row marching kernel runs from now on
+        if (!sdy_.empty()) update_xf();
+        graph_dirty_ = true;
+    }
+
+    // ------------------------------------------------- tiled kernel
+    // kind 0: full tiles (PML, faces, TDBC, inclusions); 1: lean tiles
+    struct TileCfg {
+        int TI, TV, GC, ns;
+    };
+
+    static TileCfg default_tile(bool lean) {
+        if (sizeof(R) == 4) return lean ? TileCfg{8, 32, 16, 4} : TileCfg{8, 16, 16, 4};
+        return lean ? TileCfg{8, 32, 16, 4} : TileCfg{8, 16, 16, 4};
+    }
+
+    TileGeo tile_geo(int TI, int TV, int ns) const {
+        const int W = wind_on_ ? 1 : 0;
+        TileGeo g{};
+        g.TI = TI;
+        g.TV = TV;
+        g.ns = ns;
+        g.srows = TI + 2 + W;
+        g.svec = TV + 2 + W;
+        const size_t bb = (static_cast<size_t>(g.srows) * g.svec * kVecMax * sizeof(R) + 127) / 128 * 128;
+        g.box = static_cast<int>(bb / sizeof(R));
+        g.pslot = (TI + 1) * (TV + 1) * kVecMax;
+        g.ring_off = 128 + static_cast<int>((3 * static_cast<size_t>(g.pslot) * sizeof(R) + 127) / 128 * 128);
+        return g;
+    }
+    static size_t tile_smem(const TileGeo& g) {
+        return static_cast<size_t>(g.ring_off) + static_cast<size_t>(g.ns) * 4 * g.box * sizeof(R);
+    }
+
+    void check_tile(const TileCfg& c) const {
+        if (c.TI < 2 || c.TV < 2 || c.GC < 1 || c.ns < 3 || c.ns > kMaxStages)
+            fail(-5, "tile shape needs rows >= 2, column vectors >= 2, planes >= 1 and 3..12 ring stages");
+        if ((c.TI + 1) * (c.TV + 1) > kTileMaxThreads) fail(-2, "tile needs more than 384 threads");
+        const TileGeo g = tile_geo(c.TI, c.TV, c.ns);
+        if (g.svec * kVecMax > 256 || g.srows > 256) fail(-2, "staged tile box exceeds 256 elements along an axis");
+        if (tile_smem(g) > kSmemMax) fail(-2, "tile does not fit shared memory");
+    }
+
+    template <bool FULL, bool XF>
+    static const void* tile_kernel(bool wind) {
+        return wind ? reinterpret_cast<const void*>(k_tile<R, true, kVecMax, FULL, XF>)
+                    : reinterpret_cast<const void*>(k_tile<R, false, kVecMax, FULL, XF>);
+    }
+
+    // Cuts the core planes x rows x column vectors into tiles whose
+    // boundaries follow the PML layers and their storage, the faces and the
+    // porous/air interface, classifies each as lean (interior air outside
+    // every PML layer and its storage, no inclusion; or porous-ground
+    // interior) or full, orders the full tiles heaviest first, and sizes
+    // both launches.
+    void build_tiles() {
+        const int V = kVecMax, nvec = NJP_ / V;
+        for (int k = 0; k < 2; ++k) check_tile(tcfg_[k]);
+        // lean air box: rows [li0, li1), vectors [lv0, lv1), planes [lg0, lg1),
+        // inside rows [1, NI-2) and vectors [1, nvec-2) so that the tiles at
+        // the high faces keep >= 2 rows (the i-1 pressure of row NI-1's
+        // stencil row) and >= 2 vectors (columns NJ-2..NJ-4 of the east
+        // extrapolation); an empty range adds no cuts
+        const int li0 = std::max(1, I1_ ? I1_ + 1 : 1), li1 = std::min(NI_ - 2, I2_ ? NI_ - 1 - I2_ : NI_ - 1);
+        const int jlo = std::max(1, Y1_ ? Y1_ + 1 : 1), jhi = std::min(NJ_ - 1, Y2_ ? NJ_ - 1 - Y2_ : NJ_ - 1);
+        const int lv0 = std::max(1, (jlo + V - 1) / V), lv1 = std::min(nvec - 2, jhi / V);
+        const int lk0 = K1_ ? K1_ + 1 : 1, lk1 = K2_ ? Kair_ - 1 - K2_ : Kair_ - 1;
+        const int lg0 = std::max(lk0 + gOff_, gAir0_), lg1 = lk1 + gOff_;
+        std::vector<int> rc{0, 1, NI_ - 2, NI_}, vc{0, 1, nvec - 2, nvec}, gc{1, NG_ - 1};
+        if (li0 < li1) rc.insert(rc.end(), {li0, li1});
+        if (lv0 < lv1) vc.insert(vc.end(), {lv0, lv1});
+        if (lg0 < lg1) gc.insert(gc.end(), {lg0, lg1});
+        // porous planes [1, gOff) are lean-capable; plane gOff is also air
+        // k = 0, where the PML integrals are stored, so it stays full
+        if (porous_) gc.insert(gc.end(), {gOff_, gAir0_});
+        const auto rows = segments(rc, 0, NI_);
+        const auto vecs = segments(vc, 0, nvec);
+        const auto planes = segments(gc, 1, NG_ - 1);
+        auto overlap = [](int a0, int a1, int b0, int b1) { return std::max(0, std::min(a1, b1) - std::max(a0, b0)); };
+        std::vector<std::pair<long long, TileBox>> full;
+        std::vector<TileBox> lean;
+        int maxr[2] = {2, 2}, maxv[2] = {2, 2};
+        for (const auto& pr : planes)
+            for (const auto& rr : rows)
+                for (const auto& vr : vecs) {
+                    bool is_lean;
+                    if (porous_ && pr[1] <= gOff_)  // porous ground: no PML; faces excluded
+                        is_lean = rr[0] >= 1 && rr[1] <= NI_ - 2 && vr[0] >= 1 && vr[1] <= nvec - 2;
+                    else if (porous_ && pr[0] < gAir0_)
+                        is_lean = false;
+                    else
+                        is_lean = !mask_on_ && rr[0] >= li0 && rr[1] <= li1 && vr[0] >= lv0 && vr[1] <= lv1 &&
+                                  pr[0] >= lg0 && pr[1] <= lg1;
+                    const int kind = is_lean ? 1 : 0;
+                    const TileCfg& tc = tcfg_[kind];
+                    std::vector<std::array<int, 2>> rp, vp, gp;
+                    split_even(rr[0], rr[1], tc.TI, rp);
+                    split_even(vr[0], vr[1], tc.TV, vp);
+                    split_even(pr[0], pr[1], tc.GC, gp);
+                    for (const auto& a : rp)
+                        for (const auto& bq : vp)
+                            for (const auto& cq : gp) {
+                                const TileBox t{a[0], a[1], bq[0], bq[1], cq[0], cq[1]};
+                                maxr[kind] = std::max(maxr[kind], a[1] - a[0]);
+                                maxv[kind] = std::max(maxv[kind], bq[1] - bq[0]);
+                                if (is_lean) {
+                                    lean.push_back(t);
+                                    continue;
+                                }
+                                // estimated cost: nodes with halos, times 1 + 2 per PML layer crossed
+                                const int xl = overlap(t.i0, t.i1, 0, I1_) + overlap(t.i0, t.i1, NI_ - I2_, NI_) > 0;
+                                const int yl = overlap(t.v0 * V, t.v1 * V, 0, Y1_) +
+                                                   overlap(t.v0 * V, t.v1 * V, NJ_ - Y2_, NJ_) > 0;
+                                const int zl = t.c1 > gAir0_ && (overlap(t.c0, t.c1, gOff_, gOff_ + K1_) +
+                                                                     overlap(t.c0, t.c1, gOff_ + Kair_ - K2_, NG_) > 0);
+                                const long long cost = static_cast<long long>(t.i1 - t.i0 + 1) * (t.v1 - t.v0 + 1) *
+                                                       (t.c1 - t.c0 + 1) * (1 + 2 * (xl + yl + zl));
+                                full.push_back({cost, t});
+                            }
+                }
+        std::stable_sort(full.begin(), full.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+        std::vector<TileBox> all;
+        for (const auto& f : full) all.push_back(f.second);
+        all.insert(all.end(), lean.begin(), lean.end());
+        ntile_[0] = static_cast<int>(full.size());
+        ntile_[1] = static_cast<int>(lean.size());
+        if (all.size() > tiles_cap_) {
+            if (d_tiles_) cudaFree(d_tiles_);
+            d_tiles_ = nullptr;
+            FDTD_CK(cudaMalloc(&d_tiles_, sizeof(TileBox) * all.size()));
+            tiles_cap_ = all.size();
+        }
+        FDTD_CK(cudaMemcpy(d_tiles_, all.data(), sizeof(TileBox) * all.size(), cudaMemcpyHostToDevice));
+        for (int k = 0; k < 2; ++k) {
+            tgeo_[k] = tile_geo(std::min(maxr[k], tcfg_[k].TI) < 2 ? 2 : std::min(maxr[k], tcfg_[k].TI),
+                                std::min(maxv[k], tcfg_[k].TV) < 2 ? 2 : std::min(maxv[k], tcfg_[k].TV), tcfg_[k].ns);
+            tthr_[k] = ((tgeo_[k].TI + 1) * (tgeo_[k].TV + 1) + 31) / 32 * 32;
+            tsmem_[k] = tile_smem(tgeo_[k]);
+            encode_tile_maps(k);
+        }
+        if (tsmem_[0] > 48 * 1024 || tsmem_[1] > 48 * 1024) {
+            for (bool w : {false, true})
+                for (const void* f : {tile_kernel<true, true>(w), tile_kernel<true, false>(w), tile_kernel<false, false>(w)})
+                    FDTD_CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSmemMax)));
+        }
+        if (!sdy_.empty()) update_xf();  // before the first frame upload, which sets it
+        graph_dirty_ = true;
+    }
+
+    // tensor maps of the 8 field buffers for the staged box of tile kind k
+    void encode_tile_maps(int k) {
+        const TileGeo& g = tgeo_[k];
+        const cuuint64_t dims[3] = {static_cast<cuuint64_t>(NJP_), static_cast<cuuint64_t>(NI_),
+                                    static_cast<cuuint64_t>(NG_)};
+        const cuuint64_t strides[2] = {static_cast<cuuint64_t>(NJP_) * sizeof(R),
+                                       static_cast<cuuint64_t>(NI_) * NJP_ * sizeof(R)};
+        const cuuint32_t box[3] = {static_cast<cuuint32_t>(g.svec * kVecMax), static_cast<cuuint32_t>(g.srows), 1};
+        const cuuint32_t es[3] = {1, 1, 1};
+        const CUtensorMapDataType dt = sizeof(R) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+        for (int lvl = 0; lvl < 2; ++lvl)
+            for (int f = 0; f < 4; ++f) {
+                if (reinterpret_cast<uintptr_t>(F_[lvl][f]) % 16) fail(-3, "field buffer not 16-byte aligned");
+                const CUresult r = tensor_map_encoder()(&tmaps_[k][lvl].f[f], dt, 3, F_[lvl][f], dims, strides, box, es,
+                                                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                                        CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                                                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                if (r != CUDA_SUCCESS) fail(-3, "tensor map encoding failed for the tiled kernel");
+            }
+    }
+
+    template <bool FULL, bool XF>
+    void launch_tile(int par, cudaStream_t s) {
+        const int k = FULL ? 0 : 1;
+        const Dev<R> d = params_fused(par);
+        const TileBox* w = d_tiles_ + (FULL ? 0 : ntile_[0]);
+        const dim3 grd(static_cast<unsigned>(ntile_[k])), blk(static_cast<unsigned>(tthr_[k]));
+        if (wind_on_) k_tile<R, true, kVecMax, FULL, XF><<<grd, blk, tsmem_[k], s>>>(d, tmaps_[k][par], tgeo_[k], w, par);
+        else k_tile<R, false, kVecMax, FULL, XF><<<grd, blk, tsmem_[k], s>>>(d, tmaps_[k][par], tgeo_[k], w, par);
+        FDTD_CK(cudaGetLastError());
+        ++launches_;
+    }
+
+    // one step of the tiled kernel: full tiles on s_full, lean tiles on s_lean
+    int launch_tiles(int par, cudaStream_t s_full, cudaStream_t s_lean) {
+        int n = 0;
+        if (ntile_[0]) {
+            if (xf_) launch_tile<true, true>(par, s_full);
+            else launch_tile<true, false>(par, s_full);
+            ++n;
+        }
+        if (ntile_[1]) {
+            launch_tile<false, false>(par, s_lean);
+            ++n;
+        }
+        return n;
+    }
+
+    // tile shape of kind 0 (full) or 1 (lean): rows, column vectors and
+    // planes per tile, ring stages; switches to the tiled kernel
+    void set_tile_shape_api(int kind, int TI, int TV, int GC, int ns) override {
+        FDTD_CK(cudaSetDevice(device_));
+        if (!fused_) fail(-2, "tiling applies to the fused FB_p_v pass only");
+        if (kind != 0 && kind != 1) fail(-5, "tile kind must be 0 (full) or 1 (lean)");
+        const TileCfg c{TI, TV, GC, ns};
+        check_tile(c);
+        FDTD_CK(cudaStreamSynchronize(stream_));
+        tcfg_[kind] = c;
+        tile_on_ = true;
+        build_tiles();
+    }
+
+    // {kind 0: rows, vectors, planes, stages, threads, tiles; kind 1: the same}, on = tiled kernel active
+    std::array<int, 13> tile_shape() const override {
+        std::array<int, 13> o{};
+        for (int k = 0; k < 2; ++k) {
+            o[6 * k + 0] = tcfg_[k].TI; o[6 * k + 1] = tcfg_[k].TV; o[6 * k + 2] = tcfg_[k].GC;
+            o[6 * k + 3] = tcfg_[k].ns; o[6 * k + 4] = tthr_[k]; o[6 * k + 5] = ntile_[k];
+        }
+        o[12] = tile_on_ ? 1 : 0;
+        return o;
+    }
+
+    // Project autotuner for the tiled kernel: the lean tile shape first
+    // (full tiles at their current shape), then the full tile shape, each
+    // candidate timed over nsteps steps on this domain
+    std::array<int, 5> autotune_tiles(int nsteps) {
+        std::vector<TileCfg> cands;
+        const int V = kVecMax;
+        for (int TV : {16 / V * 2, 32 / V * 2, 64 / V * 2})
+            for (int TI : {4, 8, 16})
+                for (int GC : {8, 16, 32})
+                    for (int ns : {3, 5}) {
+                        const TileCfg c{TI, TV, GC, ns};
+                        try {
+                            check_tile(c);
+                        } catch (const SolverError&) {
+                            continue;
+                        }
+                        cands.push_back(c);
+                    }
+        const int saved_horizon = horizon_;
+        reset(std::max(horizon_, (nsteps + 2) * static_cast<int>(2 * cands.size() + 2) + 4));
+        for (int kind : {1, 0}) {
+            if (!ntile_[kind]) continue;
+            TileCfg best = tcfg_[kind];
+            double best_ms = 1e300;
+            for (const TileCfg& c : cands) {
+                tcfg_[kind] = c;
+                build_tiles();
+                advance(2, nullptr);  // graph build and first touch outside the timing
+                advance(nsteps, nullptr);
+                if (last_ms_ < best_ms) { best_ms = last_ms_; best = c; }
+            }
+            tcfg_[kind] = best;
+            build_tiles();
+        }
+        reset(saved_horizon);
+        return {tcfg_[0].TI, tcfg_[0].GC, tthr_[0], kVecMax, tcfg_[0].ns};
     }
 
     // Project autotuner: time every candidate tile on this domain and keep the
@@ -1425,6 +1762,7 @@ class SolverImpl final : public SolverImplBase {
     std::array<int, 5> autotune(int nsteps) override {
         FDTD_CK(cudaSetDevice(device_));
         if (!fused_) fail(-2, "autotune applies to the fused FB_p_v pass only");
+        if (tile_on_) return autotune_tiles(nsteps);
         cudaDeviceProp prop{};
         FDTD_CK(cudaGetDeviceProperties(&prop, device_));
         const int sms = prop.multiProcessorCount;
@@ -1497,6 +1835,7 @@ class SolverImpl final : public SolverImplBase {
         size_t smem;
         bool wind;
         bool xf;
+        bool old_ok;  // the row marching kernel (batched launches) fits
         int par;
     };
     int device() const { return device_; }
@@ -1526,7 +1865,8 @@ class SolverImpl final : public SolverImplBase {
         v.threads = fused_threads_;
         v.smem = fused_smem_;
         v.wind = wind_on_;
-        v.xf = xf_;
+        v.xf = old_ok_ ? needs_xf(tiling_.VW) : true;
+        v.old_ok = old_ok_;
         v.par = par_;
         return v;
     }
@@ -1592,7 +1932,19 @@ class SolverImpl final : public SolverImplBase {
     cudaGraphExec_t graph_exec_ = nullptr;
     bool graph_dirty_ = true;
     bool fused_ = false;
+    bool old_ok_ = false;  // the row marching kernel fits this domain
     bool xf_ = true;  // marching kernel with the rarer features compiled in
+    // tiled kernel: shapes, geometry and launches of kind 0 (full) and 1 (lean)
+    bool tile_on_ = false;
+    TileCfg tcfg_[2]{};
+    TileGeo tgeo_[2]{};
+    int tthr_[2]{}, ntile_[2]{};
+    size_t tsmem_[2]{};
+    TileMaps tmaps_[2][2]{};  // [kind][time level read]
+    TileBox* d_tiles_ = nullptr;
+    size_t tiles_cap_ = 0;
+    cudaStream_t stream2_ = nullptr;
+    cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
     MarchTiling tiling_{};
     int fused_threads_ = 0;
     size_t fused_smem_ = 0;
@@ -1642,6 +1994,8 @@ void Solver::load_restart(const std::string& path, bool reference_semantics) {
 std::array<int, 5> Solver::autotune(int nsteps) { return impl_->autotune(nsteps); }
 double Solver::last_device_ms() const { return impl_->last_device_ms(); }
 void Solver::get_receivers(int first_step, int nsteps, double* out) { impl_->get_receivers(first_step, nsteps, out); }
+void Solver::set_tile_shape(int kind, int TI, int TV, int GC, int ns) { impl_->set_tile_shape_api(kind, TI, TV, GC, ns); }
+std::array<int, 13> Solver::tile_shape() const { return impl_->tile_shape(); }
 void Solver::set_wait_limit(long long polls) { impl_->set_wait_limit(polls); }
 
 // ---------------------------------------------------------------- Ensemble
@@ -1776,8 +2130,9 @@ class EnsembleImpl final : public EnsembleImplBase {
     static constexpr int kMemberStreams = 16;
 
     long long launches_per_step() const {
-        return mode_ == 1 ? static_cast<long long>(mem_.size()) : static_cast<long long>(groups_.size());
+        return mode_ == 1 ? per_step_ : static_cast<long long>(groups_.size());
     }
+    long long per_step_ = 0;  // kernels one step of mode 1 launches (counted at capture)
 
     struct Group {
         bool wind = false, xf = true;
@@ -1834,6 +2189,9 @@ class EnsembleImpl final : public EnsembleImplBase {
         std::vector<typename SolverImpl<R>::BatchView> v;
         v.reserve(mem_.size());
         for (SolverImpl<R>* m : mem_) v.push_back(m->batch_view());
+        if (mode_ == 0)
+            for (const auto& m : v)
+                if (!m.old_ok) fail(-2, "a member's rows are too wide for the batched marching kernel (use mode 1)");
         // block size class: 64-thread steps, so narrow (2D) members do not
         // share a launch with 256-thread blocks
         auto key_of = [&](size_t i) {
@@ -1960,13 +2318,16 @@ class EnsembleImpl final : public EnsembleImplBase {
             }
             FDTD_CK(cudaEventRecord(fork_, stream_));
             for (int k = 0; k < ns; ++k) FDTD_CK(cudaStreamWaitEvent(mstreams_[k], fork_, 0));
+            long long nl = 0;
             for (int s = 0; s < n; ++s)
-                for (size_t m = 0; m < mem_.size(); ++m) mem_[m]->launch_fused_on((pars_[m] + s) & 1, mstreams_[m % ns]);
+                for (size_t m = 0; m < mem_.size(); ++m)
+                    nl += mem_[m]->launch_fused_on((pars_[m] + s) & 1, mstreams_[m % ns]);
             for (int k = 0; k < ns; ++k) {
                 FDTD_CK(cudaEventRecord(mdone_[k], mstreams_[k]));
                 FDTD_CK(cudaStreamWaitEvent(stream_, mdone_[k], 0));
             }
-            launches_ += static_cast<long long>(n) * mem_.size();
+            launches_ += nl;
+            per_step_ = n > 0 ? nl / n : per_step_;
             return;
         }
         FDTD_CK(cudaEventRecord(fork_, stream_));

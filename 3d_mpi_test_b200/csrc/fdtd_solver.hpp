@@ -72,6 +72,11 @@ class Solver {
     // polls of a staged-copy wait before the fused pass reports a timeout
     // (0: at once; < 0: the default)
     void set_wait_limit(long long polls);
+    // tiled FB_p_v kernel: shape of the full (kind 0) or lean (1) tiles --
+    // rows, column vectors and planes per tile, ring stages; selects it
+    void set_tile_shape(int kind, int rows, int vectors, int planes, int stages);
+    // {per kind: rows, vectors, planes, stages, threads, tiles} x 2, tiled kernel on
+    std::array<int, 13> tile_shape() const;
 
    private:
     friend class Ensemble;

@@ -507,6 +507,7 @@ def run_gpu(args, rank, world, local_rank):
                 tile = None
         if tile is None:
             tile = a.autotune(10)  # the project's tile autotuner, on this domain
+        shape = a.tile_shape()
         a.set_receivers(rec)
         a.reset(horizon)
         for _ in range(args.warmup):
@@ -538,6 +539,7 @@ def run_gpu(args, rank, world, local_rank):
         ab = algorithmic_bytes(case, word)
         achieved = ab["bytes_per_step"] / (dev_ms * 1e-3 / steps_total) / 1e9
         results[prec] = {"gcell": gcell, "ms_per_bench_step": dev_ms / args.steps, "wall_s": wall, "tile": tile,
+                         "shape": shape,
                          "launches": launches, "achieved_gbs": achieved, "bytes_per_step": ab["bytes_per_step"],
                          "clocks": sampler.summary() if sampler else None}
         # the error statement: receiver p(t) over the workload's full 4000
@@ -568,8 +570,9 @@ def run_gpu(args, rank, world, local_rank):
     roof = {"bound": "hbm", "achieved": round(f32["achieved_gbs"], 1), "peak": hbm_peak, "unit": "GB/s",
             "frac": round(f32["achieved_gbs"] / hbm_peak, 4), "traffic": None,
             "peak_kind": peak_kind,
-            "kernel": "k_march (one launch = one FB step of the whole domain), FP32",
-            "tile_rows_planes_threads_width_stages": list(f32["tile"]),
+            "kernel": ("k_tile: full-tile and lean-tile launches, together one FB step of the whole domain, FP32"
+                       if f32["shape"]["tiled"] else "k_march (one launch = one FB step of the whole domain), FP32"),
+            "tile_shapes": f32["shape"] if f32["shape"]["tiled"] else list(f32["tile"]),
             "algorithmic_bytes_per_step": f32["bytes_per_step"]}
     fp32_error = fp32_error_statement(results["trace_f32"], results["trace_f64"], case.dt, local_rank)
     prof = os.path.join(ROOT, "profiles", "traffic.txt")
@@ -586,7 +589,7 @@ def run_gpu(args, rank, world, local_rank):
                    "cells_per_fb_step": cells, "l2": "flushed (512 MB write) between bench steps",
                    "parallelism": f"replicas x{world}" if world > 1 else "single device-resident domain"},
         "fp64": {"value": round(f64["gcell"], 3), "ms_per_step": round(f64["ms_per_bench_step"], 4),
-                 "tile_rows_planes_threads_width_stages": list(f64["tile"]),
+                 "tile_shapes": f64["shape"] if f64["shape"]["tiled"] else list(f64["tile"]),
                  "achieved_gbs": round(f64["achieved_gbs"], 1),
                  "frac": round(f64["achieved_gbs"] / hbm_peak, 4),
                  "fp32_speedup": round(f32["gcell"] / f64["gcell"], 3)},

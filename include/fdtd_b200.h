@@ -110,7 +110,8 @@ int fdtd_get_slab(fdtd_solver *h, int s, int comp, double *out, int *dims);
 size_t fdtd_state_elems(const fdtd_solver *h);
 int fdtd_copy_state(fdtd_solver *h, int dir, void *host);
 
-/* Tile shape of the single-pass FB_p_v marching kernel: rows_per_block
+/* Tile shape of the single-pass FB_p_v row marching kernel (selecting it
+ * in place of the tiled kernel below): rows_per_block
  * i-rows x all j columns x planes_per_block g-planes per thread block. A
  * thread owns vector_width consecutive columns (0: 16 bytes of columns, i.e.
  * 4 in FP32 and 2 in FP64; else 2 or 4 with vector_width * element size <=
@@ -125,10 +126,28 @@ int fdtd_copy_state(fdtd_solver *h, int dir, void *host);
 int fdtd_set_tiling(fdtd_solver *h, int rows_per_block, int planes_per_block, int threads_per_block,
                     int vector_width, int ring_stages);
 
+/* The tiled FB_p_v kernel (the default for FB_p_v): each thread block
+ * marches one tile of rows x 16-byte column vectors x planes; tiles follow
+ * the PML layers and their storage, so "full" tiles (kind 0: PML, faces,
+ * TDBC, inclusions) and "lean" tiles (kind 1: interior air or porous ground)
+ * run as two launches. fdtd_set_tile_shape sets the largest tile of a kind
+ * (rows >= 2, vectors >= 2, planes >= 1, ring_stages 3..12 planes of the
+ * TMA staging ring; at most 384 threads = (rows + 1) x (vectors + 1)) and
+ * selects the tiled kernel again after fdtd_set_tiling; FDTD_ERR_ARG for
+ * a bad shape, FDTD_ERR_UNSUPPORTED when it does not fit the device.
+ * fdtd_get_tile_shape: out[13] = per kind (full, lean) rows, vectors,
+ * planes, stages, threads per block, tiles per step; out[12] = 1 when the
+ * tiled kernel is active. No counterpart in the reference (its loops sweep
+ * the whole domain per half step, air.cpp:1476-2322). */
+int fdtd_set_tile_shape(fdtd_solver *h, int kind, int rows, int vectors, int planes, int ring_stages);
+int fdtd_get_tile_shape(const fdtd_solver *h, int *out);
+
 /* Times each candidate tile on this handle's domain (nsteps FB steps each,
  * CUDA events), keeps the fastest and returns it in best[5] (rows, planes,
  * threads, vector width, ring stages); the state is reset to t = 0
- * afterwards. */
+ * afterwards. With the tiled kernel active it tunes the lean and then the
+ * full tile shape (read them with fdtd_get_tile_shape) and best[] describes
+ * the full tiles; after fdtd_set_tiling it tunes the row marching kernel. */
 int fdtd_autotune(fdtd_solver *h, int nsteps, int *best);
 
 /* Kernel launches issued since creation (both passes, graphs included). */

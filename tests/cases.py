@@ -188,6 +188,19 @@ def wide_2d():
     return c, [(0.05, 20.5, 0.5), (0.05, 25.0, 1.0), (0.05, 40.0, 0.3)]
 
 
+def very_wide_2d():
+    """2D (NI = 3) with 1300 columns: wider than the row marching kernel's
+    limit (256 threads of one 16-byte column vector each), so only the
+    tiled kernel runs it; porous ground and PML."""
+    layer = 4
+    c = _base(ni=3, nj=1300, nk=24, steps=24, bc=(PML, POROUS, PML, PML, RIGID, RIGID),
+              pml_nodes=(0, 0, 10, 10, 0, 8), pore=(math.sqrt(1.5), 0.4, 1.0e5))
+    c.pore_Z = uniform_axis(layer + 2, -layer * D, D)
+    c.pore_dxyz = (D, D, D)
+    c.source = (0.05, 32.0, 0.4)
+    return c, [(0.05, 32.3, 0.4), (0.05, 33.0, 0.6), (0.05, 60.0, 0.3)]
+
+
 ENS_SMALL = ((24, 36), (16, 20), (10, 13))  # NJ, NK, 3D NI ranges of the small ensemble members
 
 
@@ -209,5 +222,5 @@ CASES: Dict[str, Callable[[], Tuple[Case, List]]] = {
     for f in [pml_rigid, tdbc_east, porous_ground, porous_tdbc_fine_pore, south_pml_all_faces, front_only_pml,
               back_only_pml, all_rigid, wind_linear, wind_log, wind_vortex, hill(1), hill(2), hill(3), hill(4),
               hill(5), moving_frame, fb_v_p, delayed_y1, stretched, odd_columns_wind, odd_columns_porous, narrow_y,
-              ensemble_member_2d, ensemble_member_3d, wide_2d]
+              ensemble_member_2d, ensemble_member_3d, wide_2d, very_wide_2d]
 }

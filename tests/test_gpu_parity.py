@@ -248,3 +248,78 @@ def test_half_step_past_horizon_is_state_error(case_dirs):
         assert a.receivers(0, 2).shape == (2, len(rec))
         a.reset(2)
         a.Cal_pressure()  # usable again after a reset
+
+
+# (rows, vectors, planes, ring stages) of the full and the lean tiles of the
+# tiled kernel: single-row / single-vector / single-plane tiles at the
+# minimum ring depth, odd splits, tiles larger than the domain, deep rings
+TILE_SHAPES = [((2, 2, 1, 3), (2, 2, 1, 3)), ((3, 5, 2, 4), (5, 3, 3, 3)), ((16, 8, 40, 5), (8, 32, 7, 6)),
+               ((4, 16, 5, 12), (16, 16, 64, 3))]
+
+
+@pytest.mark.parametrize("shapes", TILE_SHAPES)
+@pytest.mark.parametrize("name", ["porous_tdbc_fine_pore", "south_pml_all_faces", "wind_log", "moving_frame",
+                                  "odd_columns_wind", "odd_columns_porous", "narrow_y", "hill5", "delayed_y1"])
+def test_tile_shapes_match_oracle(name, shapes, case_dirs):
+    """The tiled kernel is exact for any tile shape: full and lean tiles,
+    halo rows and column vectors, warm-up planes, face rows and columns."""
+    d, rec, n = case_dirs[name]
+    ref = oracle.run_case(d, rec, n)
+    with pkg.Airpore(d, "f64") as a:
+        a.set_tile_shape(0, *shapes[0])
+        a.set_tile_shape(1, *shapes[1])
+        assert a.tile_shape()["tiled"]
+        a.set_receivers(rec)
+        r = a.get_output(n)
+        errs = {"receivers": rel_l2(r, ref["receivers"])}
+        for f in "puvw":
+            errs[f] = rel_l2(a.field(f), ref[f])
+            if a.has_pore:
+                errs["pore_" + f] = rel_l2(a.field(f, "pore"), ref["pore_" + f])
+        errs["psi"] = rel_l2(a.psi(), ref["psi"])
+        sl = a.slabs()
+        for s, q in ref["slabs"].items():
+            for c in "uvwp":
+                errs[f"Q{c}_{s}"] = rel_l2(sl[s][c], q[c])
+    assert max(errs.values()) <= TOL_F64, errs
+
+
+def test_kernel_selection(case_dirs):
+    """FB_p_v runs the tiled kernel by default (full + lean launches per
+    step); set_tiling selects the row marching kernel (one launch per step)
+    and set_tile_shape the tiled one again; all three agree to rounding."""
+    d, rec, n = case_dirs["porous_ground"]
+    with pkg.Airpore(d, "f64") as a:
+        ts = a.tile_shape()
+        assert ts["tiled"] and ts["full"]["tiles"] > 0 and ts["lean"]["tiles"] > 0
+        a.set_receivers(rec)
+        l0 = a.launch_count()
+        r1 = a.get_output(n)
+        assert a.launch_count() - l0 == 2 * n
+        a.set_tiling(4, 8, 256)
+        assert not a.tile_shape()["tiled"]
+        l0 = a.launch_count()
+        r2 = a.get_output(n)
+        assert a.launch_count() - l0 == n
+        a.set_tile_shape(0, 8, 16, 16, 4)
+        assert a.tile_shape()["tiled"]
+        r3 = a.get_output(n)
+    assert rel_l2(r2, r1) <= 1e-13 and rel_l2(r3, r1) <= 1e-13
+
+
+def test_rows_wider_than_row_marching_kernel(case_dirs):
+    """1300 columns: only the tiled kernel runs this domain (the row marching
+    kernel refuses its tiling), in both precisions."""
+    d, rec, n = case_dirs["very_wide_2d"]
+    ref = oracle.run_case(d, rec, n)
+    for prec, tol in (("f64", TOL_F64), ("f32", TOL_F32)):
+        with pkg.Airpore(d, prec) as a:
+            assert a.tile_shape()["tiled"]
+            with pytest.raises(pkg.FdtdError) as e:
+                a.set_tiling(2, 8, 256)
+            assert e.value.code == pkg.FDTD_ERR_UNSUPPORTED
+            a.set_receivers(rec)
+            r = a.get_output(n)
+            errs = {"receivers": rel_l2(r, ref["receivers"]), "p": rel_l2(a.field("p"), ref["p"]),
+                    "pore_p": rel_l2(a.field("p", "pore"), ref["pore_p"])}
+        assert max(errs.values()) <= tol, (prec, errs)
