@@ -8,6 +8,7 @@ An object is rebuilt when its source or any header is newer.
 
 from __future__ import annotations
 
+import concurrent.futures
 import os
 import shutil
 import subprocess
@@ -23,7 +24,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
               "--expt-relaxed-constexpr", "-I", os.path.join(ROOT, "include")]
 
-SOURCES = ["fdtd_solver.cu", "fdtd_input.cpp", "fdtd_capi.cpp", "fdtd_noalloc.cu", "fdtd_spectra.cu", "mlp.cu"]
+SOURCES = ["fdtd_k_tile.cu", "fdtd_k_march.cu", "mlp.cu", "fdtd_solver.cu", "fdtd_k_twopass.cu", "fdtd_noalloc.cu",
+           "fdtd_spectra.cu", "fdtd_input.cpp", "fdtd_capi.cpp"]
 
 
 def nvcc() -> str:
@@ -50,7 +52,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
         return LIB
     objdir = os.path.join(LIBDIR, "obj")
     os.makedirs(objdir, exist_ok=True)
-    objs = []
+    objs, cmds = [], []
     for src in SOURCES:
         obj = os.path.join(objdir, os.path.splitext(src)[0] + ".o")
         objs.append(obj)
@@ -61,7 +63,13 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
             cmd += ["-Xptxas", "-v"]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
-        subprocess.run(cmd, check=True)
+        cmds.append(cmd)
+    # the translation units are independent: compile them side by side
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        for r in list(ex.map(lambda c: subprocess.run(c, capture_output=True, text=True), cmds)):
+            sys.stderr.write(r.stdout + r.stderr)
+            if r.returncode != 0:
+                raise subprocess.CalledProcessError(r.returncode, r.args)
     cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)

@@ -1,0 +1,46 @@
+// Launchers of the time-marching kernels. Each kernel family is compiled in
+// its own translation unit (fdtd_k_*.cu) with explicit instantiations for
+// float and double, so the host solver never instantiates a kernel template
+// itself and the families compile in parallel.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "fdtd_device.cuh"
+#include "fdtd_march.cuh"
+#include "fdtd_tile.cuh"
+
+namespace fdtd {
+
+// two-pass kernels (fdtd_k_twopass.cu): pressure or velocity pass
+template <typename R>
+void run_two_pass(bool pressure, bool wind, dim3 grd, dim3 blk, cudaStream_t s, const Dev<R>& d, int code);
+
+// moving-frame row shift (fdtd_k_twopass.cu)
+template <typename R>
+void run_shift_rows(cudaStream_t s, R* a, int rows, int nj, int sh, int lead, int tempJ, int J, int west_copy);
+
+// row marching kernel (fdtd_k_march.cu); VW columns per thread (4: FP32 only)
+template <typename R>
+const void* march_kernel_ptr(int VW, bool wind, bool xf);
+template <typename R>
+void run_march(int VW, bool wind, bool xf, dim3 grd, dim3 blk, size_t smem, cudaStream_t s, const Dev<R>& d,
+               const MarchTiling& t, int par);
+
+// batched row marching kernel of the ensemble (fdtd_k_march.cu)
+template <typename R>
+const void* march_batch_kernel_ptr(int VW, bool wind, bool xf);
+template <typename R>
+void run_march_batch(int VW, bool wind, bool xf, dim3 grd, dim3 blk, size_t smem, cudaStream_t s,
+                     const BatchWork* work, const BatchEntry<R>* entries, int nm, int phase);
+
+// tiled kernel (fdtd_k_tile.cu); form 0: lean tiles, 1: full tiles,
+// 2: full tiles with the rarer features (inclusion mask, east TDBC,
+// vectors holding both y layers)
+template <typename R>
+const void* tile_kernel_ptr(int form, bool wind);
+template <typename R>
+void run_tile(int form, bool wind, dim3 grd, dim3 blk, size_t smem, cudaStream_t s, const Dev<R>& d,
+              const TileMaps& maps, const TileGeo& tg, const TileBox* work, int par);
+
+}  // namespace fdtd

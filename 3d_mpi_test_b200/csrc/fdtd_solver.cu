@@ -17,9 +17,7 @@
 #include <fstream>
 #include <cuda_runtime.h>
 
-#include "fdtd_device.cuh"
-#include "fdtd_march.cuh"
-#include "fdtd_tile.cuh"
+#include "fdtd_kernels.hpp"
 
 namespace fdtd {
 
@@ -782,13 +780,7 @@ class SolverImpl final : public SolverImplBase {
         const dim3 grd((NJ_ + 31) / 32, (NI_ + 7) / 8, NG_);
         const Dev<R> d = params(pressure, par);
         const int code = (first ? 1 : 0) | (par << 1);
-        if (pressure) {
-            if (wind_on_) k_pressure<R, true><<<grd, blk, 0, stream_>>>(d, code);
-            else k_pressure<R, false><<<grd, blk, 0, stream_>>>(d, code);
-        } else {
-            if (wind_on_) k_velocity<R, true><<<grd, blk, 0, stream_>>>(d, code);
-            else k_velocity<R, false><<<grd, blk, 0, stream_>>>(d, code);
-        }
+        run_two_pass<R>(pressure, wind_on_, grd, blk, stream_, d, code);
         FDTD_CK(cudaGetLastError());
         ++launches_;
     }
@@ -888,12 +880,7 @@ class SolverImpl final : public SolverImplBase {
 
     template <bool XF>
     static const void* march_kernel(int VW, bool wind) {
-        if constexpr (sizeof(R) == 4) {
-            if (VW == 4) return wind ? reinterpret_cast<const void*>(k_march<R, true, 4, XF>)
-                                     : reinterpret_cast<const void*>(k_march<R, false, 4, XF>);
-        }
-        return wind ? reinterpret_cast<const void*>(k_march<R, true, 2, XF>)
-                    : reinterpret_cast<const void*>(k_march<R, false, 2, XF>);
+        return march_kernel_ptr<R>(VW, wind, XF);
     }
 
     template <typename F>
@@ -969,15 +956,7 @@ class SolverImpl final : public SolverImplBase {
     template <bool XF>
     void launch_march(const Dev<R>& d, int par, cudaStream_t s) {
         const dim3 grd(tiling_.nrb, tiling_.nchunk, 1), blk(fused_threads_, 1, 1);
-        if constexpr (sizeof(R) == 4) {
-            if (tiling_.VW == 4) {
-                if (wind_on_) k_march<R, true, 4, XF><<<grd, blk, fused_smem_, s>>>(d, tiling_, par);
-                else k_march<R, false, 4, XF><<<grd, blk, fused_smem_, s>>>(d, tiling_, par);
-                return;
-            }
-        }
-        if (wind_on_) k_march<R, true, 2, XF><<<grd, blk, fused_smem_, s>>>(d, tiling_, par);
-        else k_march<R, false, 2, XF><<<grd, blk, fused_smem_, s>>>(d, tiling_, par);
+        run_march<R>(tiling_.VW, wind_on_, XF, grd, blk, fused_smem_, s, d, tiling_, par);
     }
 
     void enqueue_step(int par) {
@@ -1029,8 +1008,7 @@ class SolverImpl final : public SolverImplBase {
         // fields (all media) and p's west copy: calculation_2D.cpp:458-481
         const int rows = NI_ * NG_;
         for (int c = 0; c < 4; ++c) {
-            k_shift_rows<R><<<(rows + 127) / 128, 128, 0, stream_>>>(F_[par_][c], rows, NJP_, sh, lead, tempJ, NJ_,
-                                                                     c == 3 ? 1 : 0);
+            run_shift_rows<R>(stream_, F_[par_][c], rows, NJP_, sh, lead, tempJ, NJ_, c == 3 ? 1 : 0);
             FDTD_CK(cudaGetLastError());
             ++launches_;
         }
@@ -1039,8 +1017,7 @@ class SolverImpl final : public SolverImplBase {
             if (!slab_n_[s]) continue;
             const int r = slab_[s].ni * slab_[s].nk;
             for (int c = 0; c < 4; ++c) {
-                k_shift_rows<R><<<(r + 127) / 128, 128, 0, stream_>>>(Q_[s][par_][c], r, slab_[s].jp, sh, lead, tempJ,
-                                                                      NJ_, 0);
+                run_shift_rows<R>(stream_, Q_[s][par_][c], r, slab_[s].jp, sh, lead, tempJ, NJ_, 0);
                 FDTD_CK(cudaGetLastError());
                 ++launches_;
             }
@@ -1538,8 +1515,7 @@ class SolverImpl final : public SolverImplBase {
 
     template <bool FULL, bool XF>
     static const void* tile_kernel(bool wind) {
-        return wind ? reinterpret_cast<const void*>(k_tile<R, true, kVecMax, FULL, XF>)
-                    : reinterpret_cast<const void*>(k_tile<R, false, kVecMax, FULL, XF>);
+        return tile_kernel_ptr<R>(FULL ? (XF ? 2 : 1) : 0, wind);
     }
 
     // Cuts the core planes x rows x column vectors into tiles whose
@@ -1669,8 +1645,7 @@ class SolverImpl final : public SolverImplBase {
         const Dev<R> d = params_fused(par);
         const TileBox* w = d_tiles_ + (FULL ? 0 : ntile_[0]);
         const dim3 grd(static_cast<unsigned>(ntile_[k])), blk(static_cast<unsigned>(tthr_[k]));
-        if (wind_on_) k_tile<R, true, kVecMax, FULL, XF><<<grd, blk, tsmem_[k], s>>>(d, tmaps_[k][par], tgeo_[k], w, par);
-        else k_tile<R, false, kVecMax, FULL, XF><<<grd, blk, tsmem_[k], s>>>(d, tmaps_[k][par], tgeo_[k], w, par);
+        run_tile<R>(FULL ? (XF ? 2 : 1) : 0, wind_on_, grd, blk, tsmem_[k], s, d, tmaps_[k][par], tgeo_[k], w, par);
         FDTD_CK(cudaGetLastError());
         ++launches_;
     }
@@ -2272,13 +2247,7 @@ class EnsembleImpl final : public EnsembleImplBase {
 
     template <bool XF>
     static const void* kernel_xf(const Group& g) {
-        if constexpr (sizeof(R) == 4) {
-            if (g.VW == 4)
-                return g.wind ? reinterpret_cast<const void*>(k_march_batch<R, true, 4, XF>)
-                              : reinterpret_cast<const void*>(k_march_batch<R, false, 4, XF>);
-        }
-        return g.wind ? reinterpret_cast<const void*>(k_march_batch<R, true, 2, XF>)
-                      : reinterpret_cast<const void*>(k_march_batch<R, false, 2, XF>);
+        return march_batch_kernel_ptr<R>(g.VW, g.wind, XF);
     }
     static const void* kernel(const Group& g) { return g.xf ? kernel_xf<true>(g) : kernel_xf<false>(g); }
 
@@ -2286,15 +2255,7 @@ class EnsembleImpl final : public EnsembleImplBase {
     void launch_xf(const Group& g, int phase) {
         const dim3 grd(static_cast<unsigned>(g.work.size())), blk(g.threads);
         const int nm = static_cast<int>(g.members.size());
-        if constexpr (sizeof(R) == 4) {
-            if (g.VW == 4) {
-                if (g.wind) k_march_batch<R, true, 4, XF><<<grd, blk, g.smem, g.stream>>>(g.d_work, g.d_entries, nm, phase);
-                else k_march_batch<R, false, 4, XF><<<grd, blk, g.smem, g.stream>>>(g.d_work, g.d_entries, nm, phase);
-                return;
-            }
-        }
-        if (g.wind) k_march_batch<R, true, 2, XF><<<grd, blk, g.smem, g.stream>>>(g.d_work, g.d_entries, nm, phase);
-        else k_march_batch<R, false, 2, XF><<<grd, blk, g.smem, g.stream>>>(g.d_work, g.d_entries, nm, phase);
+        run_march_batch<R>(g.VW, g.wind, XF, grd, blk, g.smem, g.stream, g.d_work, g.d_entries, nm, phase);
     }
 
     void launch(const Group& g, int phase) {

@@ -90,6 +90,13 @@ def test_ensemble_argument_checks():
 
 
 # ------------------------------------------------------------------ GPU
+def _member_launches_per_step(a) -> int:
+    s = a.tile_shape()
+    if not s["tiled"]:
+        return 1
+    return int(s["full"]["tiles"] > 0) + int(s["lean"]["tiles"] > 0)
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("precision,tile,mode", [("f32", None, 0), ("f64", None, 0), ("f32", (2, 3, 48, 2, 5), 0),
                                                  ("f64", (8, 7, 1000, 0, 0), 0), ("f32", None, 1),
@@ -109,7 +116,9 @@ def test_batch_equals_single_solves(precision, tile, mode, tmp_path):
         assert e.advance(7) == 7
         assert e.advance(steps) == steps - 7  # capped at the members' horizon
         info = e.info()
-        per_step = info["groups"] if mode == 0 else len(mem)  # mode 1: each member's own launch
+        # mode 1: each member's own launches (tiled members: one for the
+        # full tiles and one for the lean tiles where both exist)
+        per_step = info["groups"] if mode == 0 else sum(_member_launches_per_step(a) for a in mem)
         assert info["launches"] == steps * per_step and info["blocks_per_step"] >= 6
     tol = 1e-10 if precision == "f64" else 1e-4
     same = 1e-13 if precision == "f64" else 1e-5  # batch vs single: rounding only
