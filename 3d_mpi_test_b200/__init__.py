@@ -266,16 +266,18 @@ class Airpore:
                                             vector_width, ring_stages))
 
     def set_tile_shape(self, kind: int, rows: int, vectors: int, planes: int, ring_stages: int = 4) -> None:
-        """Largest tile of the tiled kernel for kind 0 (full tiles: PML,
-        faces, TDBC) or 1 (lean interior tiles): rows, 16-byte column vectors
-        and planes per tile, TMA ring stages; selects the tiled kernel."""
+        """Largest tile of the tiled kernel for kind 0 (full tiles: faces,
+        PML edges and corners, TDBC), 1 (lean interior tiles) or 2 (tiles
+        inside one PML layer): rows, 16-byte column vectors and planes per
+        tile, TMA ring stages; selects the tiled kernel."""
         self._check(self._L.fdtd_set_tile_shape(self._h, kind, rows, vectors, planes, ring_stages))
 
     def tile_shape(self) -> dict:
-        out = (ctypes.c_int * 13)()
+        out = (ctypes.c_int * 19)()
         self._check(self._L.fdtd_get_tile_shape(self._h, out))
         keys = ("rows", "vectors", "planes", "stages", "threads", "tiles")
-        return {"full": dict(zip(keys, out[0:6])), "lean": dict(zip(keys, out[6:12])), "tiled": bool(out[12])}
+        return {"full": dict(zip(keys, out[0:6])), "lean": dict(zip(keys, out[6:12])),
+                "pml": dict(zip(keys, out[12:18])), "tiled": bool(out[18])}
 
     def autotune(self, nsteps: int = 20) -> Tuple[int, int, int, int, int]:
         best = (ctypes.c_int * 5)()

@@ -166,7 +166,7 @@ int fdtd_get_tile_shape(const fdtd_solver* h, int* out) {
     if (!h || !out) return bad("null argument");
     return guard([&] {
         const auto t = h->s->tile_shape();
-        for (int q = 0; q < 13; ++q) out[q] = t[q];
+        for (int q = 0; q < 19; ++q) out[q] = t[q];
     });
 }
 

@@ -1,5 +1,6 @@
 // Tiled FB_p_v kernel (lean and full tile forms), instantiated for float
-// (4-column vectors) and double (2-column vectors).
+// (4-column vectors) and double (2-column vectors); the single-layer PML
+// forms live in fdtd_k_tile_pml.cu.
 #include "fdtd_kernels.hpp"
 
 namespace fdtd {
@@ -7,6 +8,7 @@ namespace fdtd {
 template <typename R>
 const void* tile_kernel_ptr(int form, bool wind) {
     constexpr int V = static_cast<int>(16 / sizeof(R));
+    if (form >= 3) return tile_pml_kernel_ptr<R>(form - 3, wind);
     switch (form) {
         case 0:
             return wind ? reinterpret_cast<const void*>(k_tile<R, true, V, false, false>)
@@ -24,6 +26,10 @@ template <typename R>
 void run_tile(int form, bool wind, dim3 grd, dim3 blk, size_t smem, cudaStream_t s, const Dev<R>& d,
               const TileMaps& maps, const TileGeo& tg, const TileBox* work, int par) {
     constexpr int V = static_cast<int>(16 / sizeof(R));
+    if (form >= 3) {
+        run_tile_pml<R>(form - 3, wind, grd, blk, smem, s, d, maps, tg, work, par);
+        return;
+    }
     switch (form) {
         case 0:
             if (wind) k_tile<R, true, V, false, false><<<grd, blk, smem, s>>>(d, maps, tg, work, par);

@@ -9,6 +9,7 @@
 #include "fdtd_device.cuh"
 #include "fdtd_march.cuh"
 #include "fdtd_tile.cuh"
+#include "fdtd_tile_pml.cuh"
 
 namespace fdtd {
 
@@ -36,11 +37,20 @@ void run_march_batch(int VW, bool wind, bool xf, dim3 grd, dim3 blk, size_t smem
 
 // tiled kernel (fdtd_k_tile.cu); form 0: lean tiles, 1: full tiles,
 // 2: full tiles with the rarer features (inclusion mask, east TDBC,
-// vectors holding both y layers)
+// vectors holding both y layers), 3 + LM: PML / face tiles with the
+// layers of set LM compiled in (bit 0 x, bit 1 y, bit 2 z)
 template <typename R>
 const void* tile_kernel_ptr(int form, bool wind);
 template <typename R>
 void run_tile(int form, bool wind, dim3 grd, dim3 blk, size_t smem, cudaStream_t s, const Dev<R>& d,
               const TileMaps& maps, const TileGeo& tg, const TileBox* work, int par);
+
+// PML / face tiles (fdtd_k_tile_pml_f32.cu, fdtd_k_tile_pml_f64.cu);
+// lm: the layer set
+template <typename R>
+const void* tile_pml_kernel_ptr(int lm, bool wind);
+template <typename R>
+void run_tile_pml(int lm, bool wind, dim3 grd, dim3 blk, size_t smem, cudaStream_t s, const Dev<R>& d,
+                  const TileMaps& maps, const TileGeo& tg, const TileBox* work, int par);
 
 }  // namespace fdtd

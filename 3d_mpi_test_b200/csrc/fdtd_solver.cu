@@ -169,7 +169,7 @@ class SolverImplBase {
     virtual void get_receivers(int first_step, int nsteps, double* out) = 0;
     virtual void set_wait_limit(long long polls) = 0;
     virtual void set_tile_shape_api(int kind, int TI, int TV, int GC, int ns) = 0;
-    virtual std::array<int, 13> tile_shape() const = 0;
+    virtual std::array<int, 19> tile_shape() const = 0;
 };
 
 template <typename R>
@@ -206,11 +206,14 @@ class SolverImpl final : public SolverImplBase {
             set_tiling(TI, 16, 256, 0, 0);
         }
         if (fused_) {
-            FDTD_CK(cudaStreamCreateWithFlags(&stream2_, cudaStreamNonBlocking));
             FDTD_CK(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming));
-            FDTD_CK(cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming));
+            for (int k = 1; k < kKinds; ++k) {
+                FDTD_CK(cudaStreamCreateWithFlags(&kstream_[k], cudaStreamNonBlocking));
+                FDTD_CK(cudaEventCreateWithFlags(&ev_join_[k], cudaEventDisableTiming));
+            }
             tcfg_[0] = default_tile(false);
             tcfg_[1] = default_tile(true);
+            tcfg_[2] = default_tile(false);
             tile_on_ = true;
             build_tiles();
         }
@@ -224,8 +227,10 @@ class SolverImpl final : public SolverImplBase {
         if (d_rec_out_) cudaFree(d_rec_out_);
         if (d_tiles_) cudaFree(d_tiles_);
         if (ev_fork_) cudaEventDestroy(ev_fork_);
-        if (ev_join_) cudaEventDestroy(ev_join_);
-        if (stream2_) cudaStreamDestroy(stream2_);
+        for (int k = 1; k < kKinds; ++k) {
+            if (ev_join_[k]) cudaEventDestroy(ev_join_[k]);
+            if (kstream_[k]) cudaStreamDestroy(kstream_[k]);
+        }
         if (ev0_) cudaEventDestroy(ev0_);
         if (ev1_) cudaEventDestroy(ev1_);
         if (stream_) cudaStreamDestroy(stream_);
@@ -921,15 +926,24 @@ class SolverImpl final : public SolverImplBase {
     }
 
     // one fused step at parity par on the handle's stream; tiled form: the
-    // lean tiles run on a second stream, forked from and joined to it, so
-    // both launches share the device
+    // kinds other than the generic full tiles run on streams of their own,
+    // forked from and joined to it, so all launches of a step share the
+    // device
     void launch_fused(int par) {
-        if (tile_on_ && ntile_[1] && ntile_[0]) {
+        if (tile_on_) {
+            cudaStream_t st[kKinds];
+            st[0] = stream_;
             FDTD_CK(cudaEventRecord(ev_fork_, stream_));
-            FDTD_CK(cudaStreamWaitEvent(stream2_, ev_fork_, 0));
-            launch_tiles(par, stream_, stream2_);
-            FDTD_CK(cudaEventRecord(ev_join_, stream2_));
-            FDTD_CK(cudaStreamWaitEvent(stream_, ev_join_, 0));
+            for (int k = 1; k < kKinds; ++k) {
+                st[k] = kstream_[k];
+                if (ntile_[k]) FDTD_CK(cudaStreamWaitEvent(kstream_[k], ev_fork_, 0));
+            }
+            launch_tiles(par, st);
+            for (int k = 1; k < kKinds; ++k)
+                if (ntile_[k]) {
+                    FDTD_CK(cudaEventRecord(ev_join_[k], kstream_[k]));
+                    FDTD_CK(cudaStreamWaitEvent(stream_, ev_join_[k], 0));
+                }
         } else {
             launch_fused_on(par, stream_);
         }
@@ -938,7 +952,11 @@ class SolverImpl final : public SolverImplBase {
     // one fused step at parity par on stream s (also an ensemble's stream);
     // returns the kernels launched
     int launch_fused_on(int par, cudaStream_t s) {
-        if (tile_on_) return launch_tiles(par, s, s);
+        if (tile_on_) {
+            cudaStream_t st[kKinds];
+            for (int k = 0; k < kKinds; ++k) st[k] = s;
+            return launch_tiles(par, st);
+        }
         if (!old_ok_) fail(-2, "rows too wide for the row marching kernel");
         const Dev<R> d = params_fused(par);
         if (xf_) launch_march<true>(d, par, s);
@@ -949,7 +967,12 @@ class SolverImpl final : public SolverImplBase {
     }
 
     int launches_per_step() const {
-        if (in.scheme == FB_P_V && fused_) return tile_on_ ? (ntile_[0] ? 1 : 0) + (ntile_[1] ? 1 : 0) : 1;
+        if (in.scheme == FB_P_V && fused_) {
+            if (!tile_on_) return 1;
+            int n = 0;
+            for (int k = 0; k < kKinds; ++k) n += ntile_[k] ? 1 : 0;
+            return n;
+        }
         return 2;
     }
 
@@ -1518,64 +1541,114 @@ class SolverImpl final : public SolverImplBase {
         return tile_kernel_ptr<R>(FULL ? (XF ? 2 : 1) : 0, wind);
     }
 
-    // Cuts the core planes x rows x column vectors into tiles whose
-    // boundaries follow the PML layers and their storage, the faces and the
-    // porous/air interface, classifies each as lean (interior air outside
-    // every PML layer and its storage, no inclusion; or porous-ground
-    // interior) or full, orders the full tiles heaviest first, and sizes
-    // both launches.
+    // Tile kinds: 0 generic full tiles (the east-face column vectors, where
+    // the east extrapolation and TDBC live; every tile of a domain with
+    // inclusions), 1 lean tiles (no PML storage, no face), 2 + LM tiles of
+    // the PML / face kernel with layer set LM (bit 0 x, bit 1 y, bit 2 z).
+    // Shape configurations: 0 full, 1 lean, 2 PML / face kinds.
+    static constexpr int kKinds = 10;
+    static int cfg_of(int kind) { return kind >= 2 ? 2 : kind; }
+    int form_of(int kind) const { return kind == 0 ? (xf_ ? 2 : 1) : kind == 1 ? 0 : kind + 1; }
+
+    // Cuts the core planes x rows x column vectors into boxes at the PML
+    // storage boundaries (x1 rows [0, I1], x2 rows [NI-1-I2, NI), y1 / y2
+    // column vectors holding storage columns, z1 / z2 storage planes) and the
+    // east-face vectors, classifies each box, splits it into tiles of its
+    // kind's shape, orders the generic tiles heaviest first, and sizes every
+    // launch. A box's layer set holds the axes whose storage its rows,
+    // vectors or planes lie in; a box outside every storage region has no
+    // node of a layer and no halo node of one whose pressure it reads (the
+    // halo row next to an x storage region is its storage-only row, the last
+    // column of the halo vector next to a y storage region is past the
+    // layer, the plane below one next to a z storage region is its
+    // storage-only plane). Face rows and the west face vector join the
+    // storage boxes next to them, so no tile is a single face sheet where a
+    // PML layer borders the face.
     void build_tiles() {
         const int V = kVecMax, nvec = NJP_ / V;
-        for (int k = 0; k < 2; ++k) check_tile(tcfg_[k]);
-        // lean air box: rows [li0, li1), vectors [lv0, lv1), planes [lg0, lg1),
-        // inside rows [1, NI-2) and vectors [1, nvec-2) so that the tiles at
-        // the high faces keep >= 2 rows (the i-1 pressure of row NI-1's
-        // stencil row) and >= 2 vectors (columns NJ-2..NJ-4 of the east
-        // extrapolation); an empty range adds no cuts
-        const int li0 = std::max(1, I1_ ? I1_ + 1 : 1), li1 = std::min(NI_ - 2, I2_ ? NI_ - 1 - I2_ : NI_ - 1);
-        const int jlo = std::max(1, Y1_ ? Y1_ + 1 : 1), jhi = std::min(NJ_ - 1, Y2_ ? NJ_ - 1 - Y2_ : NJ_ - 1);
-        const int lv0 = std::max(1, (jlo + V - 1) / V), lv1 = std::min(nvec - 2, jhi / V);
-        const int lk0 = K1_ ? K1_ + 1 : 1, lk1 = K2_ ? Kair_ - 1 - K2_ : Kair_ - 1;
-        const int lg0 = std::max(lk0 + gOff_, gAir0_), lg1 = lk1 + gOff_;
-        std::vector<int> rc{0, 1, NI_ - 2, NI_}, vc{0, 1, nvec - 2, nvec}, gc{1, NG_ - 1};
-        if (li0 < li1) rc.insert(rc.end(), {li0, li1});
-        if (lv0 < lv1) vc.insert(vc.end(), {lv0, lv1});
-        if (lg0 < lg1) gc.insert(gc.end(), {lg0, lg1});
-        // porous planes [1, gOff) are lean-capable; plane gOff is also air
-        // k = 0, where the PML integrals are stored, so it stays full
-        if (porous_) gc.insert(gc.end(), {gOff_, gAir0_});
+        for (int k = 0; k < 3; ++k) check_tile(tcfg_[k]);
+        const int xa = I1_ ? I1_ + 1 : 0, xb = I2_ ? NI_ - 1 - I2_ : NI_;
+        const int za = K1_ ? gOff_ + K1_ + 1 : 0, zb = K2_ ? gOff_ + Kair_ - 1 - K2_ : NG_;
+        // the east-face vectors [ve, nvec) stay one segment: their tiles read
+        // the pressure of columns NJ-2..NJ-4 from their own slots; the PML /
+        // face kernel runs them unless the east face is the TDBC or its
+        // column starts a vector (generic kernel)
+        const int ve = nvec - 2;
+        const bool east_generic = tdbc_ || (NJ_ - 1) % V == 0;
+        if (sms_ == 0) FDTD_CK(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device_));
+        const int ya = std::min(Y1_ ? (Y1_ + 1 + V - 1) / V : 0, ve);
+        const int yb = std::min(Y2_ ? (NJ_ - 1 - Y2_) / V : nvec, ve);
+        std::vector<int> rc{0, NI_, xa, xb}, vc{0, nvec, ya, yb}, gc{1, NG_ - 1, za, zb};
+        // the east vectors join the y2 storage vectors before them when the
+        // PML / face kernel runs them (one segment, tiles of >= 2 vectors)
+        if (east_generic || !(yb < ve && ya <= yb)) vc.push_back(ve);
+        if (xa == 0) rc.push_back(1);  // a face row with no x layer beside it: own segment
+        if (xb == NI_) rc.push_back(NI_ - 2);
+        if (ya == 0) vc.push_back(1);
         const auto rows = segments(rc, 0, NI_);
         const auto vecs = segments(vc, 0, nvec);
         const auto planes = segments(gc, 1, NG_ - 1);
         auto overlap = [](int a0, int a1, int b0, int b1) { return std::max(0, std::min(a1, b1) - std::max(a0, b0)); };
         std::vector<std::pair<long long, TileBox>> full;
-        std::vector<TileBox> lean;
-        int maxr[2] = {2, 2}, maxv[2] = {2, 2};
+        std::vector<TileBox> other[kKinds];
+        int maxr[kKinds], maxv[kKinds];
+        for (int k = 0; k < kKinds; ++k) maxr[k] = maxv[k] = 2;
+        struct Box {
+            std::array<int, 2> r, v, g;
+        };
+        std::vector<Box> boxes[kKinds];
         for (const auto& pr : planes)
             for (const auto& rr : rows)
                 for (const auto& vr : vecs) {
-                    bool is_lean;
-                    if (porous_ && pr[1] <= gOff_)  // porous ground: no PML; faces excluded
-                        is_lean = rr[0] >= 1 && rr[1] <= NI_ - 2 && vr[0] >= 1 && vr[1] <= nvec - 2;
-                    else if (porous_ && pr[0] < gAir0_)
-                        is_lean = false;
-                    else
-                        is_lean = !mask_on_ && rr[0] >= li0 && rr[1] <= li1 && vr[0] >= lv0 && vr[1] <= lv1 &&
-                                  pr[0] >= lg0 && pr[1] <= lg1;
-                    const int kind = is_lean ? 1 : 0;
-                    const TileCfg& tc = tcfg_[kind];
+                    const bool rx = rr[1] <= xa || rr[0] >= xb;
+                    const bool vy1 = vr[1] <= ya, vy2 = vr[0] >= yb;
+                    const bool gz = pr[1] <= za || pr[0] >= zb;
+                    int kind;
+                    if (mask_on_ || (vr[1] > ve && east_generic) || (vy1 && vy2) || (vr[0] < ya && vr[1] > yb)) {
+                        kind = 0;
+                    } else {
+                        const int lm = (rx ? kLmX : 0) | (vy1 || vy2 ? kLmY : 0) | (gz ? kLmZ : 0);
+                        const bool faces = rr[0] < 1 || rr[1] > NI_ - 2 || vr[0] < 1 || vr[1] > ve;
+                        kind = lm == 0 && !faces ? 1 : 2 + lm;
+                    }
+                    boxes[kind].push_back({rr, vr, pr});
+                }
+        // Plane chunks: a tile marches its planes one after another, so a
+        // kind with few tiles is bound by that chain; the generic and PML /
+        // face kinds halve their chunk (down to 2 planes) until they have at
+        // least two tiles per SM
+        int gck[kKinds];
+        for (int kind = 0; kind < kKinds; ++kind) {
+            const TileCfg& tc = tcfg_[cfg_of(kind)];
+            auto count = [&](int gcs) {
+                long long n = 0;
+                for (const Box& bx : boxes[kind])
+                    n += static_cast<long long>((bx.r[1] - bx.r[0] + tc.TI - 1) / tc.TI) *
+                         ((bx.v[1] - bx.v[0] + tc.TV - 1) / tc.TV) * ((bx.g[1] - bx.g[0] + gcs - 1) / gcs);
+                return n;
+            };
+            int gcs = tc.GC;
+            if (kind != 1)
+                while (gcs > 2 && count(gcs) < 2LL * sms_) gcs = std::max(2, gcs / 2);
+            gck[kind] = gcs;
+        }
+        for (int kind = 0; kind < kKinds; ++kind)
+            for (const Box& bx : boxes[kind]) {
+                const auto &rr = bx.r, &vr = bx.v, &pr = bx.g;
+                {
+                    const TileCfg& tc = tcfg_[cfg_of(kind)];
                     std::vector<std::array<int, 2>> rp, vp, gp;
                     split_even(rr[0], rr[1], tc.TI, rp);
                     split_even(vr[0], vr[1], tc.TV, vp);
-                    split_even(pr[0], pr[1], tc.GC, gp);
+                    split_even(pr[0], pr[1], gck[kind], gp);
                     for (const auto& a : rp)
                         for (const auto& bq : vp)
                             for (const auto& cq : gp) {
                                 const TileBox t{a[0], a[1], bq[0], bq[1], cq[0], cq[1]};
                                 maxr[kind] = std::max(maxr[kind], a[1] - a[0]);
                                 maxv[kind] = std::max(maxv[kind], bq[1] - bq[0]);
-                                if (is_lean) {
-                                    lean.push_back(t);
+                                if (kind != 0) {
+                                    other[kind].push_back(t);
                                     continue;
                                 }
                                 // estimated cost: nodes with halos, times 1 + 2 per PML layer crossed
@@ -1589,12 +1662,15 @@ class SolverImpl final : public SolverImplBase {
                                 full.push_back({cost, t});
                             }
                 }
+            }
         std::stable_sort(full.begin(), full.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+        for (const auto& f : full) other[0].push_back(f.second);
         std::vector<TileBox> all;
-        for (const auto& f : full) all.push_back(f.second);
-        all.insert(all.end(), lean.begin(), lean.end());
-        ntile_[0] = static_cast<int>(full.size());
-        ntile_[1] = static_cast<int>(lean.size());
+        for (int k = 0; k < kKinds; ++k) {
+            toff_[k] = static_cast<int>(all.size());
+            ntile_[k] = static_cast<int>(other[k].size());
+            all.insert(all.end(), other[k].begin(), other[k].end());
+        }
         if (all.size() > tiles_cap_) {
             if (d_tiles_) cudaFree(d_tiles_);
             d_tiles_ = nullptr;
@@ -1602,17 +1678,20 @@ class SolverImpl final : public SolverImplBase {
             tiles_cap_ = all.size();
         }
         FDTD_CK(cudaMemcpy(d_tiles_, all.data(), sizeof(TileBox) * all.size(), cudaMemcpyHostToDevice));
-        for (int k = 0; k < 2; ++k) {
-            tgeo_[k] = tile_geo(std::min(maxr[k], tcfg_[k].TI) < 2 ? 2 : std::min(maxr[k], tcfg_[k].TI),
-                                std::min(maxv[k], tcfg_[k].TV) < 2 ? 2 : std::min(maxv[k], tcfg_[k].TV), tcfg_[k].ns);
+        bool big = false;
+        for (int k = 0; k < kKinds; ++k) {
+            const TileCfg& tc = tcfg_[cfg_of(k)];
+            tgeo_[k] = tile_geo(std::max(2, std::min(maxr[k], tc.TI)), std::max(2, std::min(maxv[k], tc.TV)), tc.ns);
             tthr_[k] = ((tgeo_[k].TI + 1) * (tgeo_[k].TV + 1) + 31) / 32 * 32;
             tsmem_[k] = tile_smem(tgeo_[k]);
             encode_tile_maps(k);
+            big = big || tsmem_[k] > 48 * 1024;
         }
-        if (tsmem_[0] > 48 * 1024 || tsmem_[1] > 48 * 1024) {
+        if (big) {
             for (bool w : {false, true})
-                for (const void* f : {tile_kernel<true, true>(w), tile_kernel<true, false>(w), tile_kernel<false, false>(w)})
-                    FDTD_CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSmemMax)));
+                for (int f = 0; f < 3 + 8; ++f)
+                    FDTD_CK(cudaFuncSetAttribute(tile_kernel_ptr<R>(f, w), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 static_cast<int>(kSmemMax)));
         }
         if (!sdy_.empty()) update_xf();  // before the first frame upload, which sets it
         graph_dirty_ = true;
@@ -1639,38 +1718,44 @@ class SolverImpl final : public SolverImplBase {
             }
     }
 
-    template <bool FULL, bool XF>
-    void launch_tile(int par, cudaStream_t s) {
-        const int k = FULL ? 0 : 1;
+    // the launch that samples the receivers and publishes the step counter:
+    // the generic kind, else the first PML / face kind present (the lean
+    // kind never does)
+    int book_kind() const {
+        if (ntile_[0]) return 0;
+        for (int k = 2; k < kKinds; ++k)
+            if (ntile_[k]) return k;
+        return -1;
+    }
+
+    void launch_tile_kind(int k, int par, cudaStream_t s) {
         const Dev<R> d = params_fused(par);
-        const TileBox* w = d_tiles_ + (FULL ? 0 : ntile_[0]);
         const dim3 grd(static_cast<unsigned>(ntile_[k])), blk(static_cast<unsigned>(tthr_[k]));
-        run_tile<R>(FULL ? (XF ? 2 : 1) : 0, wind_on_, grd, blk, tsmem_[k], s, d, tmaps_[k][par], tgeo_[k], w, par);
+        const int code = par | (k == book_kind() ? 2 : 0);
+        run_tile<R>(form_of(k), wind_on_, grd, blk, tsmem_[k], s, d, tmaps_[k][par], tgeo_[k], d_tiles_ + toff_[k], code);
         FDTD_CK(cudaGetLastError());
         ++launches_;
     }
 
-    // one step of the tiled kernel: full tiles on s_full, lean tiles on s_lean
-    int launch_tiles(int par, cudaStream_t s_full, cudaStream_t s_lean) {
+    // one step of the tiled kernel: kind k on streams[k] (several kinds
+    // may share a stream); returns the kernels launched
+    int launch_tiles(int par, const cudaStream_t* streams) {
         int n = 0;
-        if (ntile_[0]) {
-            if (xf_) launch_tile<true, true>(par, s_full);
-            else launch_tile<true, false>(par, s_full);
-            ++n;
-        }
-        if (ntile_[1]) {
-            launch_tile<false, false>(par, s_lean);
-            ++n;
-        }
+        for (int k = 0; k < kKinds; ++k)
+            if (ntile_[k]) {
+                launch_tile_kind(k, par, streams[k]);
+                ++n;
+            }
         return n;
     }
 
-    // tile shape of kind 0 (full) or 1 (lean): rows, column vectors and
-    // planes per tile, ring stages; switches to the tiled kernel
+    // tile shape of configuration 0 (full), 1 (lean) or 2 (PML / face
+    // tiles): rows, column vectors and planes per tile, ring stages;
+    // switches to the tiled kernel
     void set_tile_shape_api(int kind, int TI, int TV, int GC, int ns) override {
         FDTD_CK(cudaSetDevice(device_));
         if (!fused_) fail(-2, "tiling applies to the fused FB_p_v pass only");
-        if (kind != 0 && kind != 1) fail(-5, "tile kind must be 0 (full) or 1 (lean)");
+        if (kind < 0 || kind > 2) fail(-5, "tile kind must be 0 (full), 1 (lean) or 2 (PML / face)");
         const TileCfg c{TI, TV, GC, ns};
         check_tile(c);
         FDTD_CK(cudaStreamSynchronize(stream_));
@@ -1679,20 +1764,27 @@ class SolverImpl final : public SolverImplBase {
         build_tiles();
     }
 
-    // {kind 0: rows, vectors, planes, stages, threads, tiles; kind 1: the same}, on = tiled kernel active
-    std::array<int, 13> tile_shape() const override {
-        std::array<int, 13> o{};
-        for (int k = 0; k < 2; ++k) {
-            o[6 * k + 0] = tcfg_[k].TI; o[6 * k + 1] = tcfg_[k].TV; o[6 * k + 2] = tcfg_[k].GC;
-            o[6 * k + 3] = tcfg_[k].ns; o[6 * k + 4] = tthr_[k]; o[6 * k + 5] = ntile_[k];
+    // per configuration 0..2: rows, vectors, planes, stages, threads (the
+    // largest launch of that configuration), tiles; [18] = tiled kernel active
+    std::array<int, 19> tile_shape() const override {
+        std::array<int, 19> o{};
+        for (int c = 0; c < 3; ++c) {
+            o[6 * c + 0] = tcfg_[c].TI; o[6 * c + 1] = tcfg_[c].TV; o[6 * c + 2] = tcfg_[c].GC;
+            o[6 * c + 3] = tcfg_[c].ns;
         }
-        o[12] = tile_on_ ? 1 : 0;
+        for (int k = 0; k < kKinds; ++k) {
+            const int c = cfg_of(k);
+            o[6 * c + 4] = std::max(o[6 * c + 4], ntile_[k] ? tthr_[k] : 0);
+            o[6 * c + 5] += ntile_[k];
+        }
+        o[18] = tile_on_ ? 1 : 0;
         return o;
     }
 
-    // Project autotuner for the tiled kernel: the lean tile shape first
-    // (full tiles at their current shape), then the full tile shape, each
-    // candidate timed over nsteps steps on this domain
+    // Project autotuner for the tiled kernel: the lean tile shape first,
+    // then the PML / face shape, then the full shape (the others at
+    // their current shapes), each candidate timed over nsteps steps on this
+    // domain
     std::array<int, 5> autotune_tiles(int nsteps) {
         std::vector<TileCfg> cands;
         const int V = kVecMax;
@@ -1709,19 +1801,21 @@ class SolverImpl final : public SolverImplBase {
                         cands.push_back(c);
                     }
         const int saved_horizon = horizon_;
-        reset(std::max(horizon_, (nsteps + 2) * static_cast<int>(2 * cands.size() + 2) + 4));
-        for (int kind : {1, 0}) {
-            if (!ntile_[kind]) continue;
-            TileCfg best = tcfg_[kind];
+        reset(std::max(horizon_, (nsteps + 2) * static_cast<int>(3 * cands.size() + 2) + 4));
+        for (int cfg : {1, 2, 0}) {
+            bool used = false;
+            for (int k = 0; k < kKinds; ++k) used = used || (cfg_of(k) == cfg && ntile_[k]);
+            if (!used) continue;
+            TileCfg best = tcfg_[cfg];
             double best_ms = 1e300;
             for (const TileCfg& c : cands) {
-                tcfg_[kind] = c;
+                tcfg_[cfg] = c;
                 build_tiles();
                 advance(2, nullptr);  // graph build and first touch outside the timing
                 advance(nsteps, nullptr);
                 if (last_ms_ < best_ms) { best_ms = last_ms_; best = c; }
             }
-            tcfg_[kind] = best;
+            tcfg_[cfg] = best;
             build_tiles();
         }
         reset(saved_horizon);
@@ -1909,17 +2003,19 @@ class SolverImpl final : public SolverImplBase {
     bool fused_ = false;
     bool old_ok_ = false;  // the row marching kernel fits this domain
     bool xf_ = true;  // marching kernel with the rarer features compiled in
-    // tiled kernel: shapes, geometry and launches of kind 0 (full) and 1 (lean)
+    // tiled kernel: shape configurations (full, lean, single-layer PML) and
+    // the geometry, tiles and launch of each kind
     bool tile_on_ = false;
-    TileCfg tcfg_[2]{};
-    TileGeo tgeo_[2]{};
-    int tthr_[2]{}, ntile_[2]{};
-    size_t tsmem_[2]{};
-    TileMaps tmaps_[2][2]{};  // [kind][time level read]
+    TileCfg tcfg_[3]{};
+    TileGeo tgeo_[kKinds]{};
+    int tthr_[kKinds]{}, ntile_[kKinds]{}, toff_[kKinds]{};
+    size_t tsmem_[kKinds]{};
+    TileMaps tmaps_[kKinds][2]{};  // [kind][time level read]
     TileBox* d_tiles_ = nullptr;
     size_t tiles_cap_ = 0;
-    cudaStream_t stream2_ = nullptr;
-    cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
+    cudaStream_t kstream_[kKinds]{};  // kinds 1.. (kind 0 runs on the handle's stream)
+    int sms_ = 0;                     // multiprocessors of the device
+    cudaEvent_t ev_fork_ = nullptr, ev_join_[kKinds]{};
     MarchTiling tiling_{};
     int fused_threads_ = 0;
     size_t fused_smem_ = 0;
@@ -1970,7 +2066,7 @@ std::array<int, 5> Solver::autotune(int nsteps) { return impl_->autotune(nsteps)
 double Solver::last_device_ms() const { return impl_->last_device_ms(); }
 void Solver::get_receivers(int first_step, int nsteps, double* out) { impl_->get_receivers(first_step, nsteps, out); }
 void Solver::set_tile_shape(int kind, int TI, int TV, int GC, int ns) { impl_->set_tile_shape_api(kind, TI, TV, GC, ns); }
-std::array<int, 13> Solver::tile_shape() const { return impl_->tile_shape(); }
+std::array<int, 19> Solver::tile_shape() const { return impl_->tile_shape(); }
 void Solver::set_wait_limit(long long polls) { impl_->set_wait_limit(polls); }
 
 // ---------------------------------------------------------------- Ensemble

@@ -76,7 +76,7 @@ class Solver {
     // rows, column vectors and planes per tile, ring stages; selects it
     void set_tile_shape(int kind, int rows, int vectors, int planes, int stages);
     // {per kind: rows, vectors, planes, stages, threads, tiles} x 2, tiled kernel on
-    std::array<int, 13> tile_shape() const;
+    std::array<int, 19> tile_shape() const;
 
    private:
     friend class Ensemble;

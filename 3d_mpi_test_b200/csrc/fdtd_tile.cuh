@@ -102,12 +102,14 @@ __global__ void __launch_bounds__(kTileMaxThreads)
     const int ic = min(max(i, 1), NI - 2);  // stencil row (face rows: the clamped row)
     const int jb = (b.v0 + c) * V;
 
+    // par: bit 0 the step's parity, bit 1 this launch samples the
+    // receivers and publishes the step counter (one launch of a step does)
     int step = 0;
     bool y1_on = true;
     if (FULL) {
-        step = d.counters[par];
+        step = d.counters[par & 1];
         y1_on = step + 1 >= d.pml_y_time;
-        march_bookkeeping(d, par, step, blockIdx.x == 0);
+        march_bookkeeping(d, par & 1, step, (par & 2) != 0 && blockIdx.x == 0);
     }
 
     // column data of this thread's vector and row data of its stencil row,

@@ -128,17 +128,19 @@ int fdtd_set_tiling(fdtd_solver *h, int rows_per_block, int planes_per_block, in
 
 /* The tiled FB_p_v kernel (the default for FB_p_v): each thread block
  * marches one tile of rows x 16-byte column vectors x planes; tiles follow
- * the PML layers and their storage, so "full" tiles (kind 0: PML, faces,
- * TDBC, inclusions) and "lean" tiles (kind 1: interior air or porous ground)
- * run as two launches. fdtd_set_tile_shape sets the largest tile of a kind
- * (rows >= 2, vectors >= 2, planes >= 1, ring_stages 3..12 planes of the
- * TMA staging ring; at most 384 threads = (rows + 1) x (vectors + 1)) and
- * selects the tiled kernel again after fdtd_set_tiling; FDTD_ERR_ARG for
- * a bad shape, FDTD_ERR_UNSUPPORTED when it does not fit the device.
- * fdtd_get_tile_shape: out[13] = per kind (full, lean) rows, vectors,
- * planes, stages, threads per block, tiles per step; out[12] = 1 when the
- * tiled kernel is active. No counterpart in the reference (its loops sweep
- * the whole domain per half step, air.cpp:1476-2322). */
+ * the PML layers and their storage, so "full" tiles (kind 0: faces, PML
+ * edges and corners, storage-only PML rows, TDBC, inclusions), "lean" tiles
+ * (kind 1: interior air or porous ground) and single-layer tiles (kind 2:
+ * inside one x, y or z PML layer; three launches, one per axis) run as up
+ * to five launches per step. fdtd_set_tile_shape sets the largest tile of
+ * a kind (rows >= 2, vectors >= 2, planes >= 1, ring_stages 3..12 planes
+ * of the TMA staging ring; at most 384 threads = (rows + 1) x (vectors + 1))
+ * and selects the tiled kernel again after fdtd_set_tiling; FDTD_ERR_ARG
+ * for a bad shape, FDTD_ERR_UNSUPPORTED when it does not fit the device.
+ * fdtd_get_tile_shape: out[19] = per kind (full, lean, single-layer) rows,
+ * vectors, planes, stages, threads per block, tiles per step; out[18] = 1
+ * when the tiled kernel is active. No counterpart in the reference (its
+ * loops sweep the whole domain per half step, air.cpp:1476-2322). */
 int fdtd_set_tile_shape(fdtd_solver *h, int kind, int rows, int vectors, int planes, int ring_stages);
 int fdtd_get_tile_shape(const fdtd_solver *h, int *out);
 

@@ -166,6 +166,28 @@ def odd_columns_porous():
     return c, REC
 
 
+def pml_box_all():
+    """PML on all six faces, wide enough that tiles lie inside one x, y or
+    z layer (single-layer tile kernel) besides the edges, corners, faces
+    and the lean interior."""
+    c = _base(ni=34, nj=46, nk=30, steps=30, bc=(PML,) * 6, pml_nodes=(6, 6, 6, 6, 6, 6))
+    c.source = (0.85, 1.1, 0.75)
+    return c, [(0.85, 1.6, 0.75), (0.1, 1.1, 0.75), (0.85, 0.1, 0.5), (0.85, 1.1, 1.35), (0.2, 2.1, 1.3)]
+
+
+def pml_box_wind_porous():
+    """Porous ground, log wind, y1 PML switched on after 11 steps, layers of
+    odd and unequal widths (5 / 7 rows, 7 / 5 columns, 6 planes): the
+    single-layer tiles with wind, layer boundaries inside column vectors."""
+    layer = 5
+    c = _base(ni=32, nj=45, nk=28, steps=30, bc=(PML, POROUS, PML, PML, PML, PML), pml_nodes=(5, 7, 7, 5, 0, 6),
+              pore=(math.sqrt(1.8), 0.3, 2.0e5), velocity_coef=1.5, velocity_method=5, pml_y=(2.0, 1000.0, 11))
+    c.pore_Z = uniform_axis(layer + 2, -layer * D, D)
+    c.pore_dxyz = (D, D, D)
+    c.source = (0.8, 1.0, 0.3)
+    return c, [(0.8, 1.5, 0.3), (0.1, 1.0, 0.5), (0.8, 0.15, 0.4), (0.8, 1.0, 1.2), (0.8, 2.1, 0.1)]
+
+
 def narrow_y():
     """5 columns with 2-node y PML layers on both sides: one 16-byte column
     vector holds nodes of both y layers."""
@@ -222,5 +244,6 @@ CASES: Dict[str, Callable[[], Tuple[Case, List]]] = {
     for f in [pml_rigid, tdbc_east, porous_ground, porous_tdbc_fine_pore, south_pml_all_faces, front_only_pml,
               back_only_pml, all_rigid, wind_linear, wind_log, wind_vortex, hill(1), hill(2), hill(3), hill(4),
               hill(5), moving_frame, fb_v_p, delayed_y1, stretched, odd_columns_wind, odd_columns_porous, narrow_y,
+              pml_box_all, pml_box_wind_porous,
               ensemble_member_2d, ensemble_member_3d, wide_2d, very_wide_2d]
 }

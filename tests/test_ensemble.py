@@ -90,11 +90,16 @@ def test_ensemble_argument_checks():
 
 
 # ------------------------------------------------------------------ GPU
-def _member_launches_per_step(a) -> int:
-    s = a.tile_shape()
-    if not s["tiled"]:
-        return 1
-    return int(s["full"]["tiles"] > 0) + int(s["lean"]["tiles"] > 0)
+def _launches_per_step(case_dir, precision, tile) -> int:
+    """Kernels one FB step of this member launches on its own (tiled
+    members: one per tile kind present)."""
+    with pkg.Airpore(case_dir, precision) as b:
+        if tile:
+            b.set_tiling(*tile)
+        b.reset(2)
+        n0 = b.launch_count()
+        b.advance(1)
+        return b.launch_count() - n0
 
 
 @pytest.mark.gpu
@@ -118,7 +123,7 @@ def test_batch_equals_single_solves(precision, tile, mode, tmp_path):
         info = e.info()
         # mode 1: each member's own launches (tiled members: one for the
         # full tiles and one for the lean tiles where both exist)
-        per_step = info["groups"] if mode == 0 else sum(_member_launches_per_step(a) for a in mem)
+        per_step = info["groups"] if mode == 0 else sum(_launches_per_step(d, precision, tile) for d, _, _ in ms)
         assert info["launches"] == steps * per_step and info["blocks_per_step"] >= 6
     tol = 1e-10 if precision == "f64" else 1e-4
     same = 1e-13 if precision == "f64" else 1e-5  # batch vs single: rounding only

@@ -250,24 +250,27 @@ def test_half_step_past_horizon_is_state_error(case_dirs):
         a.Cal_pressure()  # usable again after a reset
 
 
-# (rows, vectors, planes, ring stages) of the full and the lean tiles of the
-# tiled kernel: single-row / single-vector / single-plane tiles at the
-# minimum ring depth, odd splits, tiles larger than the domain, deep rings
-TILE_SHAPES = [((2, 2, 1, 3), (2, 2, 1, 3)), ((3, 5, 2, 4), (5, 3, 3, 3)), ((16, 8, 40, 5), (8, 32, 7, 6)),
-               ((4, 16, 5, 12), (16, 16, 64, 3))]
+# (rows, vectors, planes, ring stages) of the full, the lean and the
+# single-layer PML tiles of the tiled kernel: single-row / single-vector /
+# single-plane tiles at the minimum ring depth, odd splits, tiles larger
+# than the domain, deep rings
+TILE_SHAPES = [((2, 2, 1, 3), (2, 2, 1, 3), (2, 2, 1, 3)), ((3, 5, 2, 4), (5, 3, 3, 3), (3, 3, 5, 4)),
+               ((16, 8, 40, 5), (8, 32, 7, 6), (4, 16, 64, 5)), ((4, 16, 5, 12), (16, 16, 64, 3), (16, 8, 3, 12))]
 
 
 @pytest.mark.parametrize("shapes", TILE_SHAPES)
 @pytest.mark.parametrize("name", ["porous_tdbc_fine_pore", "south_pml_all_faces", "wind_log", "moving_frame",
-                                  "odd_columns_wind", "odd_columns_porous", "narrow_y", "hill5", "delayed_y1"])
+                                  "odd_columns_wind", "odd_columns_porous", "narrow_y", "hill5", "delayed_y1",
+                                  "pml_box_all", "pml_box_wind_porous"])
 def test_tile_shapes_match_oracle(name, shapes, case_dirs):
-    """The tiled kernel is exact for any tile shape: full and lean tiles,
-    halo rows and column vectors, warm-up planes, face rows and columns."""
+    """The tiled kernel is exact for any tile shape: full, lean and
+    single-layer PML tiles, halo rows and column vectors, warm-up planes,
+    face rows and columns."""
     d, rec, n = case_dirs[name]
     ref = oracle.run_case(d, rec, n)
     with pkg.Airpore(d, "f64") as a:
-        a.set_tile_shape(0, *shapes[0])
-        a.set_tile_shape(1, *shapes[1])
+        for kind in range(3):
+            a.set_tile_shape(kind, *shapes[kind])
         assert a.tile_shape()["tiled"]
         a.set_receivers(rec)
         r = a.get_output(n)
@@ -284,18 +287,47 @@ def test_tile_shapes_match_oracle(name, shapes, case_dirs):
     assert max(errs.values()) <= TOL_F64, errs
 
 
+@pytest.mark.parametrize("name", ["pml_box_all", "pml_box_wind_porous"])
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_single_layer_tiles_match_oracle(name, precision, case_dirs):
+    """Domains wide enough for tiles inside one PML layer: every field, slab
+    and receiver against the oracle, with the single-layer launches
+    present (one per layer axis)."""
+    d, rec, n = case_dirs[name]
+    ref = oracle.run_case(d, rec, n)
+    with pkg.Airpore(d, precision) as a:
+        ts = a.tile_shape()
+        assert ts["tiled"] and ts["pml"]["tiles"] > 0
+        a.set_receivers(rec)
+        l0 = a.launch_count()
+        r = a.get_output(n)
+        assert (a.launch_count() - l0) >= 3 * n  # full, lean and at least one single-layer launch per step
+        errs = {"receivers": rel_l2(r, ref["receivers"])}
+        for f in "puvw":
+            errs[f] = rel_l2(a.field(f), ref[f])
+            if a.has_pore:
+                errs["pore_" + f] = rel_l2(a.field(f, "pore"), ref["pore_" + f])
+        sl = a.slabs()
+        for s, q in ref["slabs"].items():
+            for c in "uvwp":
+                errs[f"Q{c}_{s}"] = rel_l2(sl[s][c], q[c])
+    assert max(errs.values()) <= (TOL_F64 if precision == "f64" else TOL_F32), errs
+
+
 def test_kernel_selection(case_dirs):
-    """FB_p_v runs the tiled kernel by default (full + lean launches per
-    step); set_tiling selects the row marching kernel (one launch per step)
-    and set_tile_shape the tiled one again; all three agree to rounding."""
+    """FB_p_v runs the tiled kernel by default (a lean launch and one per
+    PML / face layer set present, besides the generic full tiles);
+    set_tiling selects the row marching kernel (one launch per step) and
+    set_tile_shape the tiled one again; all three agree to rounding."""
     d, rec, n = case_dirs["porous_ground"]
     with pkg.Airpore(d, "f64") as a:
         ts = a.tile_shape()
-        assert ts["tiled"] and ts["full"]["tiles"] > 0 and ts["lean"]["tiles"] > 0
+        assert ts["tiled"] and ts["pml"]["tiles"] > 0 and ts["lean"]["tiles"] > 0
         a.set_receivers(rec)
         l0 = a.launch_count()
         r1 = a.get_output(n)
-        assert a.launch_count() - l0 == 2 * n
+        per_step = (a.launch_count() - l0) // n
+        assert a.launch_count() - l0 == per_step * n and 2 <= per_step <= 10
         a.set_tiling(4, 8, 256)
         assert not a.tile_shape()["tiled"]
         l0 = a.launch_count()
