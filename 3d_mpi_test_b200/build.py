@@ -24,8 +24,9 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
               "--expt-relaxed-constexpr", "-I", os.path.join(ROOT, "include")]
 
-SOURCES = ["fdtd_k_tile.cu", "fdtd_k_tile_pml_f32.cu", "fdtd_k_tile_pml_f64.cu", "fdtd_k_march.cu", "mlp.cu", "fdtd_solver.cu", "fdtd_k_twopass.cu", "fdtd_noalloc.cu",
-           "fdtd_spectra.cu", "fdtd_input.cpp", "fdtd_capi.cpp"]
+SOURCES = ["fdtd_k_tile_pml_f32.cu", "fdtd_k_tile_pml_f64.cu", "fdtd_k_tile_pml_f32_ter.cu", "fdtd_k_tile_pml_f64_ter.cu",
+           "fdtd_k_tile_flat.cu", "fdtd_k_tile_ter.cu", "fdtd_k_tile.cu", "fdtd_k_march.cu", "mlp.cu", "fdtd_solver.cu",
+           "fdtd_k_twopass.cu", "fdtd_noalloc.cu", "fdtd_spectra.cu", "fdtd_input.cpp", "fdtd_capi.cpp"]
 
 
 def nvcc() -> str:

@@ -91,6 +91,10 @@ class Case:
     pore_X: Optional[List[float]] = None
     pore_Y: Optional[List[float]] = None
     pore_dxyz: Optional[Tuple[float, float, float]] = None  # line 32
+    # terrain-following grid (extension; terrain.dat): ground elevation at
+    # every Y node. Air nodes are stretched between the ground and the flat
+    # top, porous nodes follow the ground. None: flat ground.
+    terrain: Optional[List[float]] = None
 
     # ------------------------------------------------------------------ #
     @property
@@ -192,10 +196,24 @@ class Case:
             if self.pore_Z is None:
                 raise ValueError("porous south face needs pore_Z")
             files.update(self.pore_coordi_texts())
+        if self.terrain is not None:
+            if len(self.terrain) != self.NJ:
+                raise ValueError("terrain needs one elevation per Y node")
+            files["terrain.dat"] = f"{self.NJ}\n" + " ".join(_fmt(float(v)) for v in self.terrain) + "\n"
         for name, txt in files.items():
             with open(os.path.join(case_dir, name), "w") as f:
                 f.write(txt)
         return case_dir
+
+    def height(self, j: int, k: int) -> float:
+        """Physical height of air node (j, k): the file axis Z[k] stretched
+        between the ground elevation and the flat top (the same expression
+        as the solver's and the oracle's)."""
+        z = self.Z[k]
+        if self.terrain is None:
+            return z
+        H = self.Z[-1]
+        return z + self.terrain[j] * (1.0 - z / H)
 
 
 def write_receivers(path: str, receivers: Sequence[Tuple[float, float, float]]) -> str:
@@ -259,6 +277,43 @@ def porous_ground(ni=128, nj=256, nk=96, layer=16, d=0.05, steps=4000, pml=20, s
         source=src, receiver=receivers[0], dt=0.5 * d / c0,
         pore_Z=pore_Z, pore_dxyz=(d, d, d),
     )
+    return case, receivers
+
+
+def gaussian_hill(Y: Sequence[float], h: float, w: float, y0: float) -> List[float]:
+    """Ground elevation z_g(y) = h exp(-(y - y0)^2 / (2 w^2)) at the Y nodes."""
+    return [h * math.exp(-((y - y0) ** 2) / (2.0 * w * w)) for y in Y]
+
+
+def porous_hill(ni=128, nj=256, nk=96, layer=16, d=0.05, steps=4000, pml=20, seed=0, h=0.5, w=1.0,
+                sigma=2.0e5, porosity=0.3, tortuosity=1.8):
+    """The porous-ground domain of :func:`porous_ground` over an analytic
+    hill z_g(y) = h exp(-(y - y0)^2 / 2w^2) at mid-range (h = 0.5 m, w =
+    1 m): the air grid stretched vertically between the ground and the flat
+    top, the porous layer following the ground (terrain.dat). The source
+    height above the local ground is drawn from ``seed`` (uniform in
+    0.2-1 m); 8 receivers on a line 1 m above the local ground."""
+    import random
+
+    case, _ = porous_ground(ni=ni, nj=nj, nk=nk, layer=layer, d=d, steps=steps, pml=pml, seed=seed,
+                            sigma=sigma, porosity=porosity, tortuosity=tortuosity)
+    rng = random.Random(seed)
+    Y = case.Y
+    y0 = Y[nj // 2]
+    case.terrain = gaussian_hill(Y, h, w, y0)
+    zg = lambda y: h * math.exp(-((y - y0) ** 2) / (2.0 * w * w))  # noqa: E731
+    Xc = case.X[ni // 2]
+    # coordinates rounded to 1 um: input.txt lines stay inside the
+    # reference parser's 100-character comment skip
+    ys = round(Y[pml] + 10 * d + rng.uniform(0.0, 1.0) * 10 * d, 6)
+    case.source = (Xc, ys, round(zg(ys) + rng.uniform(0.2, 1.0), 6))
+    rec_y0 = ys + 1.0
+    ymax = Y[nj - pml - 2]
+    receivers = []
+    for r in range(8):
+        yr = round(min(rec_y0 + r * (ymax - rec_y0) / 7.0, ymax), 6)
+        receivers.append((Xc, yr, round(zg(yr) + 1.0, 6)))
+    case.receiver = receivers[0]
     return case, receivers
 
 

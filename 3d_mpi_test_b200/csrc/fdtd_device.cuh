@@ -66,6 +66,9 @@ struct Dev {
     // derivative factors x_over_X*rdx etc. (reference metric x scale);
     // the per-column arrays ayA / ayP are padded to NJP with zeros
     const R *axA, *ayA, *axP, *ayP, *azG;
+    // terrain-following grid (null on flat ground): z_over_Z*rdz and
+    // z_over_Y*rdz per (g, column), [NG][NJP]
+    const R *azT, *zyT;
 
     // air constants
     R dt, gP0dt, gdt, Aavdt, Aav, gP0;
@@ -234,6 +237,26 @@ __device__ __forceinline__ Arr<R, 1> el(const Arr<R, N>& a, int e) {
     return Arr<R, 1>{{a.e[e]}};
 }
 
+// -------------------------------------------------- terrain-following grid
+// Per-column factors of one plane on a grid stretched vertically under a
+// ground elevation z_g(Y) (extension of the reference's generic metric
+// form, df_over_var.cpp:5-9 with the cross term z_over_Y live; use sites
+// air.cpp:1476-2322, porous.cpp:58-143): z_over_Z * rdz and z_over_Y * rdz
+// per (plane, column), and the v at g + 1 the cross term of div u reads.
+// Without terrain (TER = false) az is the plane's 1D factor and zy is 0.
+template <typename R, int N>
+struct TerC {
+    Arr<R, N> az, zy, vk;
+};
+
+// the factors of N columns [jb, jb + N) at plane g (terrain domains)
+template <typename R, int N>
+__device__ __forceinline__ void ter_factors(const Dev<R>& d, int g, int jb, Arr<R, N>& az, Arr<R, N>& zy) {
+    const size_t o = static_cast<size_t>(g) * d.NJP + jb;
+    az = ldn<R, N>(d.azT + o);
+    zy = ldn<R, N>(d.zyT + o);
+}
+
 // -------------------------------------------------- pressure increment parts
 // PML part of the air pressure increment of N columns [jb, jb+N) of row i
 // (air::cal_fp, air.cpp:1953-2322): per active layer its sigma / beta terms
@@ -244,12 +267,13 @@ __device__ __forceinline__ Arr<R, 1> el(const Arr<R, N>& a, int e) {
 // adds exact zeros; their slab reads stay inside the padded slab row. The
 // reference multiplies every term by dt last; here dt (and gamma P0 or the
 // averaging factor) is folded into the layer coefficients first, which
-// changes only the last bits of the rounding.
-template <typename R, int N>
+// changes only the last bits of the rounding. TER: every Y derivative of a
+// slab also takes its z_over_Y part (the slab's Qv at k + 1).
+template <typename R, int N, bool TER = false>
 __device__ __forceinline__ void pml_dp_v(const Dev<R>& d, int i, int jb, int k, int xs, int ysp, int ysv, int zs,
-                                         R ax, const Arr<R, N>& ay, R az, const Arr<R, N>& gu, const Arr<R, N>& gv,
-                                         const Arr<R, N>& gw, const Arr<R, N>& pn, const PmlC<R>& X,
-                                         const PmlC<R>& Z, Arr<R, N>& dp) {
+                                         R ax, const Arr<R, N>& ay, const Arr<R, N>& az, const Arr<R, N>& zy,
+                                         const Arr<R, N>& gu, const Arr<R, N>& gv, const Arr<R, N>& gw,
+                                         const Arr<R, N>& pn, const PmlC<R>& X, const PmlC<R>& Z, Arr<R, N>& dp) {
     const R gP0 = d.gP0, dt = d.dt;
     const int NJ = d.NJ;
     const R xS = X.s * dt, xF = X.f * gP0 * dt, zS = Z.s * dt, zF = Z.f * gP0 * dt;
@@ -262,13 +286,16 @@ __device__ __forceinline__ void pml_dp_v(const Dev<R>& d, int i, int jb, int k, 
         const Arr<R, N> v0 = ldn<R, N>(S.rd[1] + q);
         const R vn = (jb + N <= NJ - 1) ? S.rd[1][q + N] : R(0);
         const Arr<R, N> w0 = ldn<R, N>(S.rd[2] + q), w1 = ldn<R, N>(S.rd[2] + q + S.ni * S.jp);
+        Arr<R, N> vk{};
+        if (TER) vk = ldn<R, N>(S.rd[1] + q + S.ni * S.jp);
         if (ysv | zs) QpX = ldn<R, N>(S.rd[3] + q);
 #pragma unroll
         for (int e = 0; e < N; ++e) {
             const R v1 = e + 1 < N ? v0.e[e + 1 < N ? e + 1 : 0] : vn;
             dQux.e[e] = ax * (u1.e[e] - u0.e[e]);
             dQvx.e[e] = ay.e[e] * (v1 - v0.e[e]);
-            dQwx.e[e] = az * (w1.e[e] - w0.e[e]);
+            if (TER) dQvx.e[e] += zy.e[e] * (vk.e[e] - v0.e[e]);
+            dQwx.e[e] = az.e[e] * (w1.e[e] - w0.e[e]);
             dp.e[e] += xF * gu.e[e] - xS * (pn.e[e] + gP0 * (dQvx.e[e] + dQwx.e[e]));
         }
     }
@@ -280,6 +307,8 @@ __device__ __forceinline__ void pml_dp_v(const Dev<R>& d, int i, int jb, int k, 
         const Arr<R, N> v0 = ldn<R, N>(S.rd[1] + q);
         const R vn = ((ysp >> (2 * (N - 1))) & 3) ? S.rd[1][q + N] : R(0);
         const Arr<R, N> w0 = ldn<R, N>(S.rd[2] + q), w1 = ldn<R, N>(S.rd[2] + q + S.ni * S.jp);
+        Arr<R, N> vk{};
+        if (TER) vk = ldn<R, N>(S.rd[1] + q + S.ni * S.jp);
         if (xs | zs) QpY = ldn<R, N>(S.rd[3] + q);
 #pragma unroll
         for (int e = 0; e < N; ++e) {
@@ -287,7 +316,8 @@ __device__ __forceinline__ void pml_dp_v(const Dev<R>& d, int i, int jb, int k, 
             const R v1 = e + 1 < N ? v0.e[e + 1 < N ? e + 1 : 0] : vn;
             const R dQuy = ax * (u1.e[e] - u0.e[e]);
             dQvy.e[e] = ay.e[e] * (v1 - v0.e[e]);
-            dQwy.e[e] = az * (w1.e[e] - w0.e[e]);
+            if (TER) dQvy.e[e] += zy.e[e] * (vk.e[e] - v0.e[e]);
+            dQwy.e[e] = az.e[e] * (w1.e[e] - w0.e[e]);
             yS.e[e] = Y[e].s * dt;
             dp.e[e] += (Y[e].f * gP0 * dt) * gv.e[e] - yS.e[e] * (pn.e[e] + gP0 * (dQuy + dQwy.e[e]));
             if (xs)
@@ -301,11 +331,14 @@ __device__ __forceinline__ void pml_dp_v(const Dev<R>& d, int i, int jb, int k, 
         const Arr<R, N> u0 = ldn<R, N>(S.rd[0] + q), u1 = ldn<R, N>(S.rd[0] + q + S.jp);
         const Arr<R, N> v0 = ldn<R, N>(S.rd[1] + q);
         const R vn = (jb + N <= NJ - 1) ? S.rd[1][q + N] : R(0);
+        Arr<R, N> vk{};
+        if (TER) vk = ldn<R, N>(S.rd[1] + q + S.ni * S.jp);
 #pragma unroll
         for (int e = 0; e < N; ++e) {
             const R v1 = e + 1 < N ? v0.e[e + 1 < N ? e + 1 : 0] : vn;
             const R dQuz = ax * (u1.e[e] - u0.e[e]);
-            const R dQvz = ay.e[e] * (v1 - v0.e[e]);
+            R dQvz = ay.e[e] * (v1 - v0.e[e]);
+            if (TER) dQvz += zy.e[e] * (vk.e[e] - v0.e[e]);
             dp.e[e] += zF * gw.e[e] - zS * (pn.e[e] + gP0 * (dQuz + dQvz));
             if (xs) dp.e[e] -= QpX.e[e] * (X.s * zS) + gP0 * ((X.g * zS) * dQux.e[e] + (Z.g * xS) * dQwx.e[e]);
             if (ysv)
@@ -316,14 +349,18 @@ __device__ __forceinline__ void pml_dp_v(const Dev<R>& d, int i, int jb, int k, 
 }
 
 // Mean-wind part of the air pressure increment at one node: one-sided
-// upwind advection of p and gamma p div U0 (air.cpp:1953-2322, wind branch).
-template <typename R>
-__device__ __forceinline__ void wind_dp(const Dev<R>& d, int j, int k, R ax, R ay, R az, R pn, R pim, R pjm, R pkm,
-                                        R& dp) {
+// upwind advection of p and gamma p div U0 (air.cpp:1953-2322, wind
+// branch). TER: the z advection coefficient takes V z_over_Y and dV/dY its
+// z_over_Y part (coef3 and Vav_over_Y of the reference's generic form).
+template <typename R, bool TER = false>
+__device__ __forceinline__ void wind_dp(const Dev<R>& d, int j, int k, R ax, R ay, R az, R zy, R pn, R pim, R pjm,
+                                        R pkm, R& dp) {
     const int wk = k * d.NJ + j, wS = d.NJ;
     const R U = ldg(d.Uw + wk), V = ldg(d.Vw + wk), W = ldg(d.Ww + wk);
-    dp += -(U * ax * d.dt) * (pn - pim) - (V * ay * d.dt) * (pn - pjm) - (W * az * d.dt) * (pn - pkm);
-    const R dVdY = ay * (ldg(d.Vw + wk + 1) - ldg(d.Vw + wk - 1)) * R(0.5);
+    const R c3 = TER ? (V * zy + W * az) * d.dt : W * az * d.dt;
+    dp += -(U * ax * d.dt) * (pn - pim) - (V * ay * d.dt) * (pn - pjm) - c3 * (pn - pkm);
+    R dVdY = ay * (ldg(d.Vw + wk + 1) - ldg(d.Vw + wk - 1)) * R(0.5);
+    if (TER) dVdY += zy * (ldg(d.Vw + wk + wS) - ldg(d.Vw + wk - wS)) * R(0.5);
     const R dWdZ = az * (ldg(d.Ww + wk + wS) - ldg(d.Ww + wk - wS)) * R(0.5);
     dp += -d.gdt * pn * (dVdY + dWdZ);
 }
@@ -335,6 +372,7 @@ __device__ __forceinline__ void wind_dp(const Dev<R>& d, int j, int k, R ax, R a
 //   u0 v0 w0 pn  the nodes' u, v, w, p_n
 //   ui vj wk     u(i+1), v(j+1), w(g+1)
 //   pim pjm pkm  p_n(i-1), p_n(j-1), p_n(g-1) (read with wind only)
+//   tc           terrain factors and v(g+1) (read with TER only)
 // Columns outside 1..NJ-2 (faces, row padding) get values the caller
 // discards; every read for them stays in bounds.
 // XF: the rarer features (porous inclusions, vectors with columns of both y
@@ -342,18 +380,21 @@ __device__ __forceinline__ void wind_dp(const Dev<R>& d, int j, int k, R ax, R a
 // domains that have none
 // PML: the PML terms are compiled in (a kernel built without them runs only
 // tiles that hold no PML node)
-template <typename R, bool WIND, int N, bool XF = true, bool PML = true>
+template <typename R, bool WIND, int N, bool XF = true, bool PML = true, bool TER = false>
 __device__ __forceinline__ Arr<R, N> p_vec(const Dev<R>& d, const PlaneC<R>& pc, const RowC<R>& rc, int i, int jb,
                                            const Arr<R, N>& ay, int ysp, const Arr<R, N>& u0, const Arr<R, N>& v0,
                                            const Arr<R, N>& w0, const Arr<R, N>& pn, const Arr<R, N>& ui,
                                            const Arr<R, N>& vj, const Arr<R, N>& wk, const Arr<R, N>& pim,
-                                           const Arr<R, N>& pjm, const Arr<R, N>& pkm) {
-    Arr<R, N> gu, gv, gw, out;
+                                           const Arr<R, N>& pjm, const Arr<R, N>& pkm,
+                                           const TerC<R, N>& tc = TerC<R, N>{}) {
+    Arr<R, N> gu, gv, gw, out, az;
 #pragma unroll
     for (int e = 0; e < N; ++e) {
+        az.e[e] = TER ? tc.az.e[e] : pc.az;
         gu.e[e] = rc.ax * (ui.e[e] - u0.e[e]);
         gv.e[e] = ay.e[e] * (vj.e[e] - v0.e[e]);
-        gw.e[e] = pc.az * (wk.e[e] - w0.e[e]);
+        if (TER) gv.e[e] += tc.zy.e[e] * (tc.vk.e[e] - v0.e[e]);
+        gw.e[e] = az.e[e] * (wk.e[e] - w0.e[e]);
     }
     if (pc.pore) {
 #pragma unroll
@@ -367,19 +408,21 @@ __device__ __forceinline__ Arr<R, N> p_vec(const Dev<R>& d, const PlaneC<R>& pc,
 #pragma unroll
         for (int e = 0; e < N; ++e)
             if (jb + e >= 1 && jb + e <= d.NJ - 2)
-                wind_dp(d, jb + e, pc.k, rc.ax, ay.e[e], pc.az, pn.e[e], pim.e[e], pjm.e[e], pkm.e[e], dp.e[e]);
+                wind_dp<R, TER>(d, jb + e, pc.k, rc.ax, ay.e[e], az.e[e], TER ? tc.zy.e[e] : R(0), pn.e[e], pim.e[e],
+                                pjm.e[e], pkm.e[e], dp.e[e]);
     }
     const int ysv = y_common<N>(ysp);
     if (PML && (rc.xs | ysv | pc.zs)) {
         if (!XF || ysv != 3) {
-            pml_dp_v<R, N>(d, i, jb, pc.k, rc.xs, ysp, ysv, pc.zs, rc.ax, ay, pc.az, gu, gv, gw, pn, rc.X, pc.Z, dp);
+            pml_dp_v<R, N, TER>(d, i, jb, pc.k, rc.xs, ysp, ysv, pc.zs, rc.ax, ay, az, tc.zy, gu, gv, gw, pn, rc.X,
+                                pc.Z, dp);
         } else {  // both y layers within N columns (very narrow grids): column by column
 #pragma unroll
             for (int e = 0; e < N; ++e) {
                 const int s = (ysp >> (2 * e)) & 3;
                 Arr<R, 1> dpe = el(dp, e);
-                pml_dp_v<R, 1>(d, i, jb + e, pc.k, rc.xs, s, s, pc.zs, rc.ax, el(ay, e), pc.az, el(gu, e), el(gv, e),
-                               el(gw, e), el(pn, e), rc.X, pc.Z, dpe);
+                pml_dp_v<R, 1, TER>(d, i, jb + e, pc.k, rc.xs, s, s, pc.zs, rc.ax, el(ay, e), el(az, e), el(tc.zy, e),
+                                    el(gu, e), el(gv, e), el(gw, e), el(pn, e), rc.X, pc.Z, dpe);
                 dp.e[e] = dpe.e[0];
             }
         }
@@ -404,15 +447,16 @@ __device__ __forceinline__ Arr<R, N> p_vec(const Dev<R>& d, const PlaneC<R>& pc,
 // pkm: the scheme's pressure at the nodes and at i-1, j-1, g-1. qp_old: the
 // slabs' Qp buffers still hold the values from before this step's pressure
 // update (single-pass form), so the advanced Qp is formed here as
-// Qp + dt * p, the expression of air::Update_PML_Qp.
-template <typename R, int N>
+// Qp + dt * p, the expression of air::Update_PML_Qp. TER: the Y derivative
+// of Qp takes its z_over_Y part.
+template <typename R, int N, bool TER = false>
 __device__ __forceinline__ void pml_dvel_v(const Dev<R>& d, int i, int jb, int k, int xs, int ysp, int ysv, int zs,
-                                           R ax, const Arr<R, N>& ay, R az, const Arr<R, N>& u0, const Arr<R, N>& v0,
-                                           const Arr<R, N>& w0, const Arr<R, N>& gpX, const Arr<R, N>& gpY,
-                                           const Arr<R, N>& gpZ, const Arr<R, N>& p0, const Arr<R, N>& pim,
-                                           const Arr<R, N>& pjm, const Arr<R, N>& pkm, bool qp_old,
-                                           const PmlC<R>& X, const PmlC<R>& Z, Arr<R, N>& du, Arr<R, N>& dv,
-                                           Arr<R, N>& dw) {
+                                           R ax, const Arr<R, N>& ay, const Arr<R, N>& az, const Arr<R, N>& zy,
+                                           const Arr<R, N>& u0, const Arr<R, N>& v0, const Arr<R, N>& w0,
+                                           const Arr<R, N>& gpX, const Arr<R, N>& gpY, const Arr<R, N>& gpZ,
+                                           const Arr<R, N>& p0, const Arr<R, N>& pim, const Arr<R, N>& pjm,
+                                           const Arr<R, N>& pkm, bool qp_old, const PmlC<R>& X, const PmlC<R>& Z,
+                                           Arr<R, N>& du, Arr<R, N>& dv, Arr<R, N>& dw) {
     const R A = d.Aav, dt = d.dt;
     const R xS = X.s * dt, zS = Z.s * dt;
     // backward differences of the slab's Qp advanced to this step
@@ -431,7 +475,8 @@ __device__ __forceinline__ void pml_dvel_v(const Dev<R>& d, int i, int jb, int k
             }
             bx.e[e] = ax * (a - b);
             by.e[e] = ay.e[e] * (a - c);
-            bz.e[e] = az * (a - f);
+            if (TER) by.e[e] += zy.e[e] * (a - f);
+            bz.e[e] = az.e[e] * (a - f);
         }
     };
     Arr<R, N> bxX{}, byX{}, bzX{}, bxY{}, byY{}, bzY{};
@@ -513,23 +558,32 @@ struct WindNb {
 
 // Mean-wind part of the air velocity increment at one node: forward-
 // difference advection (U0 . grad) u and the central-difference shear
-// u . grad U0 (air.cpp:1476-1949).
-template <typename R>
-__device__ __forceinline__ void wind_dvel(const Dev<R>& d, int j, int k, R ax, R ay, R az, R u0, R v0, R w0, R ui,
-                                          R uj, R uk, R vi, R vj, R vk, R wi, R wj, R wk, R& du, R& dv, R& dw) {
+// u . grad U0 (air.cpp:1476-1949). TER: the z advection coefficient takes
+// V z_over_Y and every d/dY of the wind its z_over_Y part.
+template <typename R, bool TER = false>
+__device__ __forceinline__ void wind_dvel(const Dev<R>& d, int j, int k, R ax, R ay, R az, R zy, R u0, R v0, R w0,
+                                          R ui, R uj, R uk, R vi, R vj, R vk, R wi, R wj, R wk, R& du, R& dv,
+                                          R& dw) {
     const int q = k * d.NJ + j, wS = d.NJ;
     const R U = ldg(d.Uw + q), V = ldg(d.Vw + q), W = ldg(d.Ww + q);
-    const R c1 = U * ax * d.dt, c2 = V * ay * d.dt, c3 = W * az * d.dt;
+    const R c1 = U * ax * d.dt, c2 = V * ay * d.dt, c3 = TER ? (V * zy + W * az) * d.dt : W * az * d.dt;
     du += -c1 * (ui - u0) - c2 * (uj - u0) - c3 * (uk - u0);
     dv += -c1 * (vi - v0) - c2 * (vj - v0) - c3 * (vk - v0);
     dw += -c1 * (wi - w0) - c2 * (wj - w0) - c3 * (wk - w0);
     const R h = R(0.5);
-    const R dUdY = ay * (ldg(d.Uw + q + 1) - ldg(d.Uw + q - 1)) * h;
-    const R dUdZ = az * (ldg(d.Uw + q + wS) - ldg(d.Uw + q - wS)) * h;
-    const R dVdY = ay * (ldg(d.Vw + q + 1) - ldg(d.Vw + q - 1)) * h;
-    const R dVdZ = az * (ldg(d.Vw + q + wS) - ldg(d.Vw + q - wS)) * h;
-    const R dWdY = ay * (ldg(d.Ww + q + 1) - ldg(d.Ww + q - 1)) * h;
-    const R dWdZ = az * (ldg(d.Ww + q + wS) - ldg(d.Ww + q - wS)) * h;
+    const R zU = ldg(d.Uw + q + wS) - ldg(d.Uw + q - wS), zV = ldg(d.Vw + q + wS) - ldg(d.Vw + q - wS),
+            zW = ldg(d.Ww + q + wS) - ldg(d.Ww + q - wS);
+    R dUdY = ay * (ldg(d.Uw + q + 1) - ldg(d.Uw + q - 1)) * h;
+    const R dUdZ = az * zU * h;
+    R dVdY = ay * (ldg(d.Vw + q + 1) - ldg(d.Vw + q - 1)) * h;
+    const R dVdZ = az * zV * h;
+    R dWdY = ay * (ldg(d.Ww + q + 1) - ldg(d.Ww + q - 1)) * h;
+    const R dWdZ = az * zW * h;
+    if (TER) {
+        dUdY += zy * zU * h;
+        dVdY += zy * zV * h;
+        dWdY += zy * zW * h;
+    }
     du += -(v0 * dUdY + w0 * dUdZ) * d.dt;
     dv += -(v0 * dVdY + w0 * dVdZ) * d.dt;
     dw += -(v0 * dWdY + w0 * dWdZ) * d.dt;
@@ -544,37 +598,43 @@ struct Vel {
 // the scheme prescribes (p_nn for FB_p_v). Air: air::cal_fuvw
 // (air.cpp:1476-1949); pore: porous::cal_fuvw (porous.cpp:58-104);
 // accumulation: calculation_2D::Cal_velocity (calculation_2D.cpp:548-579).
-// Column conventions as p_vec.
-template <typename R, bool WIND, int N, bool XF = true, bool PML = true>
+// Column conventions as p_vec; tc: terrain factors (TER only; its vk is
+// unused here).
+template <typename R, bool WIND, int N, bool XF = true, bool PML = true, bool TER = false>
 __device__ __forceinline__ Vel<R, N> vel_vec(const Dev<R>& d, const PlaneC<R>& pc, const RowC<R>& rc, int i, int jb,
                                              const Arr<R, N>& ay, int ysp, const Arr<R, N>& u0, const Arr<R, N>& v0,
                                              const Arr<R, N>& w0, const Arr<R, N>& p0, const Arr<R, N>& pim,
                                              const Arr<R, N>& pjm, const Arr<R, N>& pkm, const WindNb<R, N>& nb,
-                                             bool qp_old) {
-    const R ax = rc.ax, az = pc.az;
-    Arr<R, N> bpi, bpj, bpk;
+                                             bool qp_old, const TerC<R, N>& tc = TerC<R, N>{}) {
+    const R ax = rc.ax;
+    Arr<R, N> bpi, bpj, bpk, az;
 #pragma unroll
     for (int e = 0; e < N; ++e) {
+        az.e[e] = TER ? tc.az.e[e] : pc.az;
         bpi.e[e] = p0.e[e] - pim.e[e];
         bpj.e[e] = p0.e[e] - pjm.e[e];
         bpk.e[e] = p0.e[e] - pkm.e[e];
-    }
-    Vel<R, N> r;
-    if (pc.pore) {
-#pragma unroll
-        for (int e = 0; e < N; ++e) {
-            r.u.e[e] = u0.e[e] + (-d.pIBdtEff * (ax * bpi.e[e]) + u0.e[e] * d.pInvB - u0.e[e]);
-            r.v.e[e] = v0.e[e] + (-d.pIBdtEff * (ay.e[e] * bpj.e[e]) + v0.e[e] * d.pInvB - v0.e[e]);
-            r.w.e[e] = w0.e[e] + (-d.pIBdtEff * (az * bpk.e[e]) + w0.e[e] * d.pInvB - w0.e[e]);
-        }
-        return r;
     }
     Arr<R, N> gpX, gpY, gpZ, du, dv, dw;
 #pragma unroll
     for (int e = 0; e < N; ++e) {
         gpX.e[e] = ax * bpi.e[e];
         gpY.e[e] = ay.e[e] * bpj.e[e];
-        gpZ.e[e] = az * bpk.e[e];
+        if (TER) gpY.e[e] += tc.zy.e[e] * bpk.e[e];
+        gpZ.e[e] = az.e[e] * bpk.e[e];
+    }
+    Vel<R, N> r;
+    if (pc.pore) {
+#pragma unroll
+        for (int e = 0; e < N; ++e) {
+            r.u.e[e] = u0.e[e] + (-d.pIBdtEff * gpX.e[e] + u0.e[e] * d.pInvB - u0.e[e]);
+            r.v.e[e] = v0.e[e] + (-d.pIBdtEff * gpY.e[e] + v0.e[e] * d.pInvB - v0.e[e]);
+            r.w.e[e] = w0.e[e] + (-d.pIBdtEff * gpZ.e[e] + w0.e[e] * d.pInvB - w0.e[e]);
+        }
+        return r;
+    }
+#pragma unroll
+    for (int e = 0; e < N; ++e) {
         du.e[e] = -d.Aavdt * gpX.e[e];
         dv.e[e] = -d.Aavdt * gpY.e[e];
         dw.e[e] = -d.Aavdt * gpZ.e[e];
@@ -583,23 +643,23 @@ __device__ __forceinline__ Vel<R, N> vel_vec(const Dev<R>& d, const PlaneC<R>& p
 #pragma unroll
         for (int e = 0; e < N; ++e)
             if (jb + e >= 1 && jb + e <= d.NJ - 2)
-                wind_dvel(d, jb + e, pc.k, ax, ay.e[e], az, u0.e[e], v0.e[e], w0.e[e], nb.ui.e[e], nb.uj.e[e],
-                          nb.uk.e[e], nb.vi.e[e], nb.vj.e[e], nb.vk.e[e], nb.wi.e[e], nb.wj.e[e], nb.wk.e[e],
-                          du.e[e], dv.e[e], dw.e[e]);
+                wind_dvel<R, TER>(d, jb + e, pc.k, ax, ay.e[e], az.e[e], TER ? tc.zy.e[e] : R(0), u0.e[e], v0.e[e],
+                                  w0.e[e], nb.ui.e[e], nb.uj.e[e], nb.uk.e[e], nb.vi.e[e], nb.vj.e[e], nb.vk.e[e],
+                                  nb.wi.e[e], nb.wj.e[e], nb.wk.e[e], du.e[e], dv.e[e], dw.e[e]);
     }
     const int ysv = y_common<N>(ysp);
     if (PML && (rc.xs | ysv | pc.zs)) {
         if (!XF || ysv != 3) {
-            pml_dvel_v<R, N>(d, i, jb, pc.k, rc.xs, ysp, ysv, pc.zs, ax, ay, az, u0, v0, w0, gpX, gpY, gpZ, p0, pim,
-                             pjm, pkm, qp_old, rc.X, pc.Z, du, dv, dw);
+            pml_dvel_v<R, N, TER>(d, i, jb, pc.k, rc.xs, ysp, ysv, pc.zs, ax, ay, az, tc.zy, u0, v0, w0, gpX, gpY,
+                                  gpZ, p0, pim, pjm, pkm, qp_old, rc.X, pc.Z, du, dv, dw);
         } else {  // both y layers within N columns (very narrow grids): column by column
 #pragma unroll
             for (int e = 0; e < N; ++e) {
                 const int s = (ysp >> (2 * e)) & 3;
                 Arr<R, 1> due = el(du, e), dve = el(dv, e), dwe = el(dw, e);
-                pml_dvel_v<R, 1>(d, i, jb + e, pc.k, rc.xs, s, s, pc.zs, ax, el(ay, e), az, el(u0, e), el(v0, e),
-                                 el(w0, e), el(gpX, e), el(gpY, e), el(gpZ, e), el(p0, e), el(pim, e), el(pjm, e),
-                                 el(pkm, e), qp_old, rc.X, pc.Z, due, dve, dwe);
+                pml_dvel_v<R, 1, TER>(d, i, jb + e, pc.k, rc.xs, s, s, pc.zs, ax, el(ay, e), el(az, e), el(tc.zy, e),
+                                      el(u0, e), el(v0, e), el(w0, e), el(gpX, e), el(gpY, e), el(gpZ, e), el(p0, e),
+                                      el(pim, e), el(pjm, e), el(pkm, e), qp_old, rc.X, pc.Z, due, dve, dwe);
                 du.e[e] = due.e[0];
                 dv.e[e] = dve.e[0];
                 dw.e[e] = dwe.e[0];
@@ -629,7 +689,7 @@ __device__ __forceinline__ Vel<R, N> vel_vec(const Dev<R>& d, const PlaneC<R>& p
 
 // -------------------------------------------------- node-wise front ends
 // Pressure at an interior node with every operand read from global memory
-// (two-pass form).
+// (two-pass form; the terrain factors when the domain has them).
 template <typename R, bool WIND>
 __device__ R fresh_p(const Dev<R>& d, int i, int j, int g, bool y1_on) {
     using A = Arr<R, 1>;
@@ -645,6 +705,15 @@ __device__ R fresh_p(const Dev<R>& d, int i, int j, int g, bool y1_on) {
         pim.e[0] = P[c - si];
         pjm.e[0] = P[c - 1];
         pkm.e[0] = P[c - sg];
+    }
+    TerC<R, 1> tc{};
+    if (d.azT) {
+        ter_factors<R, 1>(d, g, j, tc.az, tc.zy);
+        tc.vk.e[0] = d.v_in[c + sg];
+        return p_vec<R, WIND, 1, true, true, true>(d, pc, rc, i, j, ay, ysp, A{{d.u_in[c]}}, A{{d.v_in[c]}},
+                                                   A{{d.w_in[c]}}, A{{P[c]}}, A{{d.u_in[c + si]}}, A{{d.v_in[c + 1]}},
+                                                   A{{d.w_in[c + sg]}}, pim, pjm, pkm, tc)
+            .e[0];
     }
     return p_vec<R, WIND, 1>(d, pc, rc, i, j, ay, ysp, A{{d.u_in[c]}}, A{{d.v_in[c]}}, A{{d.w_in[c]}}, A{{P[c]}},
                              A{{d.u_in[c + si]}}, A{{d.v_in[c + 1]}}, A{{d.w_in[c + sg]}}, pim, pjm, pkm)
@@ -667,6 +736,13 @@ __device__ Vel<R, 1> fresh_vel(const Dev<R>& d, int i, int j, int g, bool y1_on)
     if (WIND && !pc.pore)
         nb = {A{{d.u_in[c + si]}}, A{{d.u_in[c + 1]}}, A{{d.u_in[c + sg]}}, A{{d.v_in[c + si]}}, A{{d.v_in[c + 1]}},
               A{{d.v_in[c + sg]}}, A{{d.w_in[c + si]}}, A{{d.w_in[c + 1]}}, A{{d.w_in[c + sg]}}};
+    if (d.azT) {
+        TerC<R, 1> tc{};
+        ter_factors<R, 1>(d, g, j, tc.az, tc.zy);
+        return vel_vec<R, WIND, 1, true, true, true>(d, pc, rc, i, j, ay, ysp, A{{d.u_in[c]}}, A{{d.v_in[c]}},
+                                                     A{{d.w_in[c]}}, A{{p[c]}}, A{{p[c - si]}}, A{{p[c - 1]}},
+                                                     A{{p[c - sg]}}, nb, false, tc);
+    }
     return vel_vec<R, WIND, 1>(d, pc, rc, i, j, ay, ysp, A{{d.u_in[c]}}, A{{d.v_in[c]}}, A{{d.w_in[c]}}, A{{p[c]}},
                                A{{p[c - si]}}, A{{p[c - 1]}}, A{{p[c - sg]}}, nb, false);
 }

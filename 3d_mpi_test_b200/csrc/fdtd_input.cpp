@@ -172,6 +172,17 @@ std::string parse_reference_case(const std::string& dir, ReferenceInput& in) {
         e = read_axes(dir, "coordi_pore", in.pore_axes);
         if (!e.empty()) return e;
     }
+    // terrain-following grid: no counterpart in the reference (its cross
+    // metrics are fixed at zero, calculation_2D.cpp:102-104)
+    std::string tt;
+    if (slurp(dir + "/terrain.dat", tt)) {
+        Reader t{tt};
+        const int n = t.i();
+        if (t.fail || n != in.air.JMAX) return "terrain.dat must start with the Y node count of coordi_air2.dat";
+        in.terrain.resize(static_cast<size_t>(n));
+        for (double& v : in.terrain) v = t.d();
+        if (t.fail) return "malformed " + dir + "/terrain.dat";
+    }
     return "";
 }
 

@@ -55,6 +55,9 @@ struct ReferenceInput {
     double hill_box[6] = {0};
     AxisFile air, pore_axes;
     bool has_pore = false;
+    // terrain-following grid (extension, optional terrain.dat: the count of Y
+    // nodes, then the ground elevation at each); empty: flat ground
+    std::vector<double> terrain;
 };
 
 // Returns "" on success, otherwise a one-line error.

@@ -1,10 +1,10 @@
-// PML / face tile kernel (fdtd_tile_pml.cuh), float instantiations.
+// PML / face tile kernel (fdtd_tile_pml.cuh), float, flat ground.
 #include "fdtd_k_tile_pml_impl.cuh"
 
 namespace fdtd {
 
-template const void* tile_pml_kernel_ptr<float>(int, bool);
-template void run_tile_pml<float>(int, bool, dim3, dim3, size_t, cudaStream_t, const Dev<float>&, const TileMaps&,
-                                 const TileGeo&, const TileBox*, int);
+template const void* tile_pml_kernel_ptr<float, false>(int, bool);
+template void run_tile_pml<float, false>(int, bool, dim3, dim3, size_t, cudaStream_t, const Dev<float>&, const TileMaps&,
+                                     const TileGeo&, const TileBox*, int);
 
 }  // namespace fdtd

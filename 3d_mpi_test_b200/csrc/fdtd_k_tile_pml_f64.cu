@@ -1,10 +1,10 @@
-// PML / face tile kernel (fdtd_tile_pml.cuh), double instantiations.
+// PML / face tile kernel (fdtd_tile_pml.cuh), double, flat ground.
 #include "fdtd_k_tile_pml_impl.cuh"
 
 namespace fdtd {
 
-template const void* tile_pml_kernel_ptr<double>(int, bool);
-template void run_tile_pml<double>(int, bool, dim3, dim3, size_t, cudaStream_t, const Dev<double>&, const TileMaps&,
-                                 const TileGeo&, const TileBox*, int);
+template const void* tile_pml_kernel_ptr<double, false>(int, bool);
+template void run_tile_pml<double, false>(int, bool, dim3, dim3, size_t, cudaStream_t, const Dev<double>&, const TileMaps&,
+                                     const TileGeo&, const TileBox*, int);
 
 }  // namespace fdtd

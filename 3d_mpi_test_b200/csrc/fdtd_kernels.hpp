@@ -35,21 +35,28 @@ template <typename R>
 void run_march_batch(int VW, bool wind, bool xf, dim3 grd, dim3 blk, size_t smem, cudaStream_t s,
                      const BatchWork* work, const BatchEntry<R>* entries, int nm, int phase);
 
-// tiled kernel (fdtd_k_tile.cu); form 0: lean tiles, 1: full tiles,
-// 2: full tiles with the rarer features (inclusion mask, east TDBC,
-// vectors holding both y layers), 3 + LM: PML / face tiles with the
-// layers of set LM compiled in (bit 0 x, bit 1 y, bit 2 z)
+// tiled kernel; form 0: lean tiles, 1: full tiles, 2: full tiles with the
+// rarer features (inclusion mask, east TDBC, vectors holding both y
+// layers), 3 + LM: PML / face tiles with the layers of set LM compiled in
+// (bit 0 x, bit 1 y, bit 2 z); ter: terrain-following grid. Dispatch in
+// fdtd_k_tile.cu.
 template <typename R>
-const void* tile_kernel_ptr(int form, bool wind);
+const void* tile_kernel_ptr(int form, bool wind, bool ter);
 template <typename R>
-void run_tile(int form, bool wind, dim3 grd, dim3 blk, size_t smem, cudaStream_t s, const Dev<R>& d,
+void run_tile(int form, bool wind, bool ter, dim3 grd, dim3 blk, size_t smem, cudaStream_t s, const Dev<R>& d,
               const TileMaps& maps, const TileGeo& tg, const TileBox* work, int par);
 
-// PML / face tiles (fdtd_k_tile_pml_f32.cu, fdtd_k_tile_pml_f64.cu);
-// lm: the layer set
-template <typename R>
+// forms 0..2 (fdtd_k_tile_flat.cu, fdtd_k_tile_ter.cu)
+template <typename R, bool TER>
+const void* tile_base_ptr(int form, bool wind);
+template <typename R, bool TER>
+void run_tile_base(int form, bool wind, dim3 grd, dim3 blk, size_t smem, cudaStream_t s, const Dev<R>& d,
+                   const TileMaps& maps, const TileGeo& tg, const TileBox* work, int par);
+
+// PML / face tiles with layer set lm (fdtd_k_tile_pml_{f32,f64}{,_ter}.cu)
+template <typename R, bool TER>
 const void* tile_pml_kernel_ptr(int lm, bool wind);
-template <typename R>
+template <typename R, bool TER>
 void run_tile_pml(int lm, bool wind, dim3 grd, dim3 blk, size_t smem, cudaStream_t s, const Dev<R>& d,
                   const TileMaps& maps, const TileGeo& tg, const TileBox* work, int par);
 

@@ -200,7 +200,9 @@ class SolverImpl final : public SolverImplBase {
         // alternative. FB_v_p keeps the two passes.
         const int nvec = NJP_ / kVecMax;
         fused_ = in.scheme == FB_P_V;
-        old_ok_ = fused_ && nvec <= kMarchThreads && march_smem_bytes(make_tiling(2, 16, 1, kVecMax, 0)) <= kSmemMax;
+        // (the row marching kernel has no terrain-following form)
+        old_ok_ = fused_ && !terrain_ && nvec <= kMarchThreads &&
+                  march_smem_bytes(make_tiling(2, 16, 1, kVecMax, 0)) <= kSmemMax;
         if (old_ok_) {  // 4-row tiles where they fit shared memory, else 2-row
             const int TI = march_smem_bytes(make_tiling(4, 16, 256 / nvec, kVecMax, 0)) <= kSmemMax ? 4 : 2;
             set_tiling(TI, 16, 256, 0, 0);
@@ -301,6 +303,7 @@ class SolverImpl final : public SolverImplBase {
             gOff_ = 0;
             NG_ = air_.K;
         }
+        build_terrain();
         // device indexing of fields and PML slabs is 32-bit
         if (static_cast<double>(NG_) * NI_ * NJP_ >= 2147483647.0)
             fail(-2, "domain holds 2^31 or more nodes per field (32-bit device indexing)");
@@ -321,9 +324,62 @@ class SolverImpl final : public SolverImplBase {
         for (int k = 0; k < Kair_ && !wind_on_; ++k)
             for (int j = 0; j < NJ_ && !wind_on_; ++j) {
                 double U, V, W;
-                wind_at(in.velocity_method, in.velocity_coef, air_.Y[j], air_.Z[k], U, V, W);
+                wind_at(in.velocity_method, in.velocity_coef, air_.Y[j], wind_z(j, k), U, V, W);
                 if (U != 0.0 || V != 0.0 || W != 0.0) wind_on_ = true;
             }
+    }
+
+    // Terrain-following grid (no counterpart in the reference, whose cross
+    // metrics are fixed at zero, calculation_2D.cpp:102-104): the ground
+    // elevation z_g of every column, the air grid stretched vertically
+    // between the ground and its flat top H, Z(j,k) = Z[k] + z_g(j)(1 -
+    // Z[k]/H), the porous grid following the ground, Z(j,k) = Z[k] + z_g(j).
+    // The PML profiles stay on the file axes.
+    void build_terrain() {
+        terrain_ = !in.terrain.empty();
+        if (!terrain_) return;
+        if (mf_.Judge == 1) fail(-2, "a terrain-following grid does not run with the moving frame");
+        if (in.curve_judge != 0) fail(-2, "a terrain-following grid does not run with inclusions");
+        if (air_.Z[0] != 0.0) fail(-2, "a terrain-following grid needs the air axis to start at Z = 0");
+        if (porous_ && pore_.Z[pore_.K - 2] != 0.0)
+            fail(-2, "a terrain-following grid needs the porous axis to end one node above Z = 0");
+        Htop_ = air_.Z[Kair_ - 1];
+        zg_.assign(in.terrain.begin(), in.terrain.begin() + NJ_);
+        for (double z : zg_)
+            if (!(z < Htop_) || !std::isfinite(z)) fail(-2, "terrain reaches the top of the air grid");
+    }
+
+    // physical height of node (j, k) of the air (pore = false) or porous grid
+    double zh(bool pore, int j, int k) const {
+        const double z = pore ? pore_.Z[k] : air_.Z[k];
+        if (!terrain_) return z;
+        return pore ? z + zg_[j] : z + zg_[j] * (1.0 - z / Htop_);
+    }
+    // height above the local ground of air node (j, k): the wind profile's z
+    double wind_z(int j, int k) const { return terrain_ ? zh(false, j, k) - zg_[j] : air_.Z[k]; }
+
+    // per (g, column) z_over_Z * rdz and z_over_Y * rdz on the terrain grid,
+    // from central differences of the node heights (the reference's
+    // SetMovingFrame metrics, calculation_2D.cpp:416-433, with Z(j,k)):
+    // z_over_Z = X_x Y_y J = 1 / Z_z, z_over_Y = -X_x Z_y J = -Z_y / (Y_y Z_z)
+    void terrain_metrics(std::vector<double>& az, std::vector<double>& zy) const {
+        az.assign(static_cast<size_t>(NG_) * NJP_, 0.0);
+        zy.assign(static_cast<size_t>(NG_) * NJP_, 0.0);
+        for (int g = 0; g < NG_; ++g) {
+            const bool pore = g < gAir0_;
+            const Medium& m = pore ? pore_ : air_;
+            const int k = std::min(std::max(pore ? g : g - gOff_, 1), m.K - 2);
+            const double rdz = 1.0 / m.dz, rdy = 1.0 / m.dy;
+            for (int jj = 0; jj < NJP_; ++jj) {
+                const int j = std::min(std::max(jj, 1), NJ_ - 2);
+                const double Zz = (zh(pore, j, k + 1) - zh(pore, j, k - 1)) * rdz * 0.5;
+                const double Zy = (zh(pore, j + 1, k) - zh(pore, j - 1, k)) * rdy * 0.5;
+                const double Yy = (m.Y[j + 1] - m.Y[j - 1]) * rdy * 0.5;
+                const size_t o = static_cast<size_t>(g) * NJP_ + jj;
+                az[o] = rdz / Zz;
+                zy[o] = -Zy / (Yy * Zz) * rdz;
+            }
+        }
     }
 
     void build_pml_static() {
@@ -530,6 +586,10 @@ class SolverImpl final : public SolverImplBase {
         d_axA_ = track(dalloc<R>(NI_)); d_ayA_ = track(dalloc<R>(NJP_));
         d_axP_ = track(dalloc<R>(NI_)); d_ayP_ = track(dalloc<R>(NJP_));
         d_azG_ = track(dalloc<R>(NG_));
+        if (terrain_) {
+            d_azT_ = track(dalloc<R>(static_cast<size_t>(NG_) * NJP_));
+            d_zyT_ = track(dalloc<R>(static_cast<size_t>(NG_) * NJP_));
+        }
         for (int q = 0; q < 3; ++q) {
             d_sx_[q] = track(dalloc<R>(NI_));
             d_sy_[q] = track(dalloc<R>(NJ_));
@@ -555,6 +615,12 @@ class SolverImpl final : public SolverImplBase {
         std::vector<double> az(NG_, 0.0);
         for (int g = 0; g < NG_; ++g) az[g] = (g < gAir0_) ? pore_.fz[g] : air_.fz[g - gOff_];
         upload(d_azG_, az);
+        if (terrain_) {
+            std::vector<double> azt, zyt;
+            terrain_metrics(azt, zyt);
+            upload(d_azT_, azt);
+            upload(d_zyT_, zyt);
+        }
     }
 
     void upload(R* dst, const std::vector<double>& src) {
@@ -596,7 +662,7 @@ class SolverImpl final : public SolverImplBase {
             for (int k = 0; k < Kair_; ++k)
                 for (int j = 0; j < NJ_; ++j) {
                     const size_t q = static_cast<size_t>(k) * NJ_ + j;
-                    wind_at(in.velocity_method, in.velocity_coef, air_.Y[j], air_.Z[k] - 0.0, U[q], V[q], Wv[q]);
+                    wind_at(in.velocity_method, in.velocity_coef, air_.Y[j], wind_z(j, k), U[q], V[q], Wv[q]);
                 }
             upload(d_Uw_, U); upload(d_Vw_, V); upload(d_Ww_, Wv);
         }
@@ -640,7 +706,7 @@ class SolverImpl final : public SolverImplBase {
                 for (int j = NN; j < ijkmax_ && j - NN < NJ_; j++)
                     if (ry - N * Yf - Y[j - NN] <= in.dy / 8.0) { jj = j; break; }
                 for (int k = 0; k < Kair_; k++)
-                    if (rz - Z[k] <= in.dz / 8.0) { kk = k; found_k = true; break; }
+                    if (rz - (terrain_ ? zh(false, jj, k) : Z[k]) <= in.dz / 8.0) { kk = k; found_k = true; break; }
             }
             if (!found_k) ii = jj = kk = 0;
             if (ii == 0 && jj == 0 && kk == 0) ii = jj = kk = 1;
@@ -680,7 +746,8 @@ class SolverImpl final : public SolverImplBase {
             const int k = pore ? g : g - gOff_;
             for (int i = 0; i < NI_; ++i)
                 for (int j = 0; j < NJ_; ++j) {
-                    const double x = m.X[i] - in.source[0], y = m.axY[j] - in.source[1], zz = m.Z[k] - in.source[2];
+                    const double x = m.X[i] - in.source[0], y = m.axY[j] - in.source[1],
+                                 zz = zh(pore, j, k) - in.source[2];
                     const double rr = std::sqrt(std::pow(x, 2) + std::pow(y, 2) + std::pow(zz, 2));
                     p[(static_cast<size_t>(g) * NI_ + i) * NJP_ + j] = static_cast<R>(1.0 * std::exp(-gc * rr * rr));
                 }
@@ -730,6 +797,8 @@ class SolverImpl final : public SolverImplBase {
             d.u_out = F_[nw][0]; d.v_out = F_[nw][1]; d.w_out = F_[nw][2];
         }
         d.axA = d_axA_; d.ayA = d_ayA_; d.axP = d_axP_; d.ayP = d_ayP_; d.azG = d_azG_;
+        d.azT = terrain_ ? d_azT_ : nullptr;
+        d.zyT = terrain_ ? d_zyT_ : nullptr;
         const double dt = in.dt, gP0 = in.gamma * in.P0;
         d.dt = R(dt); d.gP0dt = R(in.gamma * in.P0 * dt); d.gdt = R(in.gamma * dt);
         d.Aavdt = R(in.Aav * dt); d.Aav = R(in.Aav); d.gP0 = R(gP0);
@@ -1213,6 +1282,7 @@ class SolverImpl final : public SolverImplBase {
     // file; format 1 a binary file: "FDTDCNT1", int32 zone count, then per
     // zone int32 I J K and float64 X[I], Y[J], Z[K], P[K][J][I].
     void write_contour(const std::string& path, int format) override {
+        if (terrain_) fail(-2, "contour output lists one height per grid level; a terrain-following grid has none");
         FDTD_CK(cudaSetDevice(device_));
         if (format != 0 && format != 1) fail(-5, "contour format must be 0 (Tecplot ASCII) or 1 (binary)");
         struct Zone {
@@ -1312,7 +1382,7 @@ class SolverImpl final : public SolverImplBase {
                 for (int j = 0; j < NJ_; ++j)
                     for (int k = 0; k < Kair_; ++k) {
                         double U = 0, V = 0, W = 0;
-                        if (wind_on_) wind_at(in.velocity_method, in.velocity_coef, air_.Y[j], air_.Z[k], U, V, W);
+                        if (wind_on_) wind_at(in.velocity_method, in.velocity_coef, air_.Y[j], wind_z(j, k), U, V, W);
                         put(U); put(V); put(W);
                     }
             for (int sl = 0; sl < 6; ++sl) {
@@ -1491,6 +1561,7 @@ class SolverImpl final : public SolverImplBase {
     void set_tiling_api(int TI, int GC, int nt, int vw, int stages) override {
         FDTD_CK(cudaSetDevice(device_));
         if (!fused_) fail(-2, "tiling applies to the fused FB_p_v pass only");
+        if (terrain_) fail(-2, "the row marching kernel has no terrain-following form");
         if (!old_ok_) fail(-2, "rows too wide for the row marching kernel");
         set_tiling(TI, GC, nt, vw, stages);
         tile_on_ = false;  // the row marching kernel runs from now on
@@ -1690,7 +1761,7 @@ class SolverImpl final : public SolverImplBase {
         if (big) {
             for (bool w : {false, true})
                 for (int f = 0; f < 3 + 8; ++f)
-                    FDTD_CK(cudaFuncSetAttribute(tile_kernel_ptr<R>(f, w), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                    FDTD_CK(cudaFuncSetAttribute(tile_kernel_ptr<R>(f, w, terrain_), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                  static_cast<int>(kSmemMax)));
         }
         if (!sdy_.empty()) update_xf();  // before the first frame upload, which sets it
@@ -1732,7 +1803,8 @@ class SolverImpl final : public SolverImplBase {
         const Dev<R> d = params_fused(par);
         const dim3 grd(static_cast<unsigned>(ntile_[k])), blk(static_cast<unsigned>(tthr_[k]));
         const int code = par | (k == book_kind() ? 2 : 0);
-        run_tile<R>(form_of(k), wind_on_, grd, blk, tsmem_[k], s, d, tmaps_[k][par], tgeo_[k], d_tiles_ + toff_[k], code);
+        run_tile<R>(form_of(k), wind_on_, terrain_, grd, blk, tsmem_[k], s, d, tmaps_[k][par], tgeo_[k],
+                    d_tiles_ + toff_[k], code);
         FDTD_CK(cudaGetLastError());
         ++launches_;
     }
@@ -1987,6 +2059,11 @@ class SolverImpl final : public SolverImplBase {
     R* F_[2][4]{};
     R* Q_[6][2][4]{};
     R *d_axA_ = nullptr, *d_ayA_ = nullptr, *d_axP_ = nullptr, *d_ayP_ = nullptr, *d_azG_ = nullptr;
+    // terrain-following grid: elevation per column, air top, per (g, column) factors
+    bool terrain_ = false;
+    std::vector<double> zg_;
+    double Htop_ = 0.0;
+    R *d_azT_ = nullptr, *d_zyT_ = nullptr;
     R *d_sx_[3]{}, *d_sy_[3]{}, *d_sz_[3]{};
     int8_t *d_sdx_ = nullptr, *d_sdy_ = nullptr, *d_sdz_ = nullptr, *d_mask_ = nullptr;
     R *d_Uw_ = nullptr, *d_Vw_ = nullptr, *d_Ww_ = nullptr;
@@ -2262,7 +2339,9 @@ class EnsembleImpl final : public EnsembleImplBase {
         for (SolverImpl<R>* m : mem_) v.push_back(m->batch_view());
         if (mode_ == 0)
             for (const auto& m : v)
-                if (!m.old_ok) fail(-2, "a member's rows are too wide for the batched marching kernel (use mode 1)");
+                if (!m.old_ok)
+                    fail(-2, "a member's rows are too wide for the batched marching kernel, or its grid follows "
+                             "terrain (use mode 1)");
         // block size class: 64-thread steps, so narrow (2D) members do not
         // share a launch with 256-thread blocks
         auto key_of = [&](size_t i) {

@@ -80,7 +80,8 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
         : "memory");
 }
 
-template <typename R, bool WIND, int VW, bool FULL, bool XF>
+// TER: terrain-following grid (per-column z_over_Z and z_over_Y factors)
+template <typename R, bool WIND, int VW, bool FULL, bool XF, bool TER = false>
 __global__ void __launch_bounds__(kTileMaxThreads)
     k_tile(const __grid_constant__ Dev<R> d, const __grid_constant__ TileMaps maps, const TileGeo tg,
            const TileBox* __restrict__ work, int par) {
@@ -202,9 +203,12 @@ __global__ void __launch_bounds__(kTileMaxThreads)
         rc.inmask = pc.inmask && row_in_mask;
         Arr<R, V> u0{}, v0{}, w0{}, pnew{}, ui{}, wk{};
         R vn = R(0);
+        TerC<R, V> tc{};
+        if (TER && active) ter_factors<R, V>(d, g, jb, tc.az, tc.zy);
         // ---- new pressure of the tile and its halos at plane g
         if (active) {
             const R *U = fld(sg, 0) + so, *Vf = fld(sg, 1) + so, *Wf = fld(sg, 2) + so, *P = fld(sg, 3) + so;
+            if (TER) tc.vk = ldn<R, V>(fld(sn, 1) + so);
             u0 = ldn<R, V>(U);
             v0 = ldn<R, V>(Vf);
             w0 = ldn<R, V>(Wf);
@@ -222,7 +226,8 @@ __global__ void __launch_bounds__(kTileMaxThreads)
 #pragma unroll
                 for (int e = 0; e < V; ++e) pjm.e[e] = e > 0 ? pn.e[e > 0 ? e - 1 : 0] : pj0;
             }
-            pnew = p_vec<R, WIND, V, XF, FULL>(d, pc, rc, ic, jb, ay, ys, u0, v0, w0, pn, ui, vj, wk, pim, pjm, pkm);
+            pnew = p_vec<R, WIND, V, XF, FULL, TER>(d, pc, rc, ic, jb, ay, ys, u0, v0, w0, pn, ui, vj, wk, pim, pjm,
+                                                    pkm, tc);
             if (FULL) {  // west face copies column 1; the east face is extrapolated where it is used
 #pragma unroll
                 for (int e = 0; e < V; ++e)
@@ -264,8 +269,8 @@ __global__ void __launch_bounds__(kTileMaxThreads)
                     nb.wj.e[e] = e + 1 < V ? w0.e[e1] : wn;
                 }
             }
-            const Vel<R, V> vel =
-                vel_vec<R, WIND, V, XF, FULL>(d, pc, rc, ic, jb, ay, ys, u0, v0, w0, pnew, Pi, Pj, pprev, nb, true);
+            const Vel<R, V> vel = vel_vec<R, WIND, V, XF, FULL, TER>(d, pc, rc, ic, jb, ay, ys, u0, v0, w0, pnew, Pi,
+                                                                      Pj, pprev, nb, true, tc);
             const size_t go = (static_cast<size_t>(g) * NI + i) * d.NJP + jb;
             if (!FULL) {
                 stn<R, V>(d.p_out + go, pnew);
@@ -327,9 +332,12 @@ __global__ void __launch_bounds__(kTileMaxThreads)
                                    A{{Vn[0]}},  A{{Wf[SP]}}, A{{Wf[1]}}, A{{Wn[0]}}};
                         }
                         const R ays = ldg((pc.pore ? d.ayP : d.ayA) + NJ - 2);
-                        const Vel<R, 1> s = vel_vec<R, WIND, 1, XF, FULL>(
+                        TerC<R, 1> tcs{};
+                        if (TER) ter_factors<R, 1>(d, g, NJ - 2, tcs.az, tcs.zy);
+                        const Vel<R, 1> s = vel_vec<R, WIND, 1, XF, FULL, TER>(
                             d, pc, rc, ic, NJ - 2, A{{ays}}, pc.pore ? 0 : ysm1, A{{U[0]}}, A{{Vf[0]}}, A{{Wf[0]}},
-                            A{{Pb[po - 1]}}, A{{Pb[poi - 1]}}, A{{Pb[po - 2]}}, A{{pslot(g - 1)[po - 1]}}, nbs, true);
+                            A{{Pb[po - 1]}}, A{{Pb[poi - 1]}}, A{{Pb[po - 2]}}, A{{pslot(g - 1)[po - 1]}}, nbs, true,
+                            tcs);
                         fu.e[0] = s.u.e[0];
                         fw.e[0] = s.w.e[0];
                     }

@@ -37,14 +37,16 @@ enum : int { kLmX = 1, kLmY = 2, kLmZ = 4 };
 template <typename R, int V>
 struct SlabVals {
     Arr<R, V> u0, u1, v0, w0, w1, p0, pi, pk;  // Qu, Qu(i+1), Qv, Qw, Qw(k+1), Qp, Qp(i-1), Qp(k-1)
+    Arr<R, V> vk;                               // Qv(k+1) (terrain: the z_over_Y part of dQv/dY)
     R vn, pj;                                   // Qv(j+V), Qp(j-1)
 };
 
 // Loads the words of layer axis AX (0 x, 1 y, 2 z) that a node in the
 // layer reads; CORNER: another layer is compiled in (corner products need
-// more words); vel: the thread also computes the node's velocity; vn_ok:
-// column jb+V may be read.
-template <typename R, int V, int AX, bool CORNER>
+// more words); TER: terrain-following grid (every Y derivative of a slab
+// also differences it along k); vel: the thread also computes the node's
+// velocity; vn_ok: column jb+V may be read.
+template <typename R, int V, int AX, bool CORNER, bool TER>
 __device__ __forceinline__ void slab_load(const Slab<R>& S, int q, int jb, bool vel, bool vn_ok, SlabVals<R, V>& s) {
     const int si = S.jp, sk = S.ni * S.jp;
     s.u0 = ldn<R, V>(S.rd[0] + q);
@@ -54,10 +56,11 @@ __device__ __forceinline__ void slab_load(const Slab<R>& S, int q, int jb, bool 
     if (AX != 0 || CORNER) s.u1 = ldn<R, V>(S.rd[0] + q + si);
     if (AX != 1 || CORNER) s.vn = vn_ok ? S.rd[1][q + V] : R(0);
     if (AX != 2) s.w1 = ldn<R, V>(S.rd[2] + q + sk);
+    if (TER && (AX != 1 || CORNER)) s.vk = ldn<R, V>(S.rd[1] + q + sk);
     if (vel) {
         if (AX != 0 || CORNER) s.pi = ldn<R, V>(S.rd[3] + q - si);
         if (AX != 1 || CORNER) s.pj = jb > S.ja ? S.rd[3][q - 1] : R(0);
-        if (AX != 2) s.pk = ldn<R, V>(S.rd[3] + q - sk);
+        if (AX != 2 || TER) s.pk = ldn<R, V>(S.rd[3] + q - sk);
     }
 }
 
@@ -82,7 +85,8 @@ __device__ __forceinline__ void slab_store(const Slab<R>& S, int q, int emask, R
     stn<R, V>(S.wr[3] + q, f);
 }
 
-template <typename R, bool WIND, int LM>
+// TER: terrain-following grid (per-column z_over_Z and z_over_Y factors)
+template <typename R, bool WIND, int LM, bool TER = false>
 __global__ void __launch_bounds__(kTileMaxThreads)
     k_tile_pml(const __grid_constant__ Dev<R> d, const __grid_constant__ TileMaps maps, const TileGeo tg,
                const TileBox* __restrict__ work, int par) {
@@ -212,13 +216,21 @@ __global__ void __launch_bounds__(kTileMaxThreads)
         const int yl = HY && !pore ? ysv : 0;
         const int zl = HZ && !pore ? pc.zs : 0;
         const PmlC<R> Z = pc.Z;
+        // per-column factors of this plane: z_over_Z * rdz (and on a
+        // terrain-following grid z_over_Y * rdz)
+        Arr<R, V> az, zy{};
+        if (TER && active) ter_factors<R, V>(d, g, jb, az, zy);
+        if (!TER) {
+#pragma unroll
+            for (int e = 0; e < V; ++e) az.e[e] = pc.az;
+        }
         // the slab words of the plane, ahead of the staged fields
         SlabVals<R, V> sx{}, sy{}, sz{};
-        if (HX && xl) slab_load<R, V, 0, CX>(d.sl[xl - 1], d.sl[xl - 1].q(ic, jb, k), jb, vel, vn_ok, sx);
+        if (HX && xl) slab_load<R, V, 0, CX, TER>(d.sl[xl - 1], d.sl[xl - 1].q(ic, jb, k), jb, vel, vn_ok, sx);
         if (HY && yl)  // Qv(j+V) of a y slab only where the vector's last column is in the layer
-            slab_load<R, V, 1, CY>(d.sl[yl + 1], d.sl[yl + 1].q(ic, jb, k), jb, vel,
+            slab_load<R, V, 1, CY, TER>(d.sl[yl + 1], d.sl[yl + 1].q(ic, jb, k), jb, vel,
                                    vn_ok && ((ysp >> (2 * (V - 1))) & 3) != 0, sy);
-        if (HZ && zl) slab_load<R, V, 2, CZ>(d.sl[zl + 3], d.sl[zl + 3].q(ic, jb, k), jb, vel, vn_ok, sz);
+        if (HZ && zl) slab_load<R, V, 2, CZ, TER>(d.sl[zl + 3], d.sl[zl + 3].q(ic, jb, k), jb, vel, vn_ok, sz);
         if (g == first)
             for (int x = plo; x <= g + 1; ++x) wait_plane(x);
         else
@@ -236,12 +248,15 @@ __global__ void __launch_bounds__(kTileMaxThreads)
             ui = ldn<R, V>(U + SP);
             wk = ldn<R, V>(fld(sn, 2) + so);
             vn = Vf[V];
+            Arr<R, V> vk{};
+            if (TER) vk = ldn<R, V>(fld(sn, 1) + so);
 #pragma unroll
             for (int e = 0; e < V; ++e) {
                 const R vj = e + 1 < V ? v0.e[e + 1 < V ? e + 1 : 0] : vn;
                 gu.e[e] = ax * (ui.e[e] - u0.e[e]);
                 gv.e[e] = ay.e[e] * (vj - v0.e[e]);
-                gw.e[e] = pc.az * (wk.e[e] - w0.e[e]);
+                if (TER) gv.e[e] += zy.e[e] * (vk.e[e] - v0.e[e]);
+                gw.e[e] = az.e[e] * (wk.e[e] - w0.e[e]);
             }
             Arr<R, V> dp;
             if (pore) {
@@ -256,8 +271,8 @@ __global__ void __launch_bounds__(kTileMaxThreads)
 #pragma unroll
                     for (int e = 0; e < V; ++e)
                         if (jb + e >= 1 && jb + e <= NJ - 2)
-                            wind_dp(d, jb + e, k, ax, ay.e[e], pc.az, pn.e[e], pim.e[e],
-                                    e > 0 ? pn.e[e > 0 ? e - 1 : 0] : pj0, pkm.e[e], dp.e[e]);
+                            wind_dp<R, TER>(d, jb + e, k, ax, ay.e[e], az.e[e], zy.e[e], pn.e[e], pim.e[e],
+                                            e > 0 ? pn.e[e > 0 ? e - 1 : 0] : pj0, pkm.e[e], dp.e[e]);
                 }
                 // PML terms in the order of pml_dp_v: x, y (with x-y
                 // corners), z (with x-z and y-z corners)
@@ -270,7 +285,8 @@ __global__ void __launch_bounds__(kTileMaxThreads)
                         const R v1 = e + 1 < V ? sx.v0.e[e + 1 < V ? e + 1 : 0] : sx.vn;
                         if (CX) dQux.e[e] = ax * (sx.u1.e[e] - sx.u0.e[e]);
                         dQvx.e[e] = ay.e[e] * (v1 - sx.v0.e[e]);
-                        dQwx.e[e] = pc.az * (sx.w1.e[e] - sx.w0.e[e]);
+                        if (TER) dQvx.e[e] += zy.e[e] * (sx.vk.e[e] - sx.v0.e[e]);
+                        dQwx.e[e] = az.e[e] * (sx.w1.e[e] - sx.w0.e[e]);
                         dp.e[e] += xF * gu.e[e] - xS * (pn.e[e] + gP0 * (dQvx.e[e] + dQwx.e[e]));
                     }
                 }
@@ -279,8 +295,11 @@ __global__ void __launch_bounds__(kTileMaxThreads)
                     for (int e = 0; e < V; ++e) {
                         const R v1 = e + 1 < V ? sy.v0.e[e + 1 < V ? e + 1 : 0] : sy.vn;
                         const R dQuy = ax * (sy.u1.e[e] - sy.u0.e[e]);
-                        if (CY) dQvy.e[e] = ay.e[e] * (v1 - sy.v0.e[e]);
-                        dQwy.e[e] = pc.az * (sy.w1.e[e] - sy.w0.e[e]);
+                        if (CY) {
+                            dQvy.e[e] = ay.e[e] * (v1 - sy.v0.e[e]);
+                            if (TER) dQvy.e[e] += zy.e[e] * (sy.vk.e[e] - sy.v0.e[e]);
+                        }
+                        dQwy.e[e] = az.e[e] * (sy.w1.e[e] - sy.w0.e[e]);
                         dp.e[e] += (yF.e[e] * gP0 * dt) * gv.e[e] - yS.e[e] * (pn.e[e] + gP0 * (dQuy + dQwy.e[e]));
                         if (HX && xl)
                             dp.e[e] -= sx.p0.e[e] * (X.s * yS.e[e]) +
@@ -293,7 +312,8 @@ __global__ void __launch_bounds__(kTileMaxThreads)
                     for (int e = 0; e < V; ++e) {
                         const R v1 = e + 1 < V ? sz.v0.e[e + 1 < V ? e + 1 : 0] : sz.vn;
                         const R dQuz = ax * (sz.u1.e[e] - sz.u0.e[e]);
-                        const R dQvz = ay.e[e] * (v1 - sz.v0.e[e]);
+                        R dQvz = ay.e[e] * (v1 - sz.v0.e[e]);
+                        if (TER) dQvz += zy.e[e] * (sz.vk.e[e] - sz.v0.e[e]);
                         dp.e[e] += zF * gw.e[e] - zS * (pn.e[e] + gP0 * (dQuz + dQvz));
                         if (HX && xl)
                             dp.e[e] -= sx.p0.e[e] * (X.s * zS) +
@@ -328,7 +348,8 @@ __global__ void __launch_bounds__(kTileMaxThreads)
                 Pj.e[e] = e > 0 ? pnew.e[e > 0 ? e - 1 : 0] : Pj0;
                 gpX.e[e] = ax * (pnew.e[e] - Pi.e[e]);
                 gpY.e[e] = ay.e[e] * (pnew.e[e] - Pj.e[e]);
-                gpZ.e[e] = pc.az * (pnew.e[e] - pprev.e[e]);
+                if (TER) gpY.e[e] += zy.e[e] * (pnew.e[e] - pprev.e[e]);
+                gpZ.e[e] = az.e[e] * (pnew.e[e] - pprev.e[e]);
             }
             if (pore) {
 #pragma unroll
@@ -354,7 +375,7 @@ __global__ void __launch_bounds__(kTileMaxThreads)
                     for (int e = 0; e < V; ++e) {
                         const int e1 = e + 1 < V ? e + 1 : 0;
                         if (jb + e >= 1 && jb + e <= NJ - 2)
-                            wind_dvel(d, jb + e, k, ax, ay.e[e], pc.az, u0.e[e], v0.e[e], w0.e[e], ui.e[e],
+                            wind_dvel<R, TER>(d, jb + e, k, ax, ay.e[e], az.e[e], zy.e[e], u0.e[e], v0.e[e], w0.e[e], ui.e[e],
                                       e + 1 < V ? u0.e[e1] : un, uk.e[e], vi.e[e], e + 1 < V ? v0.e[e1] : vv,
                                       vk.e[e], wi.e[e], e + 1 < V ? w0.e[e1] : wn, wk.e[e], du.e[e], dv.e[e],
                                       dw.e[e]);
@@ -371,8 +392,10 @@ __global__ void __launch_bounds__(kTileMaxThreads)
                     if (HX && xl) {
                         const R a = sx.p0.e[e] + dp0;
                         if (CX) bxX = ax * (a - (sx.pi.e[e] + dpi));
+                        const R fk = sx.pk.e[e] + dpk;
                         byX = ay.e[e] * (a - ((e > 0 ? sx.p0.e[e > 0 ? e - 1 : 0] : sx.pj) + dpj));
-                        bzX = pc.az * (a - (sx.pk.e[e] + dpk));
+                        if (TER) byX += zy.e[e] * (a - fk);
+                        bzX = az.e[e] * (a - fk);
                         du.e[e] += (X.f * A * dt) * gpX.e[e] - xS * u0.e[e];
                         dv.e[e] -= xS * (v0.e[e] + A * byX);
                         dw.e[e] -= xS * (w0.e[e] + A * bzX);
@@ -381,8 +404,12 @@ __global__ void __launch_bounds__(kTileMaxThreads)
                     if (HY && yl) {
                         const R a = sy.p0.e[e] + dp0;
                         const R bxY = ax * (a - (sy.pi.e[e] + dpi));
-                        if (CY) byY = ay.e[e] * (a - ((e > 0 ? sy.p0.e[e > 0 ? e - 1 : 0] : sy.pj) + dpj));
-                        bzY = pc.az * (a - (sy.pk.e[e] + dpk));
+                        const R fk = sy.pk.e[e] + dpk;
+                        if (CY) {
+                            byY = ay.e[e] * (a - ((e > 0 ? sy.p0.e[e > 0 ? e - 1 : 0] : sy.pj) + dpj));
+                            if (TER) byY += zy.e[e] * (a - fk);
+                        }
+                        bzY = az.e[e] * (a - fk);
                         du.e[e] -= yS.e[e] * (u0.e[e] + A * bxY);
                         dv.e[e] += (yF.e[e] * A * dt) * gpY.e[e] - yS.e[e] * v0.e[e];
                         dw.e[e] -= yS.e[e] * (w0.e[e] + A * bzY);
@@ -396,7 +423,8 @@ __global__ void __launch_bounds__(kTileMaxThreads)
                     if (HZ && zl) {
                         const R a = sz.p0.e[e] + dp0;
                         const R bxZ = ax * (a - (sz.pi.e[e] + dpi));
-                        const R byZ = ay.e[e] * (a - ((e > 0 ? sz.p0.e[e > 0 ? e - 1 : 0] : sz.pj) + dpj));
+                        R byZ = ay.e[e] * (a - ((e > 0 ? sz.p0.e[e > 0 ? e - 1 : 0] : sz.pj) + dpj));
+                        if (TER) byZ += zy.e[e] * (a - (sz.pk.e[e] + dpk));
                         du.e[e] -= zS * (u0.e[e] + A * bxZ);
                         dv.e[e] -= zS * (v0.e[e] + A * byZ);
                         dw.e[e] += (Z.f * A * dt) * gpZ.e[e] - zS * w0.e[e];

@@ -1,11 +1,15 @@
 #!/usr/bin/env python
 """Throughput benchmark of the B200 FDTD time-marching path.
 
-Workload (N=1): porous ground under air, 256 (range, Y/j) x 128 (X/i) x 96
-(Z/k) air nodes over a 16-cell Zwikker-Kosten layer (sigma 200 kPa s/m^2,
-porosity 0.3, tortuosity 1.8) with the two-plane airpore interface, 20-node
-PML on the five air faces, FB_p_v, 8 receivers; synthetic setup generated
-from a seed.  One bench step = ``--inner`` forward-backward time steps of
+Workload (N=1): porous ground under air over an analytic hill, 256 (range,
+Y/j) x 128 (X/i) x 96 (Z/k) air nodes over a 16-cell Zwikker-Kosten layer
+(sigma 200 kPa s/m^2, porosity 0.3, tortuosity 1.8) with the two-plane
+airpore interface, the hill z_g = h exp(-(y - y0)^2 / 2w^2) (h = 0.5 m,
+w = 1 m, y0 mid-range) on a terrain-following grid stretched vertically
+(metrics in FP64 on the host), 20-node PML on the five air faces, FB_p_v,
+source height above the ground drawn from a seed, 8 receivers 1 m above the
+ground; synthetic setup generated from a seed (``--flat``: the same domain
+on flat ground).  One bench step = ``--inner`` forward-backward time steps of
 the whole domain with the state resident in HBM; L2 is flushed (a 512 MB
 write) between bench steps.  The headline ``value`` is FP32; the FP64 path
 is reported beside it.
@@ -13,7 +17,10 @@ is reported beside it.
 ``--impl reference`` times the reference solver itself (the unmodified
 sources compiled under oracle/_ref/, driven through airpore's own loop) on
 the host cores: one independent single-rank process per core (the
-reference's MPI decomposition has no MPI here), aggregate throughput.
+reference's MPI decomposition has no MPI here), aggregate throughput. The
+reference has no terrain-following grid (it ignores terrain.dat and runs
+the domain on flat ground); its per-step work is the same, since it
+evaluates all nine metric terms at every node either way.
 
 Multi-GPU: replicas only -- each rank runs its own independent solve, no
 collective on the data path; value = all ranks' cell updates / max time.
@@ -52,13 +59,17 @@ sys.path.insert(0, ROOT)
 
 METRIC = "Gcell-upd/s & % HBM peak, FP32 vs FP64 at <=1e-4 rel err; surrogate speedup"
 UNIT = "Gcell-upd/s"
-WORKLOAD = "porous ground + 20-node PML, 256x128x96 air + 256x128x18 porous nodes, FB_p_v"
+WORKLOAD = ("porous ground under a Gaussian hill (h 0.5 m, w 1 m) on a terrain-following grid + 20-node PML, "
+            "256x128x96 air + 256x128x18 porous nodes, FB_p_v")
+FLAT_WORKLOAD = "porous ground + 20-node PML, 256x128x96 air + 256x128x18 porous nodes, FB_p_v"
+FLAT = "--flat" in sys.argv
 
 
 def make_case(tmp: str):
     casegen = importlib.import_module("3d_mpi_test_b200.casegen")
-    case, rec = casegen.porous_ground(ni=128, nj=256, nk=96, layer=16, d=0.05, steps=4000, pml=20, seed=0)
-    d = os.path.join(tmp, "porous_ground")
+    make = casegen.porous_ground if FLAT else casegen.porous_hill
+    case, rec = make(ni=128, nj=256, nk=96, layer=16, d=0.05, steps=4000, pml=20, seed=0)
+    d = os.path.join(tmp, "porous_ground" if FLAT else "porous_hill")
     case.write(d)
     casegen.write_receivers(os.path.join(d, "rec.txt"), rec)
     air = case.NI * case.NJ * case.NK
@@ -194,7 +205,8 @@ def cpu_baseline(case_dir: str, cells: int):
     if r is not None:
         return {"value": round(r["value"], 6), "unit": UNIT, "cores": r["cores"], "kind": "reference",
                 "sample": f"{reps} independent single-rank reference processes x 3 FB steps of the bench workload "
-                          f"(after 1 warm-up step); {r['ms_per_step']:.0f} ms/step each"}
+                          f"(after 1 warm-up step; the reference runs it on flat ground, same per-step work); "
+                          f"{r['ms_per_step']:.0f} ms/step each"}
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle  # the checker's own CPU restatement, timed only as the baseline
 
@@ -586,7 +598,7 @@ def run_gpu(args, rank, world, local_rank):
         "metric": METRIC, "value": round(f32["gcell"], 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(f32["ms_per_bench_step"], 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded case generator)",
-        "config": {"workload": WORKLOAD, "inner_fb_steps_per_bench_step": args.inner,
+        "config": {"workload": FLAT_WORKLOAD if FLAT else WORKLOAD, "inner_fb_steps_per_bench_step": args.inner,
                    "cells_per_fb_step": cells, "l2": "flushed (512 MB write) between bench steps",
                    "parallelism": f"replicas x{world}" if world > 1 else "single device-resident domain"},
         "fp64": {"value": round(f64["gcell"], 3), "ms_per_step": round(f64["ms_per_bench_step"], 4),
@@ -653,7 +665,8 @@ def run_reference_arm(args, world, rank):
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(r["ms_per_step"], 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded case generator)",
-        "config": {"workload": WORKLOAD, "inner_fb_steps_per_bench_step": 1, "cells_per_fb_step": cells,
+        "config": {"workload": FLAT_WORKLOAD if FLAT else WORKLOAD, "inner_fb_steps_per_bench_step": 1,
+                   "cells_per_fb_step": cells,
                    "parallelism": f"{reps} single-rank host processes"},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": reps, "kind": "reference",
                          "sample": f"{reps} independent single-rank reference processes, {args.steps} timed FB steps "
@@ -673,6 +686,7 @@ def main():
     ap.add_argument("--tile", default="", help="rows,planes,threads,vector-width,ring-stages of the marching kernel (default: autotune)")
     ap.add_argument("--workload", default="domain", choices=["domain", "ensemble", "surrogate", "window"])
     ap.add_argument("--no-surrogate", action="store_true", help="skip the surrogate section of the domain line")
+    ap.add_argument("--flat", action="store_true", help="the domain workload on flat ground (no hill)")
     ap.add_argument("--sur-queries", type=int, default=1_000_000, help="surrogate inference queries")
     ap.add_argument("--sur-train-steps", type=int, default=12000, help="training steps per surrogate member")
     ap.add_argument("--members", type=int, default=256, help="ensemble members (--workload ensemble)")

@@ -37,6 +37,11 @@ typedef struct {
     int IMAX, IMAX1, IMAX2, JMAX, JMAX1, JMAX2, JMAX3, KMAX, KMAX1, KMAX2, IJKMAX;
     double dt, rdx, rdy, rdz, dx1, dy1, dz1, gcoef;
     double *X, *Y, *Z, *axX, *axY, *axZ, *Xx, *Yy, *Zz, *Jac;
+    /* terrain-following grid (extension; NULL on flat ground): ground
+     * elevation zg[j], physical height Zt[j][k] of every node, and the
+     * metric derivatives Z_over_z = Zz2[j][k], Z_over_y = Zy2[j][k] that
+     * replace the reference's 1D Zz[k] and fixed-zero Z_over_y */
+    double *zg, *Zt, *Zz2, *Zy2;
     double *un, *vn, *wn, *pn, *unn, *vnn, *wnn, *pnn;
     double *psi; /* [i][k][6], calculation_2D.cpp:125-135 */
     mframe mf;
@@ -333,7 +338,8 @@ static int grid_init(grid *g, const char *dir, const char *prefix, double dt, do
 static void grid_free(grid *g)
 {
     double **ps[] = {&g->X, &g->Y, &g->Z, &g->axX, &g->axY, &g->axZ, &g->Xx, &g->Yy, &g->Zz, &g->Jac,
-                     &g->un, &g->vn, &g->wn, &g->pn, &g->unn, &g->vnn, &g->wnn, &g->pnn, &g->psi};
+                     &g->un, &g->vn, &g->wn, &g->pn, &g->unn, &g->vnn, &g->wnn, &g->pnn, &g->psi,
+                     &g->zg, &g->Zt, &g->Zz2, &g->Zy2};
     for (size_t i = 0; i < sizeof ps / sizeof ps[0]; ++i) { free(*ps[i]); *ps[i] = NULL; }
 }
 
@@ -346,7 +352,8 @@ static void grid_set_initial(grid *g, const double *src, int judge)
                 size_t c = IX(g, i, j, k);
                 g->un[c] = 0; g->vn[c] = 0; g->wn[c] = 0;
                 if (judge == 1) {
-                    double x = g->X[i] - src[0], y = g->Y[j] - src[1], z = g->Z[k] - src[2];
+                    double zk = g->Zt ? g->Zt[(size_t)j * g->K + k] : g->Z[k];
+                    double x = g->X[i] - src[0], y = g->Y[j] - src[1], z = zk - src[2];
                     double rr = sqrt(pow(x, 2) + pow(y, 2) + pow(z, 2));
                     g->pn[c] = 1.0 * exp(-g->gcoef * rr * rr);
                 } else {
@@ -366,13 +373,23 @@ static void grid_set_moving_frame(grid *g, int N)
     for (int i = 1; i < g->I - 1; i++) g->Xx[i] = (g->X[i + 1] - g->X[i - 1]) * g->rdx * 0.5;
     for (int j = 1; j < g->J - 1; j++) g->Yy[j] = (g->Y[j + 1] - g->Y[j - 1]) * g->rdy * 0.5;
     for (int k = 1; k < g->K - 1; k++) g->Zz[k] = (g->Z[k + 1] - g->Z[k - 1]) * g->rdz * 0.5;
+    if (g->Zt) { /* terrain: the same central differences of the node heights */
+        const int K = g->K;
+        for (int j = 0; j < g->J; j++)
+            for (int k = 1; k < K - 1; k++)
+                g->Zz2[(size_t)j * K + k] = (g->Zt[(size_t)j * K + k + 1] - g->Zt[(size_t)j * K + k - 1]) * g->rdz * 0.5;
+        for (int j = 1; j < g->J - 1; j++)
+            for (int k = 0; k < K; k++)
+                g->Zy2[(size_t)j * K + k] =
+                    (g->Zt[(size_t)(j + 1) * K + k] - g->Zt[(size_t)(j - 1) * K + k]) * g->rdy * 0.5;
+    }
     for (int i = 1; i < g->I - 1; i++)
         for (int j = 1; j < g->J - 1; j++)
             for (int k = 1; k < g->K - 1; k++) {
-                double jac = g->Xx[i] * g->Yy[j] * g->Zz[k] + Z_over_x * X_over_y * Y_over_z +
-                             Y_over_x * Z_over_y * X_over_z;
-                jac += -g->Xx[i] * Z_over_y * Y_over_z - Y_over_x * X_over_y * g->Zz[k] -
-                       Z_over_x * g->Yy[j] * X_over_z;
+                const double Zz = g->Zt ? g->Zz2[(size_t)j * g->K + k] : g->Zz[k];
+                const double Zy = g->Zt ? g->Zy2[(size_t)j * g->K + k] : Z_over_y;
+                double jac = g->Xx[i] * g->Yy[j] * Zz + Z_over_x * X_over_y * Y_over_z + Y_over_x * Zy * X_over_z;
+                jac += -g->Xx[i] * Zy * Y_over_z - Y_over_x * X_over_y * Zz - Z_over_x * g->Yy[j] * X_over_z;
                 g->Jac[IX(g, i, j, k)] = 1.0 / jac;
             }
     int temp_J = (N == 0) ? 0 : g->mf.JMAX - g->mf.lead_DJ;
@@ -408,19 +425,22 @@ static void grid_update_initial(grid *g)
 static inline double gov(double a, double b, double c, double d, double jac) { return (a * b - c * d) * jac; }
 
 /* The nine inverse metrics with the reference's fixed-zero cross terms
- * (calculation_2D.cpp:102-104; use sites air.cpp:1497-1514). */
+ * (calculation_2D.cpp:102-104; use sites air.cpp:1497-1514). On a
+ * terrain-following grid (extension) Z_over_z and Z_over_y are the node's
+ * own (j, k) values; the other cross terms stay zero. */
 typedef struct { double xX, xY, xZ, yX, yY, yZ, zX, zY, zZ; } metr;
 static inline metr metrics_at(const grid *g, int i, int j, int k)
 {
-    const double X_over_y = 0.0, X_over_z = 0.0, Y_over_x = 0.0, Y_over_z = 0.0, Z_over_x = 0.0,
-                 Z_over_y = 0.0;
+    const double X_over_y = 0.0, X_over_z = 0.0, Y_over_x = 0.0, Y_over_z = 0.0, Z_over_x = 0.0;
+    const double Z_over_y = g->Zt ? g->Zy2[(size_t)j * g->K + k] : 0.0;
+    const double Zz = g->Zt ? g->Zz2[(size_t)j * g->K + k] : g->Zz[k];
     double jac = g->Jac[IX(g, i, j, k)];
     metr m;
-    m.xX = gov(g->Yy[j], g->Zz[k], Y_over_z, Z_over_y, jac);
-    m.xY = gov(X_over_z, Z_over_y, X_over_y, g->Zz[k], jac);
+    m.xX = gov(g->Yy[j], Zz, Y_over_z, Z_over_y, jac);
+    m.xY = gov(X_over_z, Z_over_y, X_over_y, Zz, jac);
     m.xZ = gov(X_over_y, Y_over_z, X_over_z, g->Yy[j], jac);
-    m.yX = gov(Y_over_z, Z_over_x, Y_over_x, g->Zz[k], jac);
-    m.yY = gov(g->Xx[i], g->Zz[k], X_over_z, Z_over_x, jac);
+    m.yX = gov(Y_over_z, Z_over_x, Y_over_x, Zz, jac);
+    m.yY = gov(g->Xx[i], Zz, X_over_z, Z_over_x, jac);
     m.yZ = gov(X_over_z, Y_over_x, g->Xx[i], Y_over_z, jac);
     m.zX = gov(Y_over_x, Z_over_y, g->Yy[j], Z_over_x, jac);
     m.zY = gov(X_over_y, Z_over_x, g->Xx[i], Z_over_y, jac);
@@ -486,10 +506,13 @@ static void air_set_wind(airm *a, int N)
         for (int j = 0; j < g->J; j++)
             for (int k = 0; k < g->K; k++) {
                 double Z0 = 0.0;
+                /* terrain: height above the local ground */
+                double zk = g->Zt ? g->Zt[(size_t)j * g->K + k] : g->Z[k];
+                if (g->Zt) Z0 = g->zg[j];
                 size_t c = IX(g, i, j, k);
-                a->Uav[c] = sp_U(a, g->X[i], g->Y[j], g->Z[k] - Z0);
-                a->Vav[c] = sp_V(a, g->X[i], g->Y[j], g->Z[k] - Z0);
-                a->Wav[c] = sp_W(a, g->X[i], g->Y[j], g->Z[k] - Z0);
+                a->Uav[c] = sp_U(a, g->X[i], g->Y[j], zk - Z0);
+                a->Vav[c] = sp_V(a, g->X[i], g->Y[j], zk - Z0);
+                a->Wav[c] = sp_W(a, g->X[i], g->Y[j], zk - Z0);
             }
 }
 
@@ -1395,8 +1418,11 @@ static void get_position(const grid *g, int *ii, int *jj, int *kk, const double 
     if (NN >= g->IJKMAX) { *ii = 0; *jj = 0; *kk = 0; return; }
     for (int j = NN; j < g->IJKMAX && j - NN < g->JMAX; j++)
         if (rc[1] - N * Y_frame - g->axY[j - NN] <= g->dy1 / 8.0) { *jj = j; break; }
-    for (int k = 0; k < g->KMAX; k++)
-        if (rc[2] - g->axZ[k] <= g->dz1 / 8.0) { *kk = k; return; }
+    /* terrain: the heights of the column found */
+    for (int k = 0; k < g->KMAX; k++) {
+        double zk = g->Zt ? g->Zt[(size_t)*jj * g->K + k] : g->axZ[k];
+        if (rc[2] - zk <= g->dz1 / 8.0) { *kk = k; return; }
+    }
     *ii = 0; *jj = 0; *kk = 0;
 }
 
@@ -1412,6 +1438,60 @@ static double get_pressure(const grid *g, int ii, int jj, int kk, int N)
     return 0.0;
 }
 
+/* ------------------------------------------------------------ terrain */
+/* Terrain-following grid (extension of the reference, which pins the cross
+ * metrics to zero, calculation_2D.cpp:102-104): an optional
+ * case_dir/terrain.dat holds the count of Y nodes and the ground elevation
+ * z_g at each. Air nodes are stretched vertically between the ground and
+ * the flat top H = Z[K-1]: Z(j,k) = Z[k] + z_g(j) (1 - Z[k] / H), which is
+ * exactly Z[k] where z_g = 0; porous nodes follow the ground: Z(j,k) =
+ * Z[k] + z_g(j). The PML profiles stay on the file axes. */
+static int terrain_grid(grid *g, const double *zg, int porous, char *err, int errlen)
+{
+    const int K = g->K;
+    if (porous ? (K < 3 || g->axZ[K - 2] != 0.0) : (g->axZ[0] != 0.0)) {
+        seterr(err, errlen, "terrain needs the air axis to start at Z = 0 and the porous axis to end one node above 0");
+        return -1;
+    }
+    const double H = g->axZ[K - 1];
+    g->zg = zalloc(g->J);
+    g->Zt = zalloc((size_t)g->J * K);
+    g->Zz2 = zalloc((size_t)g->J * K);
+    g->Zy2 = zalloc((size_t)g->J * K);
+    for (int j = 0; j < g->J; j++) {
+        g->zg[j] = zg[j];
+        if (!porous && !(zg[j] < H)) { seterr(err, errlen, "terrain reaches the top of the air grid"); return -1; }
+        for (int k = 0; k < K; k++)
+            g->Zt[(size_t)j * K + k] = porous ? g->axZ[k] + zg[j] : g->axZ[k] + zg[j] * (1.0 - g->axZ[k] / H);
+    }
+    return 0;
+}
+
+static int terrain_setup(orc *o, const char *dir, char *err, int errlen)
+{
+    char path[4096];
+    snprintf(path, sizeof path, "%s/terrain.dat", dir);
+    size_t n = 0;
+    char *t = slurp(path, &n);
+    if (!t) return 0; /* flat ground */
+    rdr R = {t, n, 0, 0};
+    grid *g = &o->air.g;
+    int cnt = rd_i(&R);
+    if (R.fail || cnt != g->JMAX || o->mf.Judge == 1 || o->cjudge != 0) {
+        free(t);
+        seterr(err, errlen, "terrain.dat must hold one elevation per Y node, without moving frame or inclusions");
+        return -1;
+    }
+    double *zg = zalloc(cnt);
+    for (int j = 0; j < cnt; j++) zg[j] = rd_d(&R);
+    int fail = R.fail;
+    free(t);
+    if (fail) { free(zg); seterr(err, errlen, "malformed terrain.dat"); return -1; }
+    int rc = terrain_grid(g, zg, 0, err, errlen);
+    free(zg);
+    return rc;
+}
+
 /* ------------------------------------------------------------- public */
 orc *orc_create(const char *case_dir, char *err, int errlen)
 {
@@ -1422,6 +1502,10 @@ orc *orc_create(const char *case_dir, char *err, int errlen)
     if (grid_init(&a->g, case_dir, "coordi_air", o->dt, o->dx, o->dy, o->dz, o->mf, o->gauss_width, 0, err,
                   errlen) != 0) {
         free(o);
+        return NULL;
+    }
+    if (terrain_setup(o, case_dir, err, errlen) != 0) {
+        orc_destroy(o);
         return NULL;
     }
     a->gamma = o->gamma; a->P0 = o->P0; a->Aav = o->Aav; a->c0 = o->c0;
@@ -1441,6 +1525,10 @@ orc *orc_create(const char *case_dir, char *err, int errlen)
         }
         if (pg->I != a->g.I || pg->J != a->g.J) {
             seterr(err, errlen, "porous grid must share the air grid's I and J node counts");
+            orc_destroy(o);
+            return NULL;
+        }
+        if (o->air.g.zg && terrain_grid(pg, o->air.g.zg, 1, err, errlen) != 0) {
             orc_destroy(o);
             return NULL;
         }

@@ -239,6 +239,69 @@ def ensemble_member_3d():
     return c, rec
 
 
+# ------------------------------------------------ terrain-following grid
+# Extension of the reference (its cross metrics are fixed at zero), so these
+# cases are checked against the oracle's restatement only, not against the
+# compiled reference.
+def _hill(c: Case, h: float = 0.12, w: float = 0.3) -> Case:
+    y0 = c.Y[len(c.Y) // 2]
+    c.terrain = casegen.gaussian_hill(c.Y, h, w, y0)
+    return c
+
+
+def _above(c: Case, x: float, y: float, dz: float) -> Tuple[float, float, float]:
+    j = min(range(len(c.Y)), key=lambda q: abs(c.Y[q] - y))
+    return (x, y, c.terrain[j] + dz)
+
+
+def hill_porous():
+    """Porous ground under a Gaussian hill (h = 0.12 m, w = 0.3 m), PML on
+    the five air faces."""
+    layer = 5
+    c = _base(ni=16, nj=40, nk=24, bc=(PML, POROUS, PML, PML, PML, PML), pore=(math.sqrt(1.8), 0.3, 2.0e5))
+    c.pore_Z = uniform_axis(layer + 2, -layer * D, D)
+    c.pore_dxyz = (D, D, D)
+    _hill(c)
+    c.source = _above(c, 0.4, 0.7, 0.2)
+    return c, [_above(c, 0.4, 1.0, 0.3), _above(c, 0.4, 1.3, 0.2), _above(c, 0.3, 0.5, 0.5)]
+
+
+def hill_wind_pml6():
+    """Gaussian hill with PML on all six faces (the z1 layer follows the
+    ground) and a log wind profile over the local ground."""
+    c = _base(ni=16, nj=40, nk=26, bc=(PML,) * 6, pml_nodes=(5, 5, 5, 5, 4, 5), velocity_coef=1.5,
+              velocity_method=5)
+    _hill(c, h=0.12)
+    c.source = _above(c, 0.4, 0.8, 0.35)
+    return c, [_above(c, 0.4, 1.1, 0.3), _above(c, 0.45, 1.4, 0.25), _above(c, 0.4, 0.5, 0.5)]
+
+
+def hill_fbvp_tdbc():
+    """Gaussian hill with the FB_v_p scheme (two-pass kernels) and the east
+    TDBC."""
+    c = _base(ni=14, nj=36, nk=22, scheme=1, bc=(PML, RIGID, TDBC, PML, PML, PML), pore=(1.79, 0.877, 5.1e4))
+    _hill(c, h=0.1, w=0.25)
+    c.source = _above(c, 0.35, 0.7, 0.25)
+    return c, [_above(c, 0.35, 1.2, 0.3), _above(c, 0.3, 1.6, 0.2)]
+
+
+def hill_porous_tdbc():
+    """Porous ground under a hill with the east TDBC (generic tile kernel on
+    the terrain-following grid)."""
+    layer = 4
+    c = _base(ni=14, nj=37, nk=22, bc=(PML, POROUS, TDBC, PML, PML, PML), pore=(math.sqrt(1.5), 0.4, 1.0e5))
+    c.pore_Z = uniform_axis(layer + 2, -layer * D, D)
+    c.pore_dxyz = (D, D, D)
+    _hill(c, h=0.1, w=0.3)
+    c.source = _above(c, 0.35, 0.8, 0.2)
+    return c, [_above(c, 0.35, 1.1, 0.25), _above(c, 0.3, 1.5, 0.3)]
+
+
+TERRAIN_CASES: Dict[str, Callable[[], Tuple[Case, List]]] = {
+    f.__name__: f for f in [hill_porous, hill_wind_pml6, hill_fbvp_tdbc, hill_porous_tdbc]
+}
+
+
 CASES: Dict[str, Callable[[], Tuple[Case, List]]] = {
     f.__name__: f
     for f in [pml_rigid, tdbc_east, porous_ground, porous_tdbc_fine_pore, south_pml_all_faces, front_only_pml,
