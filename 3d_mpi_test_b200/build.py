@@ -50,6 +50,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
         [os.path.join(inc, f) for f in os.listdir(inc)]
     deps = [os.path.join(CSRC, f) for f in SOURCES] + headers
     if not force and not _stale(LIB, deps):
+        build_host_mirror(verbose)
         return LIB
     objdir = os.path.join(LIBDIR, "obj")
     os.makedirs(objdir, exist_ok=True)
@@ -75,7 +76,27 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)
+    build_host_mirror(verbose)
     return LIB
+
+
+HOST = os.path.join(PKG, "host")
+HOST_LIB = os.path.join(LIBDIR, "libairpore_b200.so")
+
+
+def build_host_mirror(verbose: bool = False) -> str:
+    """The C++ host classes (host/airpore_b200.cpp) as libairpore_b200.so
+    over libfdtd_b200.so, found next to it at run time."""
+    src = os.path.join(HOST, "airpore_b200.cpp")
+    deps = [src, os.path.join(HOST, "airpore_b200.hpp"), os.path.join(ROOT, "include", "fdtd_b200.h"), LIB]
+    if not _stale(HOST_LIB, deps):
+        return HOST_LIB
+    cmd = [shutil.which("g++") or "g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-I", os.path.join(ROOT, "include"),
+           src, "-o", HOST_LIB, "-L", LIBDIR, "-lfdtd_b200", "-Wl,-rpath,$ORIGIN"]
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    subprocess.run(cmd, check=True)
+    return HOST_LIB
 
 
 if __name__ == "__main__":

@@ -1575,9 +1575,10 @@ class SolverImpl final : public SolverImplBase {
         int TI, TV, GC, ns;
     };
 
+    // shapes measured best on a 3.7 M-node porous-ground domain (B200)
     static TileCfg default_tile(bool lean) {
-        if (sizeof(R) == 4) return lean ? TileCfg{8, 32, 16, 4} : TileCfg{8, 16, 16, 4};
-        return lean ? TileCfg{8, 32, 16, 4} : TileCfg{8, 16, 16, 4};
+        if (sizeof(R) == 4) return lean ? TileCfg{16, 8, 8, 3} : TileCfg{8, 16, 8, 3};
+        return lean ? TileCfg{8, 16, 32, 4} : TileCfg{8, 16, 16, 3};
     }
 
     TileGeo tile_geo(int TI, int TV, int ns) const {
@@ -1853,9 +1854,10 @@ class SolverImpl final : public SolverImplBase {
         return o;
     }
 
-    // Project autotuner for the tiled kernel: the lean tile shape first,
-    // then the PML / face shape, then the full shape (the others at
-    // their current shapes), each candidate timed over nsteps steps on this
+    // Project autotuner for the tiled kernel: the lean tile shape, then the
+    // PML / face shape, then the full shape (the others at their current
+    // shapes), twice over, since the kinds share the device step by step;
+    // each candidate is the better of two timings of nsteps steps on this
     // domain
     std::array<int, 5> autotune_tiles(int nsteps) {
         std::vector<TileCfg> cands;
@@ -1863,7 +1865,7 @@ class SolverImpl final : public SolverImplBase {
         for (int TV : {16 / V * 2, 32 / V * 2, 64 / V * 2})
             for (int TI : {4, 8, 16})
                 for (int GC : {8, 16, 32})
-                    for (int ns : {3, 5}) {
+                    for (int ns : {3, 4}) {
                         const TileCfg c{TI, TV, GC, ns};
                         try {
                             check_tile(c);
@@ -1872,24 +1874,35 @@ class SolverImpl final : public SolverImplBase {
                         }
                         cands.push_back(c);
                     }
+        // whole CUDA graphs of steps, as the time loop runs them
+        const int nt = std::max(1, (nsteps + kGraphSteps - 1) / kGraphSteps) * kGraphSteps;
         const int saved_horizon = horizon_;
-        reset(std::max(horizon_, (nsteps + 2) * static_cast<int>(3 * cands.size() + 2) + 4));
-        for (int cfg : {1, 2, 0}) {
-            bool used = false;
-            for (int k = 0; k < kKinds; ++k) used = used || (cfg_of(k) == cfg && ntile_[k]);
-            if (!used) continue;
-            TileCfg best = tcfg_[cfg];
-            double best_ms = 1e300;
-            for (const TileCfg& c : cands) {
-                tcfg_[cfg] = c;
-                build_tiles();
-                advance(2, nullptr);  // graph build and first touch outside the timing
-                advance(nsteps, nullptr);
-                if (last_ms_ < best_ms) { best_ms = last_ms_; best = c; }
-            }
-            tcfg_[cfg] = best;
+        reset(std::max(horizon_, (3 * nt + 2) * static_cast<int>(6 * cands.size() + 8) + 4));
+        auto time_cfg = [&]() {
             build_tiles();
-        }
+            advance(nt, nullptr);  // graph build and first touch outside the timing
+            double best = 1e300;
+            for (int rep = 0; rep < 2; ++rep) {
+                advance(nt, nullptr);
+                best = std::min(best, last_ms_);
+            }
+            return best;
+        };
+        for (int pass = 0; pass < 2; ++pass)
+            for (int cfg : {1, 2, 0}) {
+                bool used = false;
+                for (int k = 0; k < kKinds; ++k) used = used || (cfg_of(k) == cfg && ntile_[k]);
+                if (!used) continue;
+                TileCfg best = tcfg_[cfg];
+                double best_ms = time_cfg();
+                for (const TileCfg& c : cands) {
+                    tcfg_[cfg] = c;
+                    const double ms = time_cfg();
+                    if (ms < best_ms) { best_ms = ms; best = c; }
+                }
+                tcfg_[cfg] = best;
+                build_tiles();
+            }
         reset(saved_horizon);
         return {tcfg_[0].TI, tcfg_[0].GC, tthr_[0], kVecMax, tcfg_[0].ns};
     }
@@ -1931,15 +1944,17 @@ class SolverImpl final : public SolverImplBase {
                         }
                     }
         }
+        // whole CUDA graphs of steps, as the time loop runs them
+        const int nt = std::max(1, (nsteps + kGraphSteps - 1) / kGraphSteps) * kGraphSteps;
         const int saved_horizon = horizon_;
-        const int h = std::max(horizon_, (nsteps + 2) * static_cast<int>(cands.size()) + 4);
+        const int h = std::max(horizon_, 2 * nt * static_cast<int>(cands.size()) + 4);
         std::array<int, 5> best{tiling_.TI, tiling_.GC, fused_threads_, tiling_.VW, tiling_.nstage};
         double best_ms = 1e300;
         reset(h);
         for (const auto& c : cands) {
             set_tiling(c[0], c[1], c[2], c[3], c[4]);
-            advance(2, nullptr);  // graph build and first-touch outside the timing
-            advance(nsteps, nullptr);
+            advance(nt, nullptr);  // graph build and first touch outside the timing
+            advance(nt, nullptr);
             if (last_ms_ < best_ms) { best_ms = last_ms_; best = c; }
         }
         set_tiling(best[0], best[1], best[2], best[3], best[4]);
