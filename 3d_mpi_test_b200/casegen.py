@@ -95,6 +95,12 @@ class Case:
     # every Y node. Air nodes are stretched between the ground and the flat
     # top, porous nodes follow the ground. None: flat ground.
     terrain: Optional[List[float]] = None
+    # log-law wind (extension, velocity_method 7): (kappa, z0) written to
+    # logwind.dat; None keeps kappa 0.41 and z0 0.01 m
+    logwind: Optional[Tuple[float, float]] = None
+    # velocity advection by the mean wind (extension, advection.dat): None or
+    # "reference" (forward differences) or "upwind" (backward differences)
+    advection: Optional[str] = None
 
     # ------------------------------------------------------------------ #
     @property
@@ -200,6 +206,12 @@ class Case:
             if len(self.terrain) != self.NJ:
                 raise ValueError("terrain needs one elevation per Y node")
             files["terrain.dat"] = f"{self.NJ}\n" + " ".join(_fmt(float(v)) for v in self.terrain) + "\n"
+        if self.advection is not None:
+            if self.advection not in ("reference", "upwind"):
+                raise ValueError("advection must be 'reference' or 'upwind'")
+            files["advection.dat"] = self.advection + "\n"
+        if self.logwind is not None:
+            files["logwind.dat"] = f"{_fmt(float(self.logwind[0]))} {_fmt(float(self.logwind[1]))}\n"
         for name, txt in files.items():
             with open(os.path.join(case_dir, name), "w") as f:
                 f.write(txt)

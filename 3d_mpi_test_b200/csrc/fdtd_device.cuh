@@ -57,6 +57,11 @@ struct Dev {
     int rigid_south;  // air has its own south face (rigid / absorbing)
     int tdbc;         // east face is the 6-pole TDBC
     int fbvp;         // scheme FB_v_p (velocity first)
+    // advection of the velocity by the mean wind: 0 the reference's forward
+    // differences (air.cpp:1476-1949), 1 backward differences (extension,
+    // upwind for wind blowing toward +i/+j/+k; the WindNb neighbours are
+    // then the backward ones)
+    int upwind;
 
     // state: "in" = read, "out" = written
     const R *u_in, *v_in, *w_in, *p_in;  // old u,v,w (or new, FB_v_p pressure pass) and the p used
@@ -550,10 +555,12 @@ __device__ __forceinline__ void pml_dvel_v(const Dev<R>& d, int i, int jb, int k
     }
 }
 
-// forward neighbours of u, v, w for the wind advection terms
+// neighbours of u, v, w for the wind advection terms: f(i+1), f(j+1),
+// f(g+1) (the reference's forward differences), or f(i-1), f(j-1), f(g-1)
+// when d.upwind
 template <typename R, int N>
 struct WindNb {
-    Arr<R, N> ui, uj, uk, vi, vj, vk, wi, wj, wk;  // f(i+1), f(j+1), f(g+1)
+    Arr<R, N> ui, uj, uk, vi, vj, vk, wi, wj, wk;
 };
 
 // Mean-wind part of the air velocity increment at one node: forward-
@@ -566,7 +573,12 @@ __device__ __forceinline__ void wind_dvel(const Dev<R>& d, int j, int k, R ax, R
                                           R& dw) {
     const int q = k * d.NJ + j, wS = d.NJ;
     const R U = ldg(d.Uw + q), V = ldg(d.Vw + q), W = ldg(d.Ww + q);
-    const R c1 = U * ax * d.dt, c2 = V * ay * d.dt, c3 = TER ? (V * zy + W * az) * d.dt : W * az * d.dt;
+    R c1 = U * ax * d.dt, c2 = V * ay * d.dt, c3 = TER ? (V * zy + W * az) * d.dt : W * az * d.dt;
+    if (d.upwind) {  // backward differences: (f - f_back) = -(f_back - f)
+        c1 = -c1;
+        c2 = -c2;
+        c3 = -c3;
+    }
     du += -c1 * (ui - u0) - c2 * (uj - u0) - c3 * (uk - u0);
     dv += -c1 * (vi - v0) - c2 * (vj - v0) - c3 * (vk - v0);
     dw += -c1 * (wi - w0) - c2 * (wj - w0) - c3 * (wk - w0);
@@ -733,9 +745,11 @@ __device__ Vel<R, 1> fresh_vel(const Dev<R>& d, int i, int j, int g, bool y1_on)
     const size_t si = d.NJP, sg = static_cast<size_t>(d.NI) * d.NJP;
     const R* p = d.p_in;
     WindNb<R, 1> nb{};
-    if (WIND && !pc.pore)
-        nb = {A{{d.u_in[c + si]}}, A{{d.u_in[c + 1]}}, A{{d.u_in[c + sg]}}, A{{d.v_in[c + si]}}, A{{d.v_in[c + 1]}},
-              A{{d.v_in[c + sg]}}, A{{d.w_in[c + si]}}, A{{d.w_in[c + 1]}}, A{{d.w_in[c + sg]}}};
+    if (WIND && !pc.pore) {
+        const size_t ci = d.upwind ? c - si : c + si, cj = d.upwind ? c - 1 : c + 1, ck = d.upwind ? c - sg : c + sg;
+        nb = {A{{d.u_in[ci]}}, A{{d.u_in[cj]}}, A{{d.u_in[ck]}}, A{{d.v_in[ci]}}, A{{d.v_in[cj]}},
+              A{{d.v_in[ck]}}, A{{d.w_in[ci]}}, A{{d.w_in[cj]}}, A{{d.w_in[ck]}}};
+    }
     if (d.azT) {
         TerC<R, 1> tc{};
         ter_factors<R, 1>(d, g, j, tc.az, tc.zy);

@@ -183,6 +183,18 @@ std::string parse_reference_case(const std::string& dir, ReferenceInput& in) {
         for (double& v : in.terrain) v = t.d();
         if (t.fail) return "malformed " + dir + "/terrain.dat";
     }
+    if (in.velocity_method == 7 && slurp(dir + "/logwind.dat", tt)) {
+        Reader t{tt};
+        in.wind_kappa = t.d();
+        in.wind_z0 = t.d();
+        if (t.fail || !(in.wind_kappa > 0.0) || !(in.wind_z0 > 0.0)) return "logwind.dat must hold kappa > 0 and z0 > 0";
+    }
+    if (slurp(dir + "/advection.dat", tt)) {
+        Reader t{tt};
+        const std::string w = t.word();
+        if (w == "upwind") in.upwind_advection = true;
+        else if (w != "reference") return "advection.dat must hold 'upwind' or 'reference'";
+    }
     return "";
 }
 

@@ -58,6 +58,13 @@ struct ReferenceInput {
     // terrain-following grid (extension, optional terrain.dat: the count of Y
     // nodes, then the ground elevation at each); empty: flat ground
     std::vector<double> terrain;
+    // log-law wind (extension, method 7): V = (velocity_coef / kappa) ln(z / z0),
+    // optional logwind.dat holding kappa and z0
+    double wind_kappa = 0.41, wind_z0 = 0.01;
+    // velocity advection by the mean wind (extension, optional advection.dat:
+    // "reference" forward differences as air.cpp:1476-1949, or "upwind"
+    // backward differences)
+    bool upwind_advection = false;
 };
 
 // Returns "" on success, otherwise a one-line error.

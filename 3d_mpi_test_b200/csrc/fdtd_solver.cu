@@ -63,10 +63,15 @@ struct Medium {
 
 // SpeedProfile (air.cpp:71-253) for the methods whose parameters the
 // reference initialises. Returns false for methods 3 and 6, which read
-// members the reference never sets.
-bool wind_at(int method, double b, double y, double z, double& U, double& V, double& W) {
+// members the reference never sets. Method 7 (extension): the surface-layer
+// log law V = (u* / kappa) ln(z / z0) with u* = b, calm at and below z0.
+bool wind_at(int method, double b, double y, double z, double& U, double& V, double& W, double kappa = 0.41,
+             double z0 = 0.01) {
     U = V = W = 0.0;
     switch (method) {
+        case 7:
+            V = z > z0 ? b / kappa * std::log(z / z0) : 0.0;
+            return true;
         case 1:
             V = z >= 2.8 ? b * 2.8 : (z >= 0.0 ? b * z : 0.0);
             return true;
@@ -200,8 +205,9 @@ class SolverImpl final : public SolverImplBase {
         // alternative. FB_v_p keeps the two passes.
         const int nvec = NJP_ / kVecMax;
         fused_ = in.scheme == FB_P_V;
-        // (the row marching kernel has no terrain-following form)
-        old_ok_ = fused_ && !terrain_ && nvec <= kMarchThreads &&
+        // (the row marching kernel has no terrain-following form and does
+        // not stage the backward neighbours of upwind advection)
+        old_ok_ = fused_ && !terrain_ && !in.upwind_advection && nvec <= kMarchThreads &&
                   march_smem_bytes(make_tiling(2, 16, 1, kVecMax, 0)) <= kSmemMax;
         if (old_ok_) {  // 4-row tiles where they fit shared memory, else 2-row
             const int TI = march_smem_bytes(make_tiling(4, 16, 256 / nvec, kVecMax, 0)) <= kSmemMax ? 4 : 2;
@@ -324,7 +330,7 @@ class SolverImpl final : public SolverImplBase {
         for (int k = 0; k < Kair_ && !wind_on_; ++k)
             for (int j = 0; j < NJ_ && !wind_on_; ++j) {
                 double U, V, W;
-                wind_at(in.velocity_method, in.velocity_coef, air_.Y[j], wind_z(j, k), U, V, W);
+                wind_at(in.velocity_method, in.velocity_coef, air_.Y[j], wind_z(j, k), U, V, W, in.wind_kappa, in.wind_z0);
                 if (U != 0.0 || V != 0.0 || W != 0.0) wind_on_ = true;
             }
     }
@@ -662,7 +668,7 @@ class SolverImpl final : public SolverImplBase {
             for (int k = 0; k < Kair_; ++k)
                 for (int j = 0; j < NJ_; ++j) {
                     const size_t q = static_cast<size_t>(k) * NJ_ + j;
-                    wind_at(in.velocity_method, in.velocity_coef, air_.Y[j], wind_z(j, k), U[q], V[q], Wv[q]);
+                    wind_at(in.velocity_method, in.velocity_coef, air_.Y[j], wind_z(j, k), U[q], V[q], Wv[q], in.wind_kappa, in.wind_z0);
                 }
             upload(d_Uw_, U); upload(d_Vw_, V); upload(d_Ww_, Wv);
         }
@@ -782,6 +788,7 @@ class SolverImpl final : public SolverImplBase {
         d.rigid_south = !porous_;
         d.tdbc = tdbc_;
         d.fbvp = in.scheme == FB_V_P;
+        d.upwind = in.upwind_advection ? 1 : 0;
         const bool fbpv = in.scheme == FB_P_V;
         const int o = par, nw = 1 - par;
         if (pressure) {
@@ -1382,7 +1389,7 @@ class SolverImpl final : public SolverImplBase {
                 for (int j = 0; j < NJ_; ++j)
                     for (int k = 0; k < Kair_; ++k) {
                         double U = 0, V = 0, W = 0;
-                        if (wind_on_) wind_at(in.velocity_method, in.velocity_coef, air_.Y[j], wind_z(j, k), U, V, W);
+                        if (wind_on_) wind_at(in.velocity_method, in.velocity_coef, air_.Y[j], wind_z(j, k), U, V, W, in.wind_kappa, in.wind_z0);
                         put(U); put(V); put(W);
                     }
             for (int sl = 0; sl < 6; ++sl) {
@@ -1562,6 +1569,7 @@ class SolverImpl final : public SolverImplBase {
         FDTD_CK(cudaSetDevice(device_));
         if (!fused_) fail(-2, "tiling applies to the fused FB_p_v pass only");
         if (terrain_) fail(-2, "the row marching kernel has no terrain-following form");
+        if (in.upwind_advection) fail(-2, "the row marching kernel has no upwind-advection form");
         if (!old_ok_) fail(-2, "rows too wide for the row marching kernel");
         set_tiling(TI, GC, nt, vw, stages);
         tile_on_ = false;  // the row marching kernel runs from now on
@@ -1586,7 +1594,8 @@ class SolverImpl final : public SolverImplBase {
         TileGeo g{};
         g.TI = TI;
         g.TV = TV;
-        g.ns = ns;
+        // upwind wind advection keeps plane g-1 until the next barrier: one more stage
+        g.ns = (wind_on_ && in.upwind_advection) ? std::max(ns, 4) : ns;
         g.srows = TI + 2 + W;
         g.svec = TV + 2 + W;
         const size_t bb = (static_cast<size_t>(g.srows) * g.svec * kVecMax * sizeof(R) + 127) / 128 * 128;
@@ -2355,8 +2364,8 @@ class EnsembleImpl final : public EnsembleImplBase {
         if (mode_ == 0)
             for (const auto& m : v)
                 if (!m.old_ok)
-                    fail(-2, "a member's rows are too wide for the batched marching kernel, or its grid follows "
-                             "terrain (use mode 1)");
+                    fail(-2, "a member cannot run on the batched marching kernel (rows too wide, a "
+                             "terrain-following grid or upwind advection): use mode 1");
         // block size class: 64-thread steps, so narrow (2D) members do not
         // share a launch with 256-thread blocks
         auto key_of = [&](size_t i) {

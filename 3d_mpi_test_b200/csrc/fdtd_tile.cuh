@@ -81,6 +81,52 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
 }
 
 // TER: terrain-following grid (per-column z_over_Z and z_over_Y factors)
+// Wind advection neighbours of a thread's column vector at plane g from the
+// staged boxes: forward (i+1, j+1, g+1; the reference's differences) or,
+// with upwind, backward (i-1, j-1, g-1). U, Vf, Wf point at the node in the
+// plane-g box, Un.. / Um.. at it in the g+1 / g-1 boxes, SP is the staged
+// row pitch; tail: column jb + V exists (forward j neighbour of the last
+// element).
+template <typename R, int V>
+__device__ __forceinline__ WindNb<R, V> wind_nb(bool upwind, const R* U, const R* Vf, const R* Wf, const R* Un,
+                                                const R* Vn, const R* Wn, const R* Um, const R* Vm, const R* Wm,
+                                                int SP, const Arr<R, V>& u0, const Arr<R, V>& v0,
+                                                const Arr<R, V>& w0, bool tail) {
+    WindNb<R, V> nb;
+    if (!upwind) {
+        nb.ui = ldn<R, V>(U + SP);
+        nb.vi = ldn<R, V>(Vf + SP);
+        nb.wi = ldn<R, V>(Wf + SP);
+        nb.uk = ldn<R, V>(Un);
+        nb.vk = ldn<R, V>(Vn);
+        nb.wk = ldn<R, V>(Wn);
+        const R un = tail ? U[V] : R(0), vv = tail ? Vf[V] : R(0), wn = tail ? Wf[V] : R(0);
+#pragma unroll
+        for (int e = 0; e < V; ++e) {
+            const int e1 = e + 1 < V ? e + 1 : 0;
+            nb.uj.e[e] = e + 1 < V ? u0.e[e1] : un;
+            nb.vj.e[e] = e + 1 < V ? v0.e[e1] : vv;
+            nb.wj.e[e] = e + 1 < V ? w0.e[e1] : wn;
+        }
+    } else {
+        nb.ui = ldn<R, V>(U - SP);
+        nb.vi = ldn<R, V>(Vf - SP);
+        nb.wi = ldn<R, V>(Wf - SP);
+        nb.uk = ldn<R, V>(Um);
+        nb.vk = ldn<R, V>(Vm);
+        nb.wk = ldn<R, V>(Wm);
+        const R up = U[-1], vp = Vf[-1], wp = Wf[-1];
+#pragma unroll
+        for (int e = 0; e < V; ++e) {
+            const int e1 = e > 0 ? e - 1 : 0;
+            nb.uj.e[e] = e > 0 ? u0.e[e1] : up;
+            nb.vj.e[e] = e > 0 ? v0.e[e1] : vp;
+            nb.wj.e[e] = e > 0 ? w0.e[e1] : wp;
+        }
+    }
+    return nb;
+}
+
 template <typename R, bool WIND, int VW, bool FULL, bool XF, bool TER = false>
 __global__ void __launch_bounds__(kTileMaxThreads)
     k_tile(const __grid_constant__ Dev<R> d, const __grid_constant__ TileMaps maps, const TileGeo tg,
@@ -183,8 +229,13 @@ __global__ void __launch_bounds__(kTileMaxThreads)
     // planes below g are never read after the barrier of plane g, so a stage
     // is refilled once the plane it held is below the plane just passed
     int issued_hi = plo - 1;
+    // a stage is refilled once no thread reads its plane any more: planes
+    // below g after the barrier of plane g, below g - 1 when upwind wind
+    // advection reads plane g - 1 in the velocity phase (the host then
+    // keeps at least 4 stages)
+    const int lag = (WIND && d.upwind) ? 1 : 0;
     auto refill = [&](int g) {
-        while (issued_hi + 1 <= c1 && issued_hi + 1 - ns < g && !timed_out) issue(++issued_hi);
+        while (issued_hi + 1 <= c1 && issued_hi + 1 - ns < g - lag && !timed_out) issue(++issued_hi);
     };
     if (tid == 0) refill(plo);
 
@@ -251,24 +302,10 @@ __global__ void __launch_bounds__(kTileMaxThreads)
 #pragma unroll
             for (int e = 0; e < V; ++e) Pj.e[e] = e > 0 ? pnew.e[e > 0 ? e - 1 : 0] : Pj0;
             WindNb<R, V> nb{};
-            if (WIND && !pc.pore) {
-                const R *U = fld(sg, 0) + so, *Vf = fld(sg, 1) + so, *Wf = fld(sg, 2) + so;
-                nb.ui = ui;
-                nb.vi = ldn<R, V>(Vf + SP);
-                nb.wi = ldn<R, V>(Wf + SP);
-                nb.uk = ldn<R, V>(fld(sn, 0) + so);
-                nb.vk = ldn<R, V>(fld(sn, 1) + so);
-                nb.wk = wk;
-                const bool tail = jb + V <= NJ - 1;
-                const R un = tail ? U[V] : R(0), vv = tail ? vn : R(0), wn = tail ? Wf[V] : R(0);
-#pragma unroll
-                for (int e = 0; e < V; ++e) {
-                    const int e1 = e + 1 < V ? e + 1 : 0;
-                    nb.uj.e[e] = e + 1 < V ? u0.e[e1] : un;
-                    nb.vj.e[e] = e + 1 < V ? v0.e[e1] : vv;
-                    nb.wj.e[e] = e + 1 < V ? w0.e[e1] : wn;
-                }
-            }
+            if (WIND && !pc.pore)
+                nb = wind_nb<R, V>(d.upwind != 0, fld(sg, 0) + so, fld(sg, 1) + so, fld(sg, 2) + so, fld(sn, 0) + so,
+                                   fld(sn, 1) + so, fld(sn, 2) + so, fld(sm, 0) + so, fld(sm, 1) + so,
+                                   fld(sm, 2) + so, SP, u0, v0, w0, jb + V <= NJ - 1);
             const Vel<R, V> vel = vel_vec<R, WIND, V, XF, FULL, TER>(d, pc, rc, ic, jb, ay, ys, u0, v0, w0, pnew, Pi,
                                                                       Pj, pprev, nb, true, tc);
             const size_t go = (static_cast<size_t>(g) * NI + i) * d.NJP + jb;
@@ -326,11 +363,10 @@ __global__ void __launch_bounds__(kTileMaxThreads)
                         using A = Arr<R, 1>;
                         const R *U = fld(sg, 0) + so - 1, *Vf = fld(sg, 1) + so - 1, *Wf = fld(sg, 2) + so - 1;
                         WindNb<R, 1> nbs{};
-                        if (WIND && !pc.pore) {
-                            const R *Un = fld(sn, 0) + so - 1, *Vn = fld(sn, 1) + so - 1, *Wn = fld(sn, 2) + so - 1;
-                            nbs = {A{{U[SP]}},  A{{U[1]}},  A{{Un[0]}}, A{{Vf[SP]}}, A{{Vf[1]}},
-                                   A{{Vn[0]}},  A{{Wf[SP]}}, A{{Wf[1]}}, A{{Wn[0]}}};
-                        }
+                        if (WIND && !pc.pore)
+                            nbs = wind_nb<R, 1>(d.upwind != 0, U, Vf, Wf, fld(sn, 0) + so - 1, fld(sn, 1) + so - 1,
+                                                fld(sn, 2) + so - 1, fld(sm, 0) + so - 1, fld(sm, 1) + so - 1,
+                                                fld(sm, 2) + so - 1, SP, A{{U[0]}}, A{{Vf[0]}}, A{{Wf[0]}}, true);
                         const R ays = ldg((pc.pore ? d.ayP : d.ayA) + NJ - 2);
                         TerC<R, 1> tcs{};
                         if (TER) ter_factors<R, 1>(d, g, NJ - 2, tcs.az, tcs.zy);

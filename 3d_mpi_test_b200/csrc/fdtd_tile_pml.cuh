@@ -197,8 +197,13 @@ __global__ void __launch_bounds__(kTileMaxThreads)
         if (!mbar_wait(&bar[x % ns], static_cast<uint32_t>(((x - plo) / ns) & 1), spin)) timed_out = true;
     };
     int issued_hi = plo - 1;
+    // a stage is refilled once no thread reads its plane any more: planes
+    // below g after the barrier of plane g, below g - 1 when upwind wind
+    // advection reads plane g - 1 in the velocity phase (the host then
+    // keeps at least 4 stages)
+    const int lag = (WIND && d.upwind) ? 1 : 0;
     auto refill = [&](int g) {
-        while (issued_hi + 1 <= c1 && issued_hi + 1 - ns < g && !timed_out) issue(++issued_hi);
+        while (issued_hi + 1 <= c1 && issued_hi + 1 - ns < g - lag && !timed_out) issue(++issued_hi);
     };
     if (tid == 0) refill(plo);
 
@@ -366,20 +371,16 @@ __global__ void __launch_bounds__(kTileMaxThreads)
                     dw.e[e] = -d.Aavdt * gpZ.e[e];
                 }
                 if (WIND) {
-                    const R *U = fld(sg, 0) + so, *Vf = fld(sg, 1) + so, *Wf = fld(sg, 2) + so;
-                    const Arr<R, V> vi = ldn<R, V>(Vf + SP), wi = ldn<R, V>(Wf + SP);
-                    const Arr<R, V> uk = ldn<R, V>(fld(sn, 0) + so), vk = ldn<R, V>(fld(sn, 1) + so);
-                    const bool tail = jb + V <= NJ - 1;
-                    const R un = tail ? U[V] : R(0), vv = tail ? vn : R(0), wn = tail ? Wf[V] : R(0);
+                    const WindNb<R, V> nb =
+                        wind_nb<R, V>(d.upwind != 0, fld(sg, 0) + so, fld(sg, 1) + so, fld(sg, 2) + so,
+                                      fld(sn, 0) + so, fld(sn, 1) + so, fld(sn, 2) + so, fld(sm, 0) + so,
+                                      fld(sm, 1) + so, fld(sm, 2) + so, SP, u0, v0, w0, jb + V <= NJ - 1);
 #pragma unroll
-                    for (int e = 0; e < V; ++e) {
-                        const int e1 = e + 1 < V ? e + 1 : 0;
+                    for (int e = 0; e < V; ++e)
                         if (jb + e >= 1 && jb + e <= NJ - 2)
-                            wind_dvel<R, TER>(d, jb + e, k, ax, ay.e[e], az.e[e], zy.e[e], u0.e[e], v0.e[e], w0.e[e], ui.e[e],
-                                      e + 1 < V ? u0.e[e1] : un, uk.e[e], vi.e[e], e + 1 < V ? v0.e[e1] : vv,
-                                      vk.e[e], wi.e[e], e + 1 < V ? w0.e[e1] : wn, wk.e[e], du.e[e], dv.e[e],
-                                      dw.e[e]);
-                    }
+                            wind_dvel<R, TER>(d, jb + e, k, ax, ay.e[e], az.e[e], zy.e[e], u0.e[e], v0.e[e], w0.e[e],
+                                              nb.ui.e[e], nb.uj.e[e], nb.uk.e[e], nb.vi.e[e], nb.vj.e[e], nb.vk.e[e],
+                                              nb.wi.e[e], nb.wj.e[e], nb.wk.e[e], du.e[e], dv.e[e], dw.e[e]);
                 }
                 // PML terms in the order of pml_dvel_v, with Qp advanced to
                 // this step at the node and its backward neighbours

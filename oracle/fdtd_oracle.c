@@ -63,6 +63,8 @@ typedef struct {
     double *Uav, *Vav, *Wav;
     int vmethod;
     double vb, vc, valpha; /* SpeedProfile, air.cpp:40-43 */
+    double vkappa, vz0;    /* log law (extension, method 7): V = (vb / vkappa) ln(z / vz0) */
+    int upwind;            /* extension: backward-difference velocity advection (advection.dat) */
     double gamma, P0, Aav, c0;
     int jx, jy, jz;
     double sxmax, ax, symax, ay, szmax, az;
@@ -475,6 +477,8 @@ static double sp_V(airm *a, double x, double y, double z)
         return -1.0 * 2.0 / (Rr + 2.0) * sin(a->valpha);
     }
     case 5: return a->vb * log(fabs(z) / 0.1 + 1);
+    /* extension: the surface-layer log law (u_star / kappa) ln(z / z0), calm below z0 */
+    case 7: return z > a->vz0 ? a->vb / a->vkappa * log(z / a->vz0) : 0.0;
     default: return 0;
     }
 }
@@ -972,13 +976,16 @@ static void air_cal_fuvw(airm *a, const double *tu, const double *tv, const doub
                              m.zY * BDK(tp, g, i, j, k) * rdz;
                 double gpZ = m.xZ * BDI(tp, g, i, j, k) * rdx + m.yZ * BDJ(tp, g, i, j, k) * rdy +
                              m.zZ * BDK(tp, g, i, j, k) * rdz;
-                double un = -coef1 * FDI(tu, g, i, j, k) - coef2 * FDJ(tu, g, i, j, k) - coef3 * FDK(tu, g, i, j, k);
+                double un = (a->upwind ? -coef1 * BDI(tu, g, i, j, k) - coef2 * BDJ(tu, g, i, j, k) - coef3 * BDK(tu, g, i, j, k)
+                                     : -coef1 * FDI(tu, g, i, j, k) - coef2 * FDJ(tu, g, i, j, k) - coef3 * FDK(tu, g, i, j, k));
                 un += -u * U_X * dt - v * U_Y * dt - w * U_Z * dt;
                 un += -Aav * dt * (gpX);
-                double vn = -coef1 * FDI(tv, g, i, j, k) - coef2 * FDJ(tv, g, i, j, k) - coef3 * FDK(tv, g, i, j, k);
+                double vn = (a->upwind ? -coef1 * BDI(tv, g, i, j, k) - coef2 * BDJ(tv, g, i, j, k) - coef3 * BDK(tv, g, i, j, k)
+                                     : -coef1 * FDI(tv, g, i, j, k) - coef2 * FDJ(tv, g, i, j, k) - coef3 * FDK(tv, g, i, j, k));
                 vn += -u * V_X * dt - v * V_Y * dt - w * V_Z * dt;
                 vn += -Aav * dt * (gpY);
-                double wn = -coef1 * FDI(tw, g, i, j, k) - coef2 * FDJ(tw, g, i, j, k) - coef3 * FDK(tw, g, i, j, k);
+                double wn = (a->upwind ? -coef1 * BDI(tw, g, i, j, k) - coef2 * BDJ(tw, g, i, j, k) - coef3 * BDK(tw, g, i, j, k)
+                                     : -coef1 * FDI(tw, g, i, j, k) - coef2 * FDJ(tw, g, i, j, k) - coef3 * FDK(tw, g, i, j, k));
                 wn += -u * W_X * dt - v * W_Y * dt - w * W_Z * dt;
                 wn += -Aav * dt * (gpZ);
                 double sx1v = 0, bx1 = 0, sx2v = 0, bx2 = 0;
@@ -1510,6 +1517,32 @@ orc *orc_create(const char *case_dir, char *err, int errlen)
     }
     a->gamma = o->gamma; a->P0 = o->P0; a->Aav = o->Aav; a->c0 = o->c0;
     a->vmethod = o->vmethod; a->vb = o->vcoef; a->vc = o->c0; a->valpha = 1.256431;
+    a->vkappa = 0.41; a->vz0 = 0.01;
+    { /* optional case_dir/advection.dat: "upwind" or "reference" */
+        char path[4096];
+        snprintf(path, sizeof path, "%s/advection.dat", case_dir);
+        size_t n = 0;
+        char *t = slurp(path, &n);
+        if (t) {
+            a->upwind = strncmp(t, "upwind", 6) == 0;
+            int ok = a->upwind || strncmp(t, "reference", 9) == 0;
+            free(t);
+            if (!ok) { seterr(err, errlen, "advection.dat must hold 'upwind' or 'reference'"); orc_destroy(o); return NULL; }
+        }
+    }
+    if (o->vmethod == 7) { /* optional case_dir/logwind.dat: kappa z0 */
+        char path[4096];
+        snprintf(path, sizeof path, "%s/logwind.dat", case_dir);
+        size_t n = 0;
+        char *t = slurp(path, &n);
+        if (t) {
+            rdr R = {t, n, 0, 0};
+            a->vkappa = rd_d(&R); a->vz0 = rd_d(&R);
+            int bad = R.fail || !(a->vkappa > 0) || !(a->vz0 > 0);
+            free(t);
+            if (bad) { seterr(err, errlen, "logwind.dat must hold kappa > 0 and z0 > 0"); orc_destroy(o); return NULL; }
+        }
+    }
     size_t N = (size_t)a->g.I * a->g.J * a->g.K;
     a->Uav = zalloc(N); a->Vav = zalloc(N); a->Wav = zalloc(N);
     air_pml_setup(o);

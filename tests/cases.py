@@ -302,6 +302,54 @@ TERRAIN_CASES: Dict[str, Callable[[], Tuple[Case, List]]] = {
 }
 
 
+# ------------------------------------------- log-law wind, upwind advection
+# Extensions of the reference (its wind methods stop at 6 and its velocity
+# advection is a forward difference), checked against the oracle only.
+def wind_loglaw():
+    """The surface-layer log law V = (u*/kappa) ln(z/z0) (method 7,
+    kappa 0.41, z0 0.01 m) with the reference's forward-difference
+    velocity advection."""
+    return _base(velocity_coef=0.4, velocity_method=7), REC
+
+
+def wind_loglaw_upwind():
+    """The log law (kappa 0.41, z0 0.05 m from logwind.dat) with upwind
+    (backward-difference) velocity advection, porous ground."""
+    layer = 5
+    c = _base(bc=(PML, POROUS, PML, PML, PML, PML), pore=(math.sqrt(1.8), 0.3, 2.0e5), velocity_coef=0.5,
+              velocity_method=7)
+    c.pore_Z = uniform_axis(layer + 2, -layer * D, D)
+    c.pore_dxyz = (D, D, D)
+    c.logwind = (0.41, 0.05)
+    c.advection = "upwind"
+    c.source = (0.5, 0.55, 0.15)
+    return c, REC
+
+
+def wind_vortex_upwind():
+    """The reference's vortex profile (method 2, V and W components) with
+    upwind velocity advection and the east TDBC."""
+    c = _base(velocity_coef=0.0, velocity_method=2, bc=(PML, RIGID, TDBC, PML, PML, PML), pore=(1.79, 0.877, 5.1e4))
+    c.advection = "upwind"
+    return c, REC
+
+
+def hill_loglaw_upwind():
+    """Log-law wind over a hill (height above the local ground) with upwind
+    advection, PML on all six faces."""
+    c = _base(ni=16, nj=40, nk=26, bc=(PML,) * 6, pml_nodes=(5, 5, 5, 5, 4, 5), velocity_coef=0.4,
+              velocity_method=7)
+    _hill(c, h=0.12)
+    c.advection = "upwind"
+    c.source = _above(c, 0.4, 0.8, 0.35)
+    return c, [_above(c, 0.4, 1.1, 0.3), _above(c, 0.45, 1.4, 0.25), _above(c, 0.4, 0.5, 0.5)]
+
+
+EXT_CASES: Dict[str, Callable[[], Tuple[Case, List]]] = {
+    f.__name__: f for f in [wind_loglaw, wind_loglaw_upwind, wind_vortex_upwind, hill_loglaw_upwind]
+}
+
+
 CASES: Dict[str, Callable[[], Tuple[Case, List]]] = {
     f.__name__: f
     for f in [pml_rigid, tdbc_east, porous_ground, porous_tdbc_fine_pore, south_pml_all_faces, front_only_pml,
