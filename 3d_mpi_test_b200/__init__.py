@@ -35,7 +35,7 @@ F64, F32 = 0, 1
 EXPORTS = (
     "fdtd_create", "fdtd_destroy", "fdtd_dims", "fdtd_last_error", "fdtd_set_receivers", "fdtd_reset",
     "fdtd_run", "fdtd_advance", "fdtd_step_pressure", "fdtd_step_velocity", "fdtd_get_field",
-    "fdtd_set_field", "fdtd_get_psi", "fdtd_get_slab", "fdtd_state_elems", "fdtd_copy_state",
+    "fdtd_set_field", "fdtd_get_psi", "fdtd_get_ground_psi", "fdtd_get_slab", "fdtd_state_elems", "fdtd_copy_state",
     "fdtd_launch_count", "fdtd_last_device_ms", "fdtd_fb_step_noalloc", "fdtd_set_tiling", "fdtd_autotune",
     "fdtd_fft", "fdtd_spectrum", "fdtd_band_levels", "fdtd_save_restart", "fdtd_load_restart",
     "fdtd_write_contour", "fdtd_get_receivers", "fdtd_set_wait_limit", "fdtd_ensemble_create",
@@ -83,6 +83,7 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
         "fdtd_get_field": ([vp, i, i, dp], i),
         "fdtd_set_field": ([vp, i, i, dp], i),
         "fdtd_get_psi": ([vp, dp], i),
+        "fdtd_get_ground_psi": ([vp, dp], i),
         "fdtd_get_slab": ([vp, i, i, dp, ip], i),
         "fdtd_state_elems": ([vp], ctypes.c_size_t),
         "fdtd_copy_state": ([vp, i, vp], i),
@@ -216,6 +217,12 @@ class Airpore:
     def psi(self) -> np.ndarray:
         out = np.zeros((self.I, self.K, 6), dtype=np.float64)
         self._check(self._L.fdtd_get_psi(self._h, _dp(out)))
+        return out
+
+    def ground_psi(self) -> np.ndarray:
+        """Impedance-ground TDBC state [i][j][6] (tdbc_ground.dat), FP64."""
+        out = np.zeros((self.I, self.J, 6), dtype=np.float64)
+        self._check(self._L.fdtd_get_ground_psi(self._h, _dp(out)))
         return out
 
     def slabs(self):

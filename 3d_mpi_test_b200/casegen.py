@@ -21,6 +21,7 @@ lines positionally (``infile.ignore(100, '\\n')``).
 from __future__ import annotations
 
 import dataclasses
+import importlib
 import math
 import os
 from dataclasses import dataclass, field
@@ -101,6 +102,9 @@ class Case:
     # velocity advection by the mean wind (extension, advection.dat): None or
     # "reference" (forward differences) or "upwind" (backward differences)
     advection: Optional[str] = None
+    # impedance ground (extension, tdbc_ground.dat): the rigid south face
+    # becomes a 6-pole TDBC, (Zinf, tau, a[6], r[6]); ground.fit_tdbc makes one
+    ground_tdbc: Optional[Tuple[float, float, Sequence[float], Sequence[float]]] = None
 
     # ------------------------------------------------------------------ #
     @property
@@ -210,6 +214,13 @@ class Case:
             if self.advection not in ("reference", "upwind"):
                 raise ValueError("advection must be 'reference' or 'upwind'")
             files["advection.dat"] = self.advection + "\n"
+        if self.ground_tdbc is not None:
+            Zinf, tau, a, r = self.ground_tdbc
+            if len(a) != 6 or len(r) != 6:
+                raise ValueError("the ground TDBC has six poles")
+            files["tdbc_ground.dat"] = (f"{_fmt(float(Zinf))} {_fmt(float(tau))}\n"
+                                        + " ".join(_fmt(float(x)) for x in a) + "\n"
+                                        + " ".join(_fmt(float(x)) for x in r) + "\n")
         if self.logwind is not None:
             files["logwind.dat"] = f"{_fmt(float(self.logwind[0]))} {_fmt(float(self.logwind[1]))}\n"
         for name, txt in files.items():
@@ -417,22 +428,44 @@ def ensemble_member(seed: int, index: int, d: float = 0.1, pml: int = 10, layer:
     return case, receivers, params
 
 
-def moving_window(ni=256, window=1024, nk=192, total=4096, d=0.05, pml=20, trail=11, ratio=0.05, steps=20000):
-    """The long-range workload's shape: a window of `window` range nodes
-    (Y/j) x `ni` transverse x `nk` height moving over `total` range nodes
-    with the reference's moving frame (calculation_2D.cpp:405-496,
-    air.cpp:2447-2730; lead = trail, frames of trail - 1 cells, the first
-    frame shortened by `ratio`), rigid ground, PML on the other five faces,
-    no wind, Gaussian pulse at 1.5 m, receivers every 5 m at 1.5 m height."""
+def moving_window(ni=256, window=1024, nk=192, total=11264, d=0.05, pml=20, trail=11, ratio=0.05, steps=20000,
+                  ustar: Optional[float] = 0.4, sigma: Optional[float] = 50e3):
+    """The long-range configuration: a window of `window` range nodes (Y/j)
+    x `ni` transverse x `nk` height moving over `total` range nodes with the
+    reference's moving frame (calculation_2D.cpp:405-496,
+    air.cpp:2447-2730; lead = trail, frames of trail - 1 cells that follow
+    the pulse at c0, the first frame shortened by `ratio`; 11264 nodes keep
+    the window moving through 20000 steps), PML on the top, front and back
+    faces, rigid leading and trailing faces, Gaussian pulse at 1.5 m,
+    receivers every 5 m to 100 m at 1.5 m height. The frame moves at c0, so
+    no wave reaches the leading face and the waves reflected at the
+    trailing face leave the window at the next shifts; PML layers at those
+    faces grow without bound under the reference's moving frame (it moves
+    the x and z layers' integrals with the fields and leaves the y layers'
+    in place, air.cpp:2522-2729). With `ustar` the log-law wind V = (u*/0.41) ln(z / 0.01 m)
+    (method 7, logwind.dat) advects the velocity by backward differences
+    (advection.dat: the reference's forward differences grow without bound
+    under a log profile); with `sigma` the ground is the 6-pole TDBC fitted
+    to Miki's impedance at that flow resistivity on this time step
+    (tdbc_ground.dat), otherwise rigid."""
     c0, rho0, gamma = 343.0, 1.2, 1.4
+    dt = 0.5 * d / c0
     case = Case(
         X=uniform_axis(ni, 0.0, d), Y=uniform_axis(total, 0.0, d), Z=uniform_axis(nk, 0.0, d),
-        pml_nodes=(pml, pml, pml, pml, 0, pml), gauss_width=6 * d, bc=(PML, RIGID, PML, PML, PML, PML),
+        pml_nodes=(pml, pml, 0, 0, 0, pml), gauss_width=6 * d, bc=(PML, RIGID, RIGID, RIGID, PML, PML),
         time_domain=steps, gamma=gamma, P0=rho0 * c0 * c0 / gamma, c0=c0, pml_y=(2.0, 1000.0, 0),
         source=(round(ni // 2 * d, 9), round((pml + 20) * d, 9), 1.5),
-        receiver=(round(ni // 2 * d, 9), 5.0, 1.5), dt=0.5 * d / c0,
+        receiver=(round(ni // 2 * d, 9), 5.0, 1.5), dt=dt,
         mf_jmax=window, mf_lead=trail, mf_trail=trail, mf_judge=1, mf_ratio=ratio, ijkmax=total,
     )
+    if ustar:
+        case.velocity_method, case.velocity_coef = 7, ustar
+        case.logwind = (0.41, 0.01)
+        case.advection = "upwind"
+    if sigma:
+        ground = importlib.import_module(__package__ + ".ground")
+        fit = ground.fit_tdbc(sigma, dt=dt)
+        case.ground_tdbc = (fit.Zinf, fit.tau, tuple(fit.a), tuple(fit.r))
     xc = round(ni // 2 * d, 9)
     receivers = [(xc, float(r), 1.5) for r in range(5, int(total * d) - 5, 5)][:20]
     return case, receivers

@@ -137,6 +137,11 @@ int fdtd_get_psi(fdtd_solver* h, double* out) {
     return guard([&] { h->s->get_psi(out); });
 }
 
+int fdtd_get_ground_psi(fdtd_solver* h, double* out) {
+    if (!h || !out) return bad("null argument");
+    return guard([&] { h->s->get_ground_psi(out); });
+}
+
 int fdtd_get_slab(fdtd_solver* h, int s, int comp, double* out, int* dims) {
     if (!h || !dims) return bad("null argument");
     int present = 0;

@@ -980,4 +980,60 @@ __global__ void k_shift_rows(R* a, int rows, int nj, int sh, int lead, int tempJ
     if (west_copy) row[0] = row[1];
 }
 
+// Impedance ground (extension; the reference's TDBC acts on the east face
+// only, calculation_2D.cpp:986-1017). On the rigid south face w(k = 1) is
+// the face velocity: the pressure update at k = 1 takes w(2) - w(1) and the
+// rigid face holds it by the copy p(0) = p(1). After a step of the FB_p_v
+// scheme this kernel sets w(k = 1) at every interior node from the step's
+// new pressure p(k = 1) with the east face's recursion and the ground's
+// poles: v_n = den (p / Z - sum e_q psi_q) is the velocity into the ground,
+// w = -v_n, psi_q <- e_q psi_q + adt_q v_n. The interior node's thread also
+// writes the face nodes whose copies (calculation_2D.cpp:777-864, order N E
+// W F B S) end up holding its value, and recomputes the PML integral of w
+// at every node it writes from the value read this step (air::Update_PML_Qvw,
+// air.cpp:2323-2386), so the state equals an in-step override exactly.
+struct GroundC {
+    double* psi;  // [q][i][j], row pitch NJP, FP64
+    double e[6], adt[6], den, Z;
+};
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_ground_tdbc(__grid_constant__ const Dev<R> d, GroundC gc, int par) {
+    const int j = 1 + static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
+    const int i = 1 + static_cast<int>(blockIdx.y * blockDim.y + threadIdx.y);
+    if (j > d.NJ - 2 || i > d.NI - 2) return;
+    // after a step counters[next parity] holds the next step index
+    const int step = d.counters[par ^ 1] - 1;
+    const bool y1_on = step + 1 >= d.pml_y_time;
+    const int g = d.gOff + 1;  // air k = 1
+    const double p = static_cast<double>(d.p_out[d.ix(g, i, j)]);
+    const size_t qs = static_cast<size_t>(d.NI) * d.NJP;
+    double* ps = gc.psi + static_cast<size_t>(i) * d.NJP + j;
+    double pv[6];
+    double mem = 0.0;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+        pv[q] = ps[q * qs];
+        mem += gc.e[q] * pv[q];
+    }
+    const double vn = gc.den * (p / gc.Z - mem);
+#pragma unroll
+    for (int q = 0; q < 6; ++q) ps[q * qs] = gc.e[q] * pv[q] + gc.adt[q] * vn;
+    const R wv = static_cast<R>(-vn);
+    const int ia = i == 1 ? 0 : i, ib = i == d.NI - 2 ? d.NI - 1 : i;
+    const int ja = j == 1 ? 0 : j, jb = j == d.NJ - 2 ? d.NJ - 1 : j;
+    for (int ii = ia; ii <= ib; ++ii)
+        for (int jj = ja; jj <= jb; ++jj) {
+            d.w_out[d.ix(g, ii, jj)] = wv;
+#pragma unroll
+            for (int s = 0; s < 6; ++s) {
+                const Slab<R>& S = d.sl[s];
+                if (S.ni == 0 || (s == 2 && !y1_on)) continue;
+                if (!S.holds_i(ii) || !S.holds_j(jj) || !S.holds_k(1)) continue;
+                const int q = S.q(ii, jj, 1);
+                S.wr[2][q] = S.rd[2][q] + d.dt * wv;
+            }
+        }
+}
+
 }  // namespace fdtd

@@ -195,6 +195,17 @@ std::string parse_reference_case(const std::string& dir, ReferenceInput& in) {
         if (w == "upwind") in.upwind_advection = true;
         else if (w != "reference") return "advection.dat must hold 'upwind' or 'reference'";
     }
+    if (slurp(dir + "/tdbc_ground.dat", tt)) {
+        Reader t{tt};
+        in.g_zinf = t.d();
+        in.g_tau = t.d();
+        bool bad = false;
+        for (double& v : in.g_a) { v = t.d(); bad = bad || !(v >= 0.0); }
+        for (double& v : in.g_r) { v = t.d(); bad = bad || !(v >= 0.0); }
+        if (t.fail || bad || !(in.g_zinf > 0.0) || !(in.g_tau > 0.0))
+            return "tdbc_ground.dat must hold Zinf > 0, tau > 0, six a >= 0 and six r >= 0";
+        in.ground_tdbc = true;
+    }
     return "";
 }
 

@@ -65,6 +65,11 @@ struct ReferenceInput {
     // "reference" forward differences as air.cpp:1476-1949, or "upwind"
     // backward differences)
     bool upwind_advection = false;
+    // impedance ground (extension, optional tdbc_ground.dat: Zinf tau, six a,
+    // six r): the rigid south face becomes a 6-pole TDBC with the east
+    // face's recursion (calculation_2D.cpp:986-1017) and these poles
+    bool ground_tdbc = false;
+    double g_zinf = 0.0, g_tau = 0.0, g_a[6] = {0}, g_r[6] = {0};
 };
 
 // Returns "" on success, otherwise a one-line error.

@@ -21,6 +21,11 @@ void run_two_pass(bool pressure, bool wind, dim3 grd, dim3 blk, cudaStream_t s, 
 template <typename R>
 void run_shift_rows(cudaStream_t s, R* a, int rows, int nj, int sh, int lead, int tempJ, int J, int west_copy);
 
+// impedance ground after a step at parity par (fdtd_k_twopass.cu); d holds
+// the step's fused parameters (new level = 1 - par)
+template <typename R>
+void run_ground_tdbc(cudaStream_t s, const Dev<R>& d, const GroundC& gc, int par);
+
 // row marching kernel (fdtd_k_march.cu); VW columns per thread (4: FP32 only)
 template <typename R>
 const void* march_kernel_ptr(int VW, bool wind, bool xf);

@@ -161,6 +161,7 @@ class SolverImplBase {
     virtual void get_field(int medium, int comp, double* out) = 0;
     virtual void set_field(int medium, int comp, const double* in) = 0;
     virtual void get_psi(double* out) = 0;
+    virtual void get_ground_psi(double* out) = 0;
     virtual int get_slab(int s, int comp, double* out, int* dims) = 0;
     virtual size_t state_elems() const = 0;
     virtual void copy_state(int dir, void* host) = 0;
@@ -325,6 +326,7 @@ class SolverImpl final : public SolverImplBase {
             at += kTdA[q] * tb;
         }
         td_den_ = 1.0 / (1 + at);
+        build_ground();
         // wind presence (any non-zero value on frame 0)
         wind_on_ = false;
         for (int k = 0; k < Kair_ && !wind_on_; ++k)
@@ -353,6 +355,26 @@ class SolverImpl final : public SolverImplBase {
         zg_.assign(in.terrain.begin(), in.terrain.begin() + NJ_);
         for (double z : zg_)
             if (!(z < Htop_) || !std::isfinite(z)) fail(-2, "terrain reaches the top of the air grid");
+    }
+
+    // impedance ground (extension, tdbc_ground.dat): the rigid south face as a
+    // 6-pole TDBC with the east face's recursion (calculation_2D.cpp:986-1017)
+    // and the file's poles; t_bar = dt / tau as on the east face
+    void build_ground() {
+        ground_ = in.ground_tdbc;
+        if (!ground_) return;
+        if (in.south != BT_RIGID) fail(-2, "the impedance ground replaces a rigid south face (south code 1)");
+        if (in.scheme != FB_P_V) fail(-2, "the impedance ground is implemented for scheme FB_p_v");
+        if (terrain_) fail(-2, "the impedance ground does not run on a terrain-following grid");
+        const double tb = in.dt / in.g_tau;
+        double at = 0.0;
+        for (int q = 0; q < 6; ++q) {
+            gc_.e[q] = std::exp(-1 * in.g_r[q] * tb);
+            gc_.adt[q] = in.g_a[q] * tb;
+            at += in.g_a[q] * tb;
+        }
+        gc_.den = 1.0 / (1 + at);
+        gc_.Z = in.g_zinf;
     }
 
     // physical height of node (j, k) of the air (pore = false) or porous grid
@@ -608,6 +630,7 @@ class SolverImpl final : public SolverImplBase {
         if (mask_on_) h2d(d_mask_, mask_.data(), mask_.size());
         const size_t P = static_cast<size_t>(NI_) * Kair_ * 6;
         d_psi_[0] = track(dalloc<double>(P)); d_psi_[1] = track(dalloc<double>(P));
+        if (ground_) gc_.psi = track(dalloc<double>(ground_psi_n()));
         d_rec_node_ = track(dalloc<long long>(kMaxRec));
         d_counters_ = track(dalloc<int>(2));
         d_status_ = track(dalloc<int>(1));
@@ -768,6 +791,7 @@ class SolverImpl final : public SolverImplBase {
         const size_t P = static_cast<size_t>(NI_) * Kair_ * 6;
         zero(d_psi_[0], P * sizeof(double));
         zero(d_psi_[1], P * sizeof(double));
+        if (ground_) zero(gc_.psi, ground_psi_n() * sizeof(double));
         zero(d_counters_, 2 * sizeof(int));
         zero(d_status_, sizeof(int));
         par_ = 0;
@@ -1043,13 +1067,14 @@ class SolverImpl final : public SolverImplBase {
     }
 
     int launches_per_step() const {
+        const int g = ground_ ? 1 : 0;
         if (in.scheme == FB_P_V && fused_) {
-            if (!tile_on_) return 1;
+            if (!tile_on_) return 1 + g;
             int n = 0;
             for (int k = 0; k < kKinds; ++k) n += ntile_[k] ? 1 : 0;
-            return n;
+            return n + g;
         }
-        return 2;
+        return 2 + g;
     }
 
     template <bool XF>
@@ -1068,7 +1093,17 @@ class SolverImpl final : public SolverImplBase {
             launch_pass(false, par, true);
             launch_pass(true, par, false);
         }
+        if (ground_) launch_ground(par);
     }
+
+    // impedance ground after the step at parity par, on the handle's stream
+    void launch_ground(int par) {
+        run_ground_tdbc<R>(stream_, params_fused(par), gc_, par);
+        FDTD_CK(cudaGetLastError());
+        ++launches_;
+    }
+    size_t ground_psi_n() const { return static_cast<size_t>(6) * NI_ * NJP_; }
+    bool has_ground() const { return ground_; }
 
     static constexpr int kGraphSteps = 16;  // even: parity pattern repeats
 
@@ -1108,6 +1143,12 @@ class SolverImpl final : public SolverImplBase {
         const int rows = NI_ * NG_;
         for (int c = 0; c < 4; ++c) {
             run_shift_rows<R>(stream_, F_[par_][c], rows, NJP_, sh, lead, tempJ, NJ_, c == 3 ? 1 : 0);
+            FDTD_CK(cudaGetLastError());
+            ++launches_;
+        }
+        // the impedance ground's state moves with the frame like the fields
+        if (ground_) {
+            run_shift_rows<double>(stream_, gc_.psi, 6 * NI_, NJP_, sh, lead, tempJ, NJ_, 0);
             FDTD_CK(cudaGetLastError());
             ++launches_;
         }
@@ -1221,6 +1262,7 @@ class SolverImpl final : public SolverImplBase {
         FDTD_CK(cudaSetDevice(device_));
         if (in.scheme != FB_P_V) fail(-2, "half steps are exposed for FB_p_v only");
         launch_pass(false, par_, false);
+        if (ground_) launch_ground(par_);
         par_ ^= 1;
         ++steps_;
         ++n_in_frame_;
@@ -1277,6 +1319,17 @@ class SolverImpl final : public SolverImplBase {
 
     void get_psi(double* out) override {
         d2h(out, d_psi_[par_], sizeof(double) * NI_ * Kair_ * 6);
+    }
+
+    // impedance-ground state as [i][j][6] (device layout [q][i][j])
+    void get_ground_psi(double* out) override {
+        if (!ground_) fail(-2, "the case has no impedance ground (tdbc_ground.dat)");
+        std::vector<double> h(ground_psi_n());
+        d2h(h.data(), gc_.psi, h.size() * sizeof(double));
+        for (int i = 0; i < NI_; ++i)
+            for (int j = 0; j < NJ_; ++j)
+                for (int q = 0; q < 6; ++q)
+                    out[(static_cast<size_t>(i) * NJ_ + j) * 6 + q] = h[(static_cast<size_t>(q) * NI_ + i) * NJP_ + j];
     }
 
     // ------------------------------------------------------- contour
@@ -1366,6 +1419,7 @@ class SolverImpl final : public SolverImplBase {
     // moving frame and the TDBC too.
     void save_restart(const std::string& path) override {
         FDTD_CK(cudaSetDevice(device_));
+        if (ground_) fail(-2, "restart files do not carry the impedance ground's state");
         std::ofstream f(path, std::ios::out | std::ios::trunc | std::ios::binary);
         if (!f) fail(-1, "cannot write restart file " + path);
         f << 1 << " " << 0 << " " << steps_ << std::endl;
@@ -1435,6 +1489,7 @@ class SolverImpl final : public SolverImplBase {
     // integrals and Psi restart from zero in frame 0.
     void load_restart(const std::string& path, bool reference_semantics) override {
         FDTD_CK(cudaSetDevice(device_));
+        if (ground_) fail(-2, "restart files do not carry the impedance ground's state");
         std::ifstream f(path, std::ios::in | std::ios::binary);
         if (!f) fail(-1, "cannot read restart file " + path);
         int size = 0, rank = 0, index = 0;
@@ -2085,6 +2140,8 @@ class SolverImpl final : public SolverImplBase {
     R *d_axA_ = nullptr, *d_ayA_ = nullptr, *d_axP_ = nullptr, *d_ayP_ = nullptr, *d_azG_ = nullptr;
     // terrain-following grid: elevation per column, air top, per (g, column) factors
     bool terrain_ = false;
+    bool ground_ = false;  // impedance ground (tdbc_ground.dat)
+    GroundC gc_{};
     std::vector<double> zg_;
     double Htop_ = 0.0;
     R *d_azT_ = nullptr, *d_zyT_ = nullptr;
@@ -2153,6 +2210,7 @@ void Solver::step_velocity() { impl_->step_velocity(); }
 void Solver::get_field(int m, int c, double* out) { impl_->get_field(m, c, out); }
 void Solver::set_field(int m, int c, const double* in) { impl_->set_field(m, c, in); }
 void Solver::get_psi(double* out) { impl_->get_psi(out); }
+void Solver::get_ground_psi(double* out) { impl_->get_ground_psi(out); }
 int Solver::get_slab(int s, int c, double* out, int* dims) { return impl_->get_slab(s, c, out, dims); }
 size_t Solver::state_elems() const { return impl_->state_elems(); }
 void Solver::copy_state(int dir, void* host) { impl_->copy_state(dir, host); }
@@ -2197,6 +2255,7 @@ class EnsembleImpl final : public EnsembleImplBase {
         device_ = mem_[0]->device();
         for (size_t a = 0; a < mem_.size(); ++a) {
             if (mem_[a]->device() != device_) fail(-5, "ensemble members must share one device");
+            if (mem_[a]->has_ground()) fail(-5, "an ensemble member cannot have an impedance ground");
             for (size_t b = 0; b < a; ++b)
                 if (mem_[a] == mem_[b]) fail(-5, "a solver appears twice in the ensemble");
         }

@@ -56,6 +56,8 @@ class Solver {
     void get_field(int medium, int comp, double* out);
     void set_field(int medium, int comp, const double* in);
     void get_psi(double* out);
+    // impedance-ground TDBC state [i][j][6], FP64 (tdbc_ground.dat)
+    void get_ground_psi(double* out);
     int get_slab(int s, int comp, double* out, int* dims);
     size_t state_elems() const;
     void copy_state(int dir, void* host);

@@ -67,6 +67,12 @@ std::vector<double> air::psi() const {
     return out;
 }
 
+std::vector<double> air::ground_psi() const {
+    std::vector<double> out(static_cast<size_t>(I_) * J_ * 6);
+    check(fdtd_get_ground_psi(h_, out.data()));
+    return out;
+}
+
 // ------------------------------------------------------------------- airpore
 airpore::airpore(const std::string& case_dir, Precision precision, int device) : device_(device) {
     check(fdtd_create(case_dir.c_str(), precision, device, &h_));

@@ -82,6 +82,8 @@ class air : public calculation_2D {
     std::vector<double> pml_slab(int s, char comp, std::array<int, 3>* dims = nullptr) const;
     // TDBC state Psi[i][k][6] (calculation_2D.h:71), FP64
     std::vector<double> psi() const;
+    // impedance-ground TDBC state Psi[i][j][6] (extension, tdbc_ground.dat)
+    std::vector<double> ground_psi() const;
 };
 
 // porous (porous.h): the Zwikker-Kosten ground grid
@@ -91,7 +93,8 @@ class porous : public calculation_2D {
 };
 
 // airpore (airpore.h:24-68): owns the device domain built from a case
-// directory (input.txt + coordi_*.dat [+ coordi_pore*.dat, terrain.dat])
+// directory (input.txt + coordi_*.dat [+ coordi_pore*.dat, terrain.dat,
+// logwind.dat, advection.dat, tdbc_ground.dat])
 class airpore {
    public:
     explicit airpore(const std::string& case_dir, Precision precision = FP64, int device = 0);

@@ -328,8 +328,10 @@ def run_ensemble(args, rank, world, local_rank):
     }
 
 
-WINDOW_WORKLOAD = ("moving window 256 (i) x 1024 (j) x 192 (k) = 50.3 M nodes over a 4096-node range, "
-                   "frames of 10 cells, rigid ground, 20-node PML, no wind, FP32")
+WINDOW_WORKLOAD = ("moving window 256 (i) x 1024 (j) x 192 (k) = 50.3 M nodes over an 11264-node range, "
+                   "frames of 10 cells following the pulse at c0, log-law wind u*=0.4 m/s kappa=0.41 z0=0.01 m "
+                   "(upwind advection), 6-pole TDBC ground fitted to Miki at 50 kPa s/m^2, 20-node PML on top, "
+                   "front and back, rigid leading and trailing faces, FP32 fields, FP64 TDBC state")
 
 
 def run_window(args, rank, world, local_rank):
@@ -370,7 +372,7 @@ def run_window(args, rank, world, local_rank):
     steps_total = args.steps * inner
     gcell = group.throughput(cells, steps_total, ms)
     ms = group.max_over_ranks(ms)
-    slab = 2 * 21 * 1024 * 192 + 2 * 256 * 21 * 192 + 256 * 1024 * 21  # x1 x2 y1 y2 z2 storage nodes
+    slab = 2 * 21 * 1024 * 192 + 256 * 1024 * 21  # x1 x2 z2 storage nodes
     bytes_step = cells * 8 * 4 + slab * 8 * 4
     achieved = bytes_step / (ms * 1e-3 / steps_total) / 1e9
     a.close()
@@ -388,6 +390,67 @@ def run_window(args, rank, world, local_rank):
                      "frac": round(achieved / hbm_peak, 4), "peak_kind": peak_kind,
                      "algorithmic_bytes_per_step": bytes_step},
         "gpu_launches": int(launches), "clocks": sampler.summary(),
+    }
+
+
+def run_window_full(args, local_rank):
+    """The long-range configuration run end to end once per precision:
+    `--window-steps` steps (20000) of the moving window with its wind and
+    ground, receivers every 5 m to 100 m at 1.5 m. Reports each run's
+    device rate, the FP32 receiver error against FP64 (rel L2 of p(t) and
+    dB per third-octave band, 50 Hz - 2 kHz), the peak pressure and the
+    FP64 band levels per receiver (written to --window-out as .npz)."""
+    import numpy as np
+    import torch
+
+    pkg = importlib.import_module("3d_mpi_test_b200")
+    casegen = importlib.import_module("3d_mpi_test_b200.casegen")
+    torch.cuda.set_device(local_rank)
+    tmp = tempfile.mkdtemp(prefix="bench_winfull_")
+    n = args.window_steps
+    case, rec = casegen.moving_window(steps=n)
+    d = case.write(os.path.join(tmp, "window"))
+    cells = case.NI * 1024 * case.NK
+    runs = {}
+    for prec in ("f32", "f64"):
+        a = pkg.Airpore(d, prec, device=local_rank)
+        a.set_receivers(rec)
+        a.reset(n)
+        sampler = ClockSampler(local_rank)
+        t0 = time.perf_counter()
+        with sampler:
+            r = a.advance(n)
+        wall = time.perf_counter() - t0
+        ms = a.last_device_ms()
+        p = a.field("p")
+        runs[prec] = {"rec": np.asarray(r), "ms": ms, "wall_s": wall, "gcell": cells * n / (ms * 1e-3) / 1e9,
+                      "p_max": float(np.abs(p).max()), "finite": bool(np.all(np.isfinite(p))),
+                      "clocks": sampler.summary(), "launches": a.launch_count()}
+        a.close()
+    fft_m = int(np.ceil(np.log2(n)))
+    lv = {k: pkg.band_levels(v["rec"].T, fft_m, case.dt) for k, v in runs.items()}
+    dl = np.abs(lv["f32"] - lv["f64"])
+    r32, r64 = runs["f32"]["rec"], runs["f64"]["rec"]
+    per_rec = np.linalg.norm(r32 - r64, axis=0) / np.maximum(np.linalg.norm(r64, axis=0), 1e-300)
+    if args.window_out:
+        np.savez(args.window_out, rec_f32=r32, rec_f64=r64, levels_f32=lv["f32"], levels_f64=lv["f64"],
+                 centres=np.asarray(pkg.THIRD_OCTAVE_50_2K), ranges=np.asarray([x[1] for x in rec]))
+    shutil.rmtree(tmp, ignore_errors=True)
+    return {
+        "metric": "Gcell-upd/s of the long-range configuration run end to end (FP32)",
+        "value": round(runs["f32"]["gcell"], 3), "unit": UNIT, "n_gpus": 1, "steps": n, "warmup": 0,
+        "higher_is_better": True, "dtype": "f32", "data": "synthetic (seeded case generator)",
+        "config": {"workload": WINDOW_WORKLOAD, "fb_steps": n, "receivers_m": [x[1] for x in rec]},
+        "f64_gcell": round(runs["f64"]["gcell"], 3),
+        "device_s": {k: round(v["ms"] / 1e3, 3) for k, v in runs.items()},
+        "wall_s": {k: round(v["wall_s"], 3) for k, v in runs.items()},
+        "finite": {k: v["finite"] for k, v in runs.items()},
+        "p_max_final": {k: v["p_max"] for k, v in runs.items()},
+        "rec_p_max": float(np.abs(r64).max()),
+        "fp32_error": {"rel_l2_all": float(np.linalg.norm(r32 - r64) / np.linalg.norm(r64)),
+                       "rel_l2_per_receiver_max": float(per_rec.max()),
+                       "band_db_max": float(dl.max()), "band_db_mean": float(dl.mean())},
+        "clocks": {k: v["clocks"] for k, v in runs.items()},
     }
 
 
@@ -685,6 +748,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tile", default="", help="rows,planes,threads,vector-width,ring-stages of the marching kernel (default: autotune)")
     ap.add_argument("--workload", default="domain", choices=["domain", "ensemble", "surrogate", "window"])
+    ap.add_argument("--window-steps", type=int, default=0,
+                    help="--workload window: run the configuration end to end for this many steps per precision "
+                         "instead of timing bench steps")
+    ap.add_argument("--window-out", default="", help="npz for the end-to-end window run's traces and band levels")
     ap.add_argument("--no-surrogate", action="store_true", help="skip the surrogate section of the domain line")
     ap.add_argument("--flat", action="store_true", help="the domain workload on flat ground (no hill)")
     ap.add_argument("--sur-queries", type=int, default=1_000_000, help="surrogate inference queries")
@@ -715,6 +782,8 @@ def main():
     try:
         if args.workload == "ensemble":
             line = run_ensemble(args, rank, world, local_rank)
+        elif args.workload == "window" and args.window_steps > 0:
+            line = run_window_full(args, local_rank) if rank == 0 else None
         elif args.workload == "window":
             line = run_window(args, rank, world, local_rank)
         elif args.workload == "surrogate":

@@ -27,6 +27,10 @@
  *   fdtd_set_field     write of the same arrays (restart input,
  *                      calculation_2D.cpp:522-545)
  *   fdtd_get_psi       calculation_2D::Psi (TDBC state, calculation_2D.h:71)
+ *   fdtd_get_ground_psi no counterpart: the state of the impedance-ground
+ *                      TDBC (optional tdbc_ground.dat), an extension that
+ *                      runs the east face's recursion (calculation_2D.cpp:
+ *                      986-1017) on the ground face with fitted poles
  *   fdtd_get_slab      air::Qux1..Qpz2 PML integrals (air.h:40-42)
  *   fdtd_get_receivers the receiver series airpore::get_output collects
  *                      through get_pressure (airpore.cpp:566-580)
@@ -96,6 +100,12 @@ int fdtd_set_field(fdtd_solver *h, int medium, int comp, const double *in);
 
 /* TDBC state [i][k][6] of the air grid (FP64). */
 int fdtd_get_psi(fdtd_solver *h, double *out);
+
+/* Impedance-ground TDBC state [i][j][6] (FP64) of a case with
+ * tdbc_ground.dat; FDTD_ERR_UNSUPPORTED without one. Extension: the
+ * reference's TDBC state exists for the east face only
+ * (calculation_2D.h:71). */
+int fdtd_get_ground_psi(fdtd_solver *h, double *out);
 
 /* PML integral slab s (0 x1, 1 x2, 2 y1, 3 y2, 4 z1, 5 z2), comp 0 u 1 v 2 w
  * 3 p, in the reference slab shape [d0][d1][d2]. dims receives the shape;

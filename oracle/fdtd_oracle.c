@@ -103,6 +103,11 @@ struct orc {
     /* receivers */
     int nrec;
     int *ri, *rj, *rk;
+    /* extension: impedance ground, a 6-pole TDBC on the rigid south face
+     * (case_dir/tdbc_ground.dat: Zinf tau a0..a5 r0..r5) */
+    int gtdbc;
+    double gZ, gtau, ga[6], gr[6];
+    double *gpsi; /* [i][j][6] */
 };
 
 #define IX(g, i, j, k) ((((size_t)(i)) * (size_t)(g)->J + (size_t)(j)) * (size_t)(g)->K + (size_t)(k))
@@ -1256,6 +1261,36 @@ static void update_psi(double *psi, double w, double dt)
 {
     for (int k = 0; k < 6; k++) psi[k] = exp(-1 * TD_R[k] * dt) * psi[k] + TD_A[k] * w * dt;
 }
+/* Impedance ground (extension; the reference's TDBC acts on the east face
+ * only). The face between the south nodes k = 0 and k = 1 is where w(k = 1)
+ * sits: the pressure update at k = 1 takes w(2) - w(1), and the rigid face
+ * holds it by the copy p(0) = p(1). The impedance face sets w(1) at every
+ * interior node from the new pressure p(1) with the east face's recursive
+ * convolution (calculation_2D.cpp:986-1017) and its own poles: the normal
+ * velocity into the ground is v_n = -w, p / Z = v_n + sum psi_q, and
+ * psi_q <- exp(-r_q dt') psi_q + a_q dt' v_n with dt' = dt / tau, i.e.
+ * Z(w) = Z_inf (1 + sum a_q / (r_q + i w tau)) for small dt'. Runs before
+ * the face copies, which then carry w(1) to the edge nodes. */
+static void bc_velocity_tdbc_ground(orc *o)
+{
+    grid *g = &o->air.g;
+    const double dtp = g->dt / o->gtau;
+    double e[6], adt = 0;
+    for (int q = 0; q < 6; q++) {
+        e[q] = exp(-1 * o->gr[q] * dtp);
+        adt += o->ga[q] * dtp;
+    }
+    for (int i = 1; i < g->I - 1; i++)
+        for (int j = 1; j < g->J - 1; j++) {
+            double *psi = &o->gpsi[((size_t)i * g->J + j) * 6];
+            double mem = 0;
+            for (int q = 0; q < 6; q++) mem += e[q] * psi[q];
+            const double vn = 1.0 / (1 + adt) * (g->pnn[IX(g, i, j, 1)] / o->gZ - mem);
+            g->wnn[IX(g, i, j, 1)] = -vn;
+            for (int q = 0; q < 6; q++) psi[q] = e[q] * psi[q] + o->ga[q] * dtp * vn;
+        }
+}
+
 static void bc_velocity_tdbc_east(grid *g, double Z, double tau)
 {
     const int I = g->I, J = g->J, K = g->K;
@@ -1375,6 +1410,7 @@ static void airpore_cal_velocity(orc *o)
     else if (o->scheme == S_FB_P_V) air_cal_fuvw(a, g->un, g->vn, g->wn, g->pnn, o->scheme);
     if (o->scheme == S_FB_V_P || o->scheme == S_FB_P_V) grid_accumulate_v(g);
     if (o->case_no != 1) return;
+    if (o->gtdbc) bc_velocity_tdbc_ground(o);
     bc_velocity(g, F_NORTH);
     if (o->bc_e == BT_TDBC) bc_velocity_tdbc_east(g, o->Zinf, o->tau);
     else bc_velocity(g, F_EAST);
@@ -1408,6 +1444,21 @@ static void airpore_set_moving_frame(orc *o, int MF)
 {
     /* airpore::SetMovingFrame, airpore.cpp:881-897 */
     grid_set_moving_frame(&o->air.g, MF);
+    if (o->gtdbc && MF != 0) { /* the ground state moves with the frame, like the fields */
+        grid *g = &o->air.g;
+        const int temp_J = g->mf.JMAX - g->mf.lead_DJ, sh = g->mf.trail_DJ - 1;
+        if (temp_J != 0)
+            for (int i = 0; i < g->I; i++)
+                for (int j = 0; j < g->J; j++) {
+                    double *d = &o->gpsi[((size_t)i * g->J + j) * 6];
+                    if (j < temp_J + 1 && j + g->mf.lead_DJ - 1 < g->J - 1) {
+                        const double *s = &o->gpsi[((size_t)i * g->J + j + sh) * 6];
+                        for (int q = 0; q < 6; q++) d[q] = s[q];
+                    } else if (j >= temp_J + 1) {
+                        for (int q = 0; q < 6; q++) d[q] = 0.0;
+                    }
+                }
+    }
     air_set_wind(&o->air, MF);
     air_set_q_move(&o->air, MF);
     if (o->has_pore) grid_set_moving_frame(&o->pore, MF);
@@ -1543,6 +1594,33 @@ orc *orc_create(const char *case_dir, char *err, int errlen)
             if (bad) { seterr(err, errlen, "logwind.dat must hold kappa > 0 and z0 > 0"); orc_destroy(o); return NULL; }
         }
     }
+    { /* optional case_dir/tdbc_ground.dat: Zinf tau a0..a5 r0..r5 */
+        char path[4096];
+        snprintf(path, sizeof path, "%s/tdbc_ground.dat", case_dir);
+        size_t n = 0;
+        char *t = slurp(path, &n);
+        if (t) {
+            rdr R = {t, n, 0, 0};
+            o->gZ = rd_d(&R); o->gtau = rd_d(&R);
+            int bad = 0;
+            for (int q = 0; q < 6; q++) { o->ga[q] = rd_d(&R); bad |= !(o->ga[q] >= 0); }
+            for (int q = 0; q < 6; q++) { o->gr[q] = rd_d(&R); bad |= !(o->gr[q] >= 0); }
+            bad |= R.fail || !(o->gZ > 0) || !(o->gtau > 0);
+            free(t);
+            if (bad) {
+                seterr(err, errlen, "tdbc_ground.dat must hold Zinf > 0, tau > 0, six a >= 0 and six r >= 0");
+                orc_destroy(o);
+                return NULL;
+            }
+            if (o->case_no != 1 || o->bc_s != BT_RIGID || o->scheme != S_FB_P_V || a->g.zg || a->g.K < 3) {
+                seterr(err, errlen, "the impedance ground needs a rigid south face, scheme FB_p_v and no terrain");
+                orc_destroy(o);
+                return NULL;
+            }
+            o->gtdbc = 1;
+            o->gpsi = zalloc((size_t)a->g.I * a->g.J * 6);
+        }
+    }
     size_t N = (size_t)a->g.I * a->g.J * a->g.K;
     a->Uav = zalloc(N); a->Vav = zalloc(N); a->Wav = zalloc(N);
     air_pml_setup(o);
@@ -1584,6 +1662,7 @@ void orc_destroy(orc *o)
     free(o->air.cr_uc);
     if (o->has_pore) grid_free(&o->pore);
     free(o->ri); free(o->rj); free(o->rk);
+    free(o->gpsi);
     free(o);
 }
 
@@ -1696,6 +1775,13 @@ int orc_set_field(orc *o, int m, int comp, const double *in)
 int orc_get_psi(const orc *o, double *out)
 {
     memcpy(out, o->air.g.psi, sizeof(double) * o->air.g.I * o->air.g.K * 6);
+    return 0;
+}
+
+int orc_get_ground_psi(const orc *o, double *out)
+{
+    if (!o->gtdbc) return -1;
+    memcpy(out, o->gpsi, sizeof(double) * o->air.g.I * o->air.g.J * 6);
     return 0;
 }
 

@@ -36,6 +36,8 @@ int orc_get_field(const orc *o, int medium, int comp, double *out);
 int orc_set_field(orc *o, int medium, int comp, const double *in);
 /* TDBC state [i][k][6] of the air grid. */
 int orc_get_psi(const orc *o, double *out);
+/* Impedance-ground TDBC state [i][j][6] (tdbc_ground.dat); -1 without one. */
+int orc_get_ground_psi(const orc *o, double *out);
 /* slab 0..5 = x1 x2 y1 y2 z1 z2; comp 0 u 1 v 2 w 3 p. dims[3] out.
  * Returns 1 if the slab exists, 0 if not. */
 int orc_get_slab(const orc *o, int slab, int comp, double *out, int *dims);

@@ -45,6 +45,7 @@ def lib():
         L.orc_get_field.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
         L.orc_set_field.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
         L.orc_get_psi.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
+        L.orc_get_ground_psi.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
         L.orc_get_slab.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                    ctypes.POINTER(ctypes.c_int)]
         L.orc_get_wind.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
@@ -117,6 +118,11 @@ class OracleCase:
         out = np.zeros((self.I, self.K, 6), dtype=np.float64)
         lib().orc_get_psi(self._h, _dp(out))
         return out
+
+    def ground_psi(self) -> Optional[np.ndarray]:
+        """Impedance-ground TDBC state [i][j][6], None without tdbc_ground.dat."""
+        out = np.zeros((self.I, self.J, 6), dtype=np.float64)
+        return out if lib().orc_get_ground_psi(self._h, _dp(out)) == 0 else None
 
     def slabs(self) -> Dict[str, Dict[str, np.ndarray]]:
         res: Dict[str, Dict[str, np.ndarray]] = {}

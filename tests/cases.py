@@ -5,6 +5,7 @@ to well under a second per case."""
 
 from __future__ import annotations
 
+import functools
 import importlib
 import math
 from typing import Callable, Dict, List, Tuple
@@ -347,6 +348,65 @@ def hill_loglaw_upwind():
 
 EXT_CASES: Dict[str, Callable[[], Tuple[Case, List]]] = {
     f.__name__: f for f in [wind_loglaw, wind_loglaw_upwind, wind_vortex_upwind, hill_loglaw_upwind]
+}
+
+
+# ----------------------------------------------------- impedance ground
+# Extension of the reference (its TDBC acts on the east face only): the
+# rigid south face as a 6-pole TDBC with poles fitted to Miki's impedance,
+# checked against the oracle only.
+ground = importlib.import_module("3d_mpi_test_b200.ground")
+
+
+@functools.lru_cache(maxsize=None)
+def miki_poles(sigma: float, dt: float = 0.5 * D / C0):
+    """(Zinf, tau, a, r) fitted to Miki at flow resistivity sigma on the
+    discrete recursion of time step dt."""
+    f = ground.fit_tdbc(sigma, dt=dt)
+    return (f.Zinf, f.tau, tuple(f.a), tuple(f.r))
+
+
+def ground_box():
+    """Miki ground at 50 kPa s/m^2 under a PML box."""
+    c = _base()
+    c.ground_tdbc = miki_poles(50e3)
+    c.source = (0.5, 0.55, 0.15)
+    return c, REC + [(0.5, 0.7, 0.05)]
+
+
+def ground_rigid_sides():
+    """Miki ground at 200 kPa s/m^2 with rigid east/west/front/back faces
+    (face copies of w at k = 1 on every side), PML top."""
+    c = _base(bc=(PML, RIGID, RIGID, RIGID, RIGID, RIGID), pml_nodes=(0, 0, 0, 0, 0, 5))
+    c.ground_tdbc = miki_poles(200e3)
+    c.source = (0.3, 0.4, 0.1)
+    return c, REC
+
+
+def ground_loglaw_tdbc_east():
+    """Config 3's physics on a small box: log-law wind with upwind
+    advection over the Miki ground, the east TDBC too, y1 PML switched on
+    late."""
+    c = _base(bc=(PML, RIGID, TDBC, PML, PML, PML), pore=(1.79, 0.877, 5.1e4), velocity_coef=0.4,
+              velocity_method=7, pml_y=(2.0, 1000.0, 13))
+    c.ground_tdbc = miki_poles(50e3)
+    c.logwind = (0.41, 0.01)
+    c.advection = "upwind"
+    c.source = (0.5, 0.55, 0.2)
+    return c, REC
+
+
+def ground_moving_frame():
+    """The moving frame over the Miki ground: the ground state moves with
+    the frame."""
+    c, rec = moving_frame()
+    c.ground_tdbc = miki_poles(50e3)
+    c.source = (0.5, 0.4, 0.1)
+    return c, rec
+
+
+GROUND_CASES: Dict[str, Callable[[], Tuple[Case, List]]] = {
+    f.__name__: f for f in [ground_box, ground_rigid_sides, ground_loglaw_tdbc_east, ground_moving_frame]
 }
 
 
