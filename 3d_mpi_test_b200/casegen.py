@@ -344,7 +344,7 @@ ENSEMBLE_SIZES = ((64, 512), (32, 192), (32, 96))  # NJ, NK, 3D NI: inclusive ra
 
 
 def ensemble_member(seed: int, index: int, d: float = 0.1, pml: int = 10, layer: int = 8, steps: int = 100,
-                    n_receivers: int = 8, sizes=ENSEMBLE_SIZES):
+                    n_receivers: int = 8, sizes=ENSEMBLE_SIZES, wind: str = "loglaw"):
     """Member ``index`` of the seeded batched-ensemble workload: one
     independent outdoor-sound solve whose size and physics are drawn from
     ``numpy.random.default_rng([seed, index])``:
@@ -363,8 +363,13 @@ def ensemble_member(seed: int, index: int, d: float = 0.1, pml: int = 10, layer:
       ground half way down the range, made with the reference's sphere
       inclusion (curve_judge 1, air.cpp:1019-1031) and its canopy
       parameters; heights under two cells leave it out;
-    - logarithmic wind V(z) = b ln(z / 0.1 + 1) (velocity_method 5,
-      air.cpp:175-177) with b = u* / 0.4 and u* uniform in 0..0.6 m/s.
+    - wind with u* uniform in 0..0.6 m/s: ``wind="loglaw"`` the log law
+      V(z) = (u*/0.41) ln(z / 0.01 m) (method 7) with upwind velocity
+      advection (advection.dat), which stays bounded over long runs;
+      ``wind="reference"`` the reference's V(z) = b ln(z / 0.1 + 1)
+      (velocity_method 5, air.cpp:175-177) with b = u* / 0.4 and its
+      forward-difference advection, which grows without bound after a few
+      thousand steps (the row marching kernels run only this one).
 
     Uniform spacing ``d``, PML of ``pml`` nodes on every air face but the
     ground, CFL 0.5. ``sizes`` replaces the three node-count ranges (small
@@ -412,6 +417,10 @@ def ensemble_member(seed: int, index: int, d: float = 0.1, pml: int = 10, layer:
         dt=0.5 * d / c0, velocity_coef=ustar / 0.4, velocity_method=5,
         pore_Z=uniform_axis(layer + 2, -layer * d, d), pore_dxyz=(d, d, d),
     )
+    if wind == "loglaw":
+        case.velocity_method, case.velocity_coef, case.advection = 7, ustar, "upwind"
+    elif wind != "reference":
+        raise ValueError("wind must be 'loglaw' or 'reference'")
     # hill: nodes of its bounding box, snapped to the grid, below the top PML
     r_cells = int(round(hill_h / d))
     r_cells = min(r_cells, nk - pml - 4, (nj - 2 * pml) // 4)

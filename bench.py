@@ -242,7 +242,7 @@ def run_ensemble(args, rank, world, local_rank):
     specs, cells, mem = [], 0, []
     t_setup = time.perf_counter()
     for i in range(args.members):
-        c, rec, p = casegen.ensemble_member(rank, i, steps=horizon)
+        c, rec, p = casegen.ensemble_member(rank, i, steps=horizon, wind="reference" if args.ens_mode == 0 else "loglaw")
         d = c.write(os.path.join(tmp, f"m{i:03d}"))
         specs.append((d, rec, p))
         cells += c.NI * c.NJ * (c.NK + len(c.pore_Z))
@@ -251,7 +251,9 @@ def run_ensemble(args, rank, world, local_rank):
         a.reset(horizon)
         mem.append(a)
     ens = pkg.Ensemble(mem, mode=args.ens_mode)
-    tile = ens.autotune(3)
+    # mode 0 runs the batched row marching kernel, whose tiles the ensemble
+    # autotuner picks; in mode 1 every member runs its own tiled kernels
+    tile = ens.autotune(3) if args.ens_mode == 0 else None
     for a in mem:
         a.reset(horizon)
     setup_s = time.perf_counter() - t_setup
@@ -315,7 +317,7 @@ def run_ensemble(args, rank, world, local_rank):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded ensemble generator)",
         "config": {"workload": ENS_WORKLOAD, "members": args.members, "cells_per_fb_step": cells,
                    "inner_fb_steps_per_bench_step": inner, "l2": "inputs larger than L2",
-                   "tile_rows_planes": list(tile), "launch_groups": info["groups"],
+                   "tile_rows_planes": list(tile) if tile else "per-member tiled kernels", "launch_groups": info["groups"],
                    "launch_mode": ["one batched launch per group per step",
                                    "each member's own launch, 16 streams"][args.ens_mode],
                    "blocks_per_fb_step": info["blocks_per_step"], "setup_s": round(setup_s, 1),
@@ -544,6 +546,42 @@ def run_surrogate(queries: int = 1_000_000, members: int = 5, steps: int = 12000
     }
 
 
+def run_profile(args, local_rank):
+    """One precision of the headline workload for a profiler: autotuned
+    tiles (or --tile-shapes), two warm-up FB steps, then --profile-steps FB
+    steps between cudaProfilerStart and cudaProfilerStop (ncu
+    --profile-from-start off captures just those). Prints the tile shapes
+    and the device time of the profiled steps."""
+    import torch
+
+    pkg = importlib.import_module("3d_mpi_test_b200")
+    torch.cuda.set_device(local_rank)
+    tmp = tempfile.mkdtemp(prefix="bench_prof_")
+    case_dir, rec, cells, case = make_case(tmp)
+    a = pkg.Airpore(case_dir, args.profile_prec, device=local_rank)
+    if args.tile_shapes:
+        for kind, spec in enumerate(args.tile_shapes.split(";")):
+            if spec:
+                a.set_tile_shape(kind, *(int(x) for x in spec.split(",")))
+    else:
+        a.autotune(10)
+    a.set_receivers(rec)
+    a.reset(args.profile_steps + 8)
+    a.advance(2)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()
+    a.advance(args.profile_steps)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    ms = a.last_device_ms()
+    out = {"profile": args.profile_prec, "fb_steps": args.profile_steps, "device_ms": round(ms, 4),
+           "gcell": round(cells * args.profile_steps / (ms * 1e-3) / 1e9, 3), "tile_shapes": a.tile_shape(),
+           "workload": FLAT_WORKLOAD if FLAT else WORKLOAD}
+    a.close()
+    shutil.rmtree(tmp, ignore_errors=True)
+    return out
+
+
 def run_gpu(args, rank, world, local_rank):
     import numpy as np
     import torch
@@ -752,6 +790,11 @@ def main():
                     help="--workload window: run the configuration end to end for this many steps per precision "
                          "instead of timing bench steps")
     ap.add_argument("--window-out", default="", help="npz for the end-to-end window run's traces and band levels")
+    ap.add_argument("--profile-steps", type=int, default=0,
+                    help="run this many FB steps of the headline workload between cudaProfilerStart/Stop and exit")
+    ap.add_argument("--profile-prec", default="f32", choices=["f32", "f64"])
+    ap.add_argument("--tile-shapes", default="",
+                    help="--profile-steps: 'rows,vectors,planes,stages' per tile kind (full;lean;pml) instead of autotuning")
     ap.add_argument("--no-surrogate", action="store_true", help="skip the surrogate section of the domain line")
     ap.add_argument("--flat", action="store_true", help="the domain workload on flat ground (no hill)")
     ap.add_argument("--sur-queries", type=int, default=1_000_000, help="surrogate inference queries")
@@ -780,7 +823,9 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     try:
-        if args.workload == "ensemble":
+        if args.profile_steps > 0:
+            line = run_profile(args, local_rank) if rank == 0 else None
+        elif args.workload == "ensemble":
             line = run_ensemble(args, rank, world, local_rank)
         elif args.workload == "window" and args.window_steps > 0:
             line = run_window_full(args, local_rank) if rank == 0 else None

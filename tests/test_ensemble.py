@@ -35,10 +35,11 @@ def rel(a, b):
     return float(np.linalg.norm(a - b) / n) if n else float(np.linalg.norm(a - b))
 
 
-def _members(tmp_path, n, steps, seed=11):
+def _members(tmp_path, n, steps, seed=11, wind="loglaw"):
     out = []
     for i in range(n):
-        c, rec, p = casegen.ensemble_member(seed, i, pml=4, layer=4, steps=steps, n_receivers=3, sizes=SMALL)
+        c, rec, p = casegen.ensemble_member(seed, i, pml=4, layer=4, steps=steps, n_receivers=3, sizes=SMALL,
+                                            wind=wind)
         d = str(tmp_path / f"m{i}")
         c.write(d)
         out.append((d, rec, p))
@@ -108,7 +109,9 @@ def _launches_per_step(case_dir, precision, tile) -> int:
                                                  ("f64", (3, 5, 32, 2, 5), 1)])
 def test_batch_equals_single_solves(precision, tile, mode, tmp_path):
     steps = 37  # a graph of 16 steps twice plus 5 single launches
-    ms = _members(tmp_path, 6, steps)
+    # the row marching kernels (mode 0, explicit tilings) run only the
+    # reference's forward-difference advection
+    ms = _members(tmp_path, 6, steps, wind="reference" if (mode == 0 or tile) else "loglaw")
     mem = []
     for d, rec, _ in ms:
         a = pkg.Airpore(d, precision)
@@ -195,7 +198,7 @@ def test_unsupported_members_are_rejected(tmp_path):
 @pytest.mark.gpu
 def test_ensemble_autotune_keeps_results(tmp_path):
     steps = 20
-    ms = _members(tmp_path, 4, steps, seed=2)
+    ms = _members(tmp_path, 4, steps, seed=2, wind="reference")
     mem = []
     for d, rec, _ in ms:
         a = pkg.Airpore(d, "f32")
