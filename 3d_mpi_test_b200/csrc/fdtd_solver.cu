@@ -1721,6 +1721,21 @@ class SolverImpl final : public SolverImplBase {
         if (xa == 0) rc.push_back(1);  // a face row with no x layer beside it: own segment
         if (xb == NI_) rc.push_back(NI_ - 2);
         if (ya == 0) vc.push_back(1);
+        // the inclusion mask's box, widened by two rows, two column vectors
+        // and two planes (a tile also computes the pressure of its halo row,
+        // halo vector and warm-up plane), is cut out: only the tiles inside
+        // it need the generic kernel's mask terms. A face row or column
+        // computes at its clamped neighbour, so a box that reaches the
+        // first or last interior row / vector takes the face with it.
+        std::array<int, 2> mr{0, 0}, mv{0, 0}, mg{0, 0};
+        if (mask_on_) {
+            mr = {mi0_ - 2 <= 1 ? 0 : mi0_ - 2, mi1_ + 3 >= NI_ - 1 ? NI_ : mi1_ + 3};
+            mv = {mj0_ / V - 2 <= 1 ? 0 : mj0_ / V - 2, mj1_ / V + 3 >= ve ? nvec : mj1_ / V + 3};
+            mg = {std::max(gOff_ + mk0_ - 2, 1), std::min(gOff_ + mk1_ + 3, NG_ - 1)};
+            rc.push_back(mr[0]); rc.push_back(mr[1]);
+            vc.push_back(mv[0]); vc.push_back(mv[1]);
+            gc.push_back(mg[0]); gc.push_back(mg[1]);
+        }
         const auto rows = segments(rc, 0, NI_);
         const auto vecs = segments(vc, 0, nvec);
         const auto planes = segments(gc, 1, NG_ - 1);
@@ -1740,7 +1755,10 @@ class SolverImpl final : public SolverImplBase {
                     const bool vy1 = vr[1] <= ya, vy2 = vr[0] >= yb;
                     const bool gz = pr[1] <= za || pr[0] >= zb;
                     int kind;
-                    if (mask_on_ || (vr[1] > ve && east_generic) || (vy1 && vy2) || (vr[0] < ya && vr[1] > yb)) {
+                    const bool in_mask = mask_on_ && overlap(rr[0], rr[1], mr[0], mr[1]) > 0 &&
+                                         overlap(vr[0], vr[1], mv[0], mv[1]) > 0 &&
+                                         overlap(pr[0], pr[1], mg[0], mg[1]) > 0;
+                    if (in_mask || (vr[1] > ve && east_generic) || (vy1 && vy2) || (vr[0] < ya && vr[1] > yb)) {
                         kind = 0;
                     } else {
                         const int lm = (rx ? kLmX : 0) | (vy1 || vy2 ? kLmY : 0) | (gz ? kLmZ : 0);
@@ -2077,6 +2095,15 @@ class SolverImpl final : public SolverImplBase {
         FDTD_CK(cudaStreamSynchronize(stream_));
         return std::max(0, std::min(n, mf_limit_ - n_in_frame_));
     }
+    // thread blocks one fused step launches
+    long long blocks_per_step() const {
+        if (tile_on_) {
+            long long n = 0;
+            for (int k = 0; k < kKinds; ++k) n += ntile_[k];
+            return n;
+        }
+        return static_cast<long long>(tiling_.nrb) * tiling_.nchunk;
+    }
     BatchView batch_view() const {
         BatchView v{};
         v.dev[0] = params_fused(0);
@@ -2352,7 +2379,10 @@ class EnsembleImpl final : public EnsembleImplBase {
     }
     std::array<long long, 2> shape() const override {
         long long blocks = 0;
-        for (const Group& g : groups_) blocks += static_cast<long long>(g.work.size());
+        if (mode_ == 1)
+            for (const SolverImpl<R>* m : mem_) blocks += m->blocks_per_step();
+        else
+            for (const Group& g : groups_) blocks += static_cast<long long>(g.work.size());
         return {static_cast<long long>(groups_.size()), blocks};
     }
 
