@@ -44,7 +44,7 @@ EXPORTS = (
     # include/fdtd_surrogate.h (signatures in surrogate.py)
     "fdtd_tc_gemm", "fdtd_net_create", "fdtd_net_destroy", "fdtd_net_n_params", "fdtd_net_get_params",
     "fdtd_net_set_params", "fdtd_net_set_data", "fdtd_net_get_normalization", "fdtd_net_set_normalization",
-    "fdtd_net_train", "fdtd_net_gradients", "fdtd_net_predict", "fdtd_net_predict_device", "fdtd_net_info",
+    "fdtd_net_train", "fdtd_net_gradients", "fdtd_net_predict", "fdtd_net_predict_device", "fdtd_net_set_fused", "fdtd_net_info",
     "fdtd_net_ensemble_predict", "fdtd_ray_features", "fdtd_net_ensemble_predict_rays",
 )
 

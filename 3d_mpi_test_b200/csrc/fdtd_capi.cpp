@@ -412,6 +412,14 @@ int fdtd_net_ensemble_predict_rays(fdtd_net* const* nets, int members, const flo
     });
 }
 
+int fdtd_net_set_fused(fdtd_net* h, int on, int* served) {
+    if (!h) return bad("null argument");
+    return guard([&] {
+        const bool ok = h->n->set_fused(on != 0);
+        if (served) *served = ok ? 1 : 0;
+    });
+}
+
 int fdtd_net_info(const fdtd_net* h, long long* launches, double* last_ms) {
     if (!h) return bad("null argument");
     if (launches) *launches = h->n->launches();

@@ -1029,33 +1029,29 @@ class SolverImpl final : public SolverImplBase {
     // kinds other than the generic full tiles run on streams of their own,
     // forked from and joined to it, so all launches of a step share the
     // device
-    void launch_fused(int par) {
+    void launch_fused(int par) { launch_fused_on(par, stream_); }
+
+    // one fused step at parity par on stream s (also an ensemble's stream);
+    // returns the kernels launched. Tiled: the kinds other than the generic
+    // full tiles run on this domain's kind streams, forked from s and
+    // joined back to it (as in launch_fused), so the kinds of one step
+    // share the device inside an ensemble too.
+    int launch_fused_on(int par, cudaStream_t s) {
         if (tile_on_) {
             cudaStream_t st[kKinds];
-            st[0] = stream_;
-            FDTD_CK(cudaEventRecord(ev_fork_, stream_));
+            st[0] = s;
+            FDTD_CK(cudaEventRecord(ev_fork_, s));
             for (int k = 1; k < kKinds; ++k) {
                 st[k] = kstream_[k];
                 if (ntile_[k]) FDTD_CK(cudaStreamWaitEvent(kstream_[k], ev_fork_, 0));
             }
-            launch_tiles(par, st);
+            const int n = launch_tiles(par, st);
             for (int k = 1; k < kKinds; ++k)
                 if (ntile_[k]) {
                     FDTD_CK(cudaEventRecord(ev_join_[k], kstream_[k]));
-                    FDTD_CK(cudaStreamWaitEvent(stream_, ev_join_[k], 0));
+                    FDTD_CK(cudaStreamWaitEvent(s, ev_join_[k], 0));
                 }
-        } else {
-            launch_fused_on(par, stream_);
-        }
-    }
-
-    // one fused step at parity par on stream s (also an ensemble's stream);
-    // returns the kernels launched
-    int launch_fused_on(int par, cudaStream_t s) {
-        if (tile_on_) {
-            cudaStream_t st[kKinds];
-            for (int k = 0; k < kKinds; ++k) st[k] = s;
-            return launch_tiles(par, st);
+            return n;
         }
         if (!old_ok_) fail(-2, "rows too wide for the row marching kernel");
         const Dev<R> d = params_fused(par);
@@ -1701,6 +1697,7 @@ class SolverImpl final : public SolverImplBase {
     // storage boxes next to them, so no tile is a single face sheet where a
     // PML layer borders the face.
     void build_tiles() {
+        ++tiles_gen_;
         const int V = kVecMax, nvec = NJP_ / V;
         for (int k = 0; k < 3; ++k) check_tile(tcfg_[k]);
         const int xa = I1_ ? I1_ + 1 : 0, xb = I2_ ? NI_ - 1 - I2_ : NI_;
@@ -2075,7 +2072,10 @@ class SolverImpl final : public SolverImplBase {
         bool xf;
         bool old_ok;  // the row marching kernel (batched launches) fits
         int par;
+        bool tile_on;   // the tiled kernels run the fused step
+        int tiles_gen;  // tile rebuild count
     };
+    bool tiled() const { return tile_on_; }
     int device() const { return device_; }
     int horizon() const { return horizon_; }
     // Readies the domain for lock-step steps taken by batched launches
@@ -2115,6 +2115,8 @@ class SolverImpl final : public SolverImplBase {
         v.xf = old_ok_ ? needs_xf(tiling_.VW) : true;
         v.old_ok = old_ok_;
         v.par = par_;
+        v.tile_on = tile_on_;
+        v.tiles_gen = tiles_gen_;
         return v;
     }
     // n steps were taken by batched launches
@@ -2185,6 +2187,7 @@ class SolverImpl final : public SolverImplBase {
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
     cudaGraphExec_t graph_exec_ = nullptr;
     bool graph_dirty_ = true;
+    int tiles_gen_ = 0;          // counts tile rebuilds (captured launches depend on the tiles)
     bool fused_ = false;
     bool old_ok_ = false;  // the row marching kernel fits this domain
     bool xf_ = true;  // marching kernel with the rarer features compiled in
@@ -2295,6 +2298,7 @@ class EnsembleImpl final : public EnsembleImplBase {
     ~EnsembleImpl() override {
         cudaSetDevice(device_);
         if (stream_) cudaStreamSynchronize(stream_);
+
         if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
         for (Group& g : groups_) release(g);
         for (cudaEvent_t e : mdone_) cudaEventDestroy(e);
@@ -2343,6 +2347,11 @@ class EnsembleImpl final : public EnsembleImplBase {
     std::array<int, 2> autotune(int nsteps) override {
         FDTD_CK(cudaSetDevice(device_));
         nsteps = std::max(nsteps, 1);
+        if (mode_ == 1) {
+            bool tiled = false;
+            for (SolverImpl<R>* m : mem_) tiled = tiled || m->tiled();
+            if (tiled) return autotune_tiles(nsteps);
+        }
         std::vector<int> saved;
         for (SolverImpl<R>* m : mem_) saved.push_back(m->horizon());
         const std::array<int, 3> TIs{2, 4, 8};
@@ -2361,6 +2370,52 @@ class EnsembleImpl final : public EnsembleImplBase {
         apply_tiling(best[0], best[1]);
         for (size_t i = 0; i < mem_.size(); ++i) mem_[i]->reset(saved[i]);
         return best;
+    }
+
+    // Mode 1 with tiled members: one set of tile shapes (full, lean, PML /
+    // face: rows, column vectors, planes, ring stages) for every member,
+    // picked from a few candidates by timing nsteps steps of the whole
+    // ensemble; returns the chosen set's lean rows and planes. A candidate
+    // a member cannot take (shared memory) is skipped. Every member ends
+    // reset to t = 0 with its horizon kept.
+    std::array<int, 2> autotune_tiles(int nsteps) {
+        using C = std::array<int, 4>;
+        struct Set { C full, lean, pml; };
+        std::vector<Set> sets;
+        if (sizeof(R) == 4)
+            sets = {{{8, 16, 8, 3}, {16, 8, 8, 3}, {8, 16, 8, 3}},       {{8, 16, 8, 3}, {8, 32, 8, 4}, {8, 16, 8, 3}},
+                    {{8, 16, 16, 3}, {8, 32, 16, 4}, {8, 16, 16, 3}},    {{8, 16, 16, 4}, {16, 16, 16, 4}, {8, 16, 16, 4}},
+                    {{8, 8, 16, 3}, {8, 16, 32, 4}, {8, 8, 16, 3}},      {{16, 8, 16, 3}, {16, 16, 32, 4}, {16, 8, 16, 3}}};
+        else
+            sets = {{{8, 16, 16, 3}, {8, 16, 32, 4}, {8, 16, 16, 3}},    {{4, 16, 16, 3}, {4, 64, 16, 4}, {4, 16, 16, 3}},
+                    {{8, 8, 16, 3}, {8, 32, 32, 4}, {8, 8, 16, 3}},      {{8, 16, 32, 4}, {16, 16, 32, 4}, {8, 16, 32, 4}}};
+        std::vector<int> saved;
+        for (SolverImpl<R>* m : mem_) saved.push_back(m->horizon());
+        const int h = (nsteps + 2) * static_cast<int>(sets.size()) + 4;
+        for (SolverImpl<R>* m : mem_) m->reset(h);
+        int best = -1;
+        double best_ms = 1e300;
+        auto apply = [&](const Set& st) {
+            for (SolverImpl<R>* m : mem_) {
+                m->set_tile_shape_api(0, st.full[0], st.full[1], st.full[2], st.full[3]);
+                m->set_tile_shape_api(1, st.lean[0], st.lean[1], st.lean[2], st.lean[3]);
+                m->set_tile_shape_api(2, st.pml[0], st.pml[1], st.pml[2], st.pml[3]);
+            }
+        };
+        for (size_t c = 0; c < sets.size(); ++c) {
+            try {
+                apply(sets[c]);
+            } catch (const SolverError&) {
+                continue;
+            }
+            advance(2);  // graph build outside the timing
+            advance(nsteps);
+            if (last_ms_ < best_ms) { best_ms = last_ms_; best = static_cast<int>(c); }
+        }
+        if (best < 0) fail(-2, "no tile shape set fits every member");
+        apply(sets[best]);
+        for (size_t i = 0; i < mem_.size(); ++i) mem_[i]->reset(saved[i]);
+        return {sets[best].lean[0], sets[best].lean[2]};
     }
 
     double last_device_ms() const override { return last_ms_; }
@@ -2476,9 +2531,10 @@ class EnsembleImpl final : public EnsembleImplBase {
             sig.insert(sig.end(), {gi[i], tl.TI, tl.nrb, tl.GC, tl.nchunk, tl.rows_max, tl.nstage, tl.trows, tl.VW,
                                    v[i].threads, static_cast<int>(v[i].smem)});
             pars_.push_back(v[i].par);
-            if (mode_ == 1) {  // per-member launches capture their parameters by value
+            if (mode_ == 1) {  // per-member launches capture their parameters and tiles by value
                 const uintptr_t r = reinterpret_cast<uintptr_t>(v[i].dev[0].rec_out);
-                sig.insert(sig.end(), {v[i].par, v[i].dev[0].nrec, static_cast<int>(r), static_cast<int>(r >> 32)});
+                sig.insert(sig.end(), {v[i].par, v[i].dev[0].nrec, static_cast<int>(r), static_cast<int>(r >> 32),
+                                       v[i].tile_on ? 1 : 0, v[i].tiles_gen});
             }
         }
         if (sig != sig_ || groups_.empty()) {

@@ -21,6 +21,7 @@
 
 #include "fdtd_solver.hpp"
 #include "mlp.hpp"
+#include "mlp_fused.cuh"
 #include "mlp_tc.cuh"
 
 namespace fdtd {
@@ -606,25 +607,44 @@ class NetImpl {
         ensure_infer();
         ck(cudaMemsetAsync(status_.p, 0, sizeof(int), s), "status");
         ck(cudaEventRecord(e0_, s), "event");
-        for (int r0 = 0; r0 < n; r0 += kChunk) {
-            const int valid = std::min(kChunk, n - r0);
-            const int rows = round_up(valid, kTileM);
-            const dim3 blk(K0_, std::max(1, 256 / K0_));
-            k_pack<<<(rows + blk.y - 1) / blk.y, blk, 0, s>>>(X, nin_, nullptr, nullptr, r0, valid, rows, norm(0),
-                                                             norm(1), iX_.as<__nv_bfloat16>(), K0_, nullptr);
-            ck(cudaGetLastError(), "pack");
-            ++launches_;
-            for (int l = 0; l < L_; ++l) {
-                Plan p = infer_[l];
-                p.g.M = rows;
-                launch(p, s);
+        if (use_fused_ && fused_ok_) {
+            // per pass: pack + one fused launch that writes the denormalised rows
+            for (int r0 = 0; r0 < n; r0 += kFusedChunk) {
+                const int valid = std::min(kFusedChunk, n - r0);
+                const int rows = round_up(valid, kTileM);
+                const dim3 blk(K0_, std::max(1, 256 / K0_));
+                k_pack<<<(rows + blk.y - 1) / blk.y, blk, 0, s>>>(X, nin_, nullptr, nullptr, r0, valid, rows, norm(0),
+                                                                 norm(1), fX_.as<__nv_bfloat16>(), K0_, nullptr);
+                ck(cudaGetLastError(), "pack");
+                FusedArgs a = fargs_;
+                a.M = rows;
+                a.valid = valid;
+                a.y = Y + static_cast<size_t>(r0) * nout_;
+                k_mlp_fused<<<std::min(rows / kTileM, sm_count()), kFusedThreads, fused_smem_bytes(), s>>>(fmaps_, a);
+                ck(cudaGetLastError(), "fused inference");
+                launches_ += 2;
+            }
+        } else {
+            for (int r0 = 0; r0 < n; r0 += kChunk) {
+                const int valid = std::min(kChunk, n - r0);
+                const int rows = round_up(valid, kTileM);
+                const dim3 blk(K0_, std::max(1, 256 / K0_));
+                k_pack<<<(rows + blk.y - 1) / blk.y, blk, 0, s>>>(X, nin_, nullptr, nullptr, r0, valid, rows, norm(0),
+                                                                 norm(1), iX_.as<__nv_bfloat16>(), K0_, nullptr);
+                ck(cudaGetLastError(), "pack");
+                ++launches_;
+                for (int l = 0; l < L_; ++l) {
+                    Plan p = infer_[l];
+                    p.g.M = rows;
+                    launch(p, s);
+                    ++launches_;
+                }
+                const size_t cnt = static_cast<size_t>(valid) * nout_;
+                k_denorm<<<static_cast<unsigned>((cnt + 255) / 256), 256, 0, s>>>(iY_.as<float>(), NO_, valid, nout_, norm(2),
+                                                                                   norm(3), Y + static_cast<size_t>(r0) * nout_);
+                ck(cudaGetLastError(), "denorm");
                 ++launches_;
             }
-            const size_t cnt = static_cast<size_t>(valid) * nout_;
-            k_denorm<<<static_cast<unsigned>((cnt + 255) / 256), 256, 0, s>>>(iY_.as<float>(), NO_, valid, nout_, norm(2),
-                                                                               norm(3), Y + static_cast<size_t>(r0) * nout_);
-            ck(cudaGetLastError(), "denorm");
-            ++launches_;
         }
         ck(cudaEventRecord(e1_, s), "event");
         ck(cudaStreamSynchronize(s), "predict");
@@ -635,6 +655,12 @@ class NetImpl {
     }
 
     long long launches() const { return launches_; }
+    // returns whether the fused kernel serves this network's shapes
+    bool set_fused(bool on) {
+        ensure_infer();
+        use_fused_ = on;
+        return fused_ok_;
+    }
     double last_ms() const { return last_ms_; }
     int n_in() const { return nin_; }
     int n_out() const { return nout_; }
@@ -722,6 +748,32 @@ class NetImpl {
                 infer_.push_back(make_plan(kEpiBiasF32, kChunk, Np_[l], Kp_[l], in, Wb_[l].p, b_[l].as<float>(), nullptr,
                                            0, iY_.p, Np_[l], nullptr, 0, st));
         }
+        fused_ok_ = L_ >= 2 && L_ <= kFusedMaxLayers && K0_ == kTileK && NO_ == kFusedHalf;
+        for (int l = 0; l < L_ && fused_ok_; ++l) {
+            if (l < L_ - 1 && Np_[l] != kFusedWidth) fused_ok_ = false;
+            if (l > 0 && Kp_[l] != kFusedWidth) fused_ok_ = false;
+        }
+        if (!fused_ok_) return;
+        static bool attr = false;
+        if (!attr) {
+            ck(cudaFuncSetAttribute(k_mlp_fused, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(fused_smem_bytes())),
+               "fused inference shared-memory attribute");
+            attr = true;
+        }
+        fX_ = Buf(static_cast<size_t>(kFusedChunk) * K0_ * 2);
+        fmaps_.x = bf16_map(fX_.p, kFusedChunk, K0_, kTileM);
+        fargs_.L = L_;
+        for (int l = 0; l < L_; ++l) {
+            fmaps_.w[l] = bf16_map(Wb_[l].p, Np_[l], Kp_[l], kFusedHalf);
+            fargs_.nkb[l] = Kp_[l] / kTileK;
+            fargs_.nhalf[l] = Np_[l] / kFusedHalf;
+            fargs_.bias[l] = b_[l].as<float>();
+        }
+        fargs_.nout = nout_;
+        fargs_.omean = norm(2);
+        fargs_.osd = norm(3);
+        fargs_.status = st;
     }
 
     // one training step: minibatch rows from idx (by the device step
@@ -772,6 +824,13 @@ class NetImpl {
     std::vector<Buf> H_, HT_, dZ_, dZT_;
     Buf X0_, X0T_, Y_, status_, step_, norm_, Xd_, Td_, idx_, lr_, loss_;
     Buf iX_, iH_[2], iY_;
+    // fused inference (one persistent kernel for all layers) where the
+    // shapes fit it: 64 inputs, hidden layers of 512, 256 outputs
+    bool fused_ok_ = false, use_fused_ = true;
+    static constexpr int kFusedChunk = 1 << 18;  // fused inference rows per pass
+    Buf fX_;
+    FusedMaps fmaps_{};
+    FusedArgs fargs_{};
     std::vector<float> norm_h_;
     std::vector<Plan> fwd_, wgrad_, dgrad_, infer_;
     int n_data_ = 0;
@@ -804,6 +863,7 @@ void Net::predict_device(const float* X, int n, float* Y, void* stream) {
     impl_->predict_device(X, n, Y, static_cast<cudaStream_t>(stream));
 }
 long long Net::launches() const { return impl_->launches(); }
+bool Net::set_fused(bool on) { return impl_->set_fused(on); }
 int Net::n_in() const { return impl_->n_in(); }
 int Net::n_out() const { return impl_->n_out(); }
 int Net::device() const { return impl_->device(); }

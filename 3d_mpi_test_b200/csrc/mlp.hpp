@@ -51,6 +51,10 @@ class Net {
     // the same on device buffers (X [n][n_in], Y [n][n_out] FP32) on a stream
     void predict_device(const float* X, int n, float* Y, void* stream);
     long long launches() const;
+    // inference by one fused kernel for all layers (default, where the
+    // shapes fit it) or by one GEMM per layer; returns whether the fused
+    // kernel serves this network
+    bool set_fused(bool on);
     double last_device_ms() const;
     int n_in() const;
     int n_out() const;

@@ -45,6 +45,7 @@ def _declare(L) -> None:
         "fdtd_net_predict": ([vp, _FP, i, _FP], i),
         "fdtd_net_predict_device": ([vp, vp, i, vp, vp], i),
         "fdtd_net_info": ([vp, ll, d], i),
+        "fdtd_net_set_fused": ([vp, i, ctypes.POINTER(i)], i),
         "fdtd_net_ensemble_predict": ([ctypes.POINTER(vp), i, _FP, i, _FP, _FP], i),
         "fdtd_ray_features": ([vp, i, i, i, i, i, i, vp, vp], i),
         "fdtd_net_ensemble_predict_rays": ([ctypes.POINTER(vp), i, _FP, i, i, i, i, i, i, _FP, _FP], i),
@@ -183,6 +184,13 @@ class Net:
         """Inference on device buffers X [n][n_in], Y [n][n_out] (FP32)."""
         _check(self._L, self._L.fdtd_net_predict_device(self._h, ctypes.c_void_p(X_ptr), n, ctypes.c_void_p(Y_ptr),
                                                         ctypes.c_void_p(stream) if stream else None))
+
+    def set_fused(self, on: bool = True) -> bool:
+        """Inference by one fused kernel for all layers (default) or one GEMM
+        per layer; returns whether the fused kernel serves this network."""
+        served = ctypes.c_int()
+        _check(self._L, self._L.fdtd_net_set_fused(self._h, int(on), ctypes.byref(served)))
+        return bool(served.value)
 
     def info(self) -> dict:
         n, ms = ctypes.c_longlong(), ctypes.c_double()

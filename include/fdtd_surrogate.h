@@ -93,6 +93,13 @@ int fdtd_ray_features(const float *P, int n, int n_par, int col_hs, int col_hr, 
 int fdtd_net_ensemble_predict_rays(fdtd_net *const *nets, int members, const float *P, int n, int n_par, int col_hs,
                                    int col_hr, int col_range, int n_rec, float *mean, float *spread);
 
+/* Inference path: on != 0 one fused persistent kernel for all layers
+ * (activations stay in shared and tensor memory; the default where the
+ * shapes fit it: 64 padded inputs, hidden layers of 512, 256 padded
+ * outputs), on = 0 one tensor-core GEMM per layer. served (may be NULL)
+ * receives whether the fused kernel serves this network. */
+int fdtd_net_set_fused(fdtd_net *h, int on, int *served);
+
 /* kernel launches so far and device milliseconds of the last train /
  * predict call */
 int fdtd_net_info(const fdtd_net *h, long long *launches, double *last_ms);

@@ -196,18 +196,25 @@ def test_unsupported_members_are_rejected(tmp_path):
 
 
 @pytest.mark.gpu
-def test_ensemble_autotune_keeps_results(tmp_path):
+@pytest.mark.parametrize("mode", [0, 1])
+def test_ensemble_autotune_keeps_results(mode, tmp_path):
+    """Mode 0 tunes the batched row marching kernel's rows and plane chunk;
+    mode 1 picks one set of tile shapes for every member's tiled kernels
+    (returning the lean tiles' rows and planes)."""
     steps = 20
-    ms = _members(tmp_path, 4, steps, seed=2, wind="reference")
+    ms = _members(tmp_path, 4, steps, seed=2, wind="reference" if mode == 0 else "loglaw")
     mem = []
     for d, rec, _ in ms:
         a = pkg.Airpore(d, "f32")
         a.set_receivers(rec)
         a.reset(steps)
         mem.append(a)
-    with pkg.Ensemble(mem) as e:
+    with pkg.Ensemble(mem, mode=mode) as e:
         TI, GC = e.autotune(3)
-        assert TI in (2, 4, 8) and GC in (4, 8, 16, 32)
+        if mode == 0:
+            assert TI in (2, 4, 8) and GC in (4, 8, 16, 32)
+        else:
+            assert TI in (8, 16) and GC in (8, 16, 32)
         assert e.advance(steps) == steps  # members were reset to t = 0 with their horizon
     for (d, rec, _), a in zip(ms, mem):
         o = oracle.run_case(d, rec, steps)

@@ -177,3 +177,37 @@ def test_inference_across_chunks_matches_single_rows():
         for r0 in (0, 65530, 69990):
             np.testing.assert_array_equal(net.predict(Xq[r0:r0 + 10]), Y[r0:r0 + 10])
         assert net.predict(np.zeros((0, 11), np.float32)).shape == (0, 136)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("hidden", [4, 2])
+def test_fused_inference_matches_layer_gemms(hidden):
+    """The fused inference kernel (all layers in one persistent launch,
+    activations in shared and tensor memory) gives the answers of the
+    per-layer GEMMs: the same bf16 rounding points and the same K order."""
+    X, T = _data(2048, 11, 136, 5)
+    with sur.Net(11, 136, width=512, hidden=hidden, batch=256, seed=3) as net:
+        net.set_data(X, T)
+        net.train(40, lr=1e-3, lr_final=1e-3)
+        Xq = np.tile(X, (9000 // len(X) + 1, 1))[:9000] + np.linspace(0, 1, 9000, dtype=np.float32)[:, None]
+        assert net.set_fused(False)  # the shapes fit the fused kernel
+        l0 = net.info()["launches"]
+        Y_layers = net.predict(Xq)
+        per_layers = net.info()["launches"] - l0
+        net.set_fused(True)
+        l0 = net.info()["launches"]
+        Y_fused = net.predict(Xq)
+        per_fused = net.info()["launches"] - l0
+    assert per_fused == 2 and per_layers == 2 + hidden + 1  # pack + network (+ denormalise)
+    scale = np.abs(Y_layers).max()
+    assert np.abs(Y_fused - Y_layers).max() <= 1e-5 * scale, np.abs(Y_fused - Y_layers).max()
+
+
+@pytest.mark.gpu
+def test_fused_inference_declines_other_shapes():
+    X, T = _data(512, 11, 20, 6)
+    with sur.Net(11, 20, width=256, hidden=2, batch=256, seed=4) as net:
+        net.set_data(X, T)
+        assert not net.set_fused(True)  # width 256: the per-layer GEMMs serve it
+        Y = net.predict(X[:300])
+        assert Y.shape == (300, 20) and np.all(np.isfinite(Y))

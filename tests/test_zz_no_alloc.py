@@ -5,7 +5,7 @@ device memory through its own pool and hands the library finished buffers).
 It must reproduce the handle-based path (fdtd_create + fdtd_step_pressure +
 fdtd_step_velocity) on the same rigid-box case, on two calls in a row, within
 the parity tolerances used elsewhere (FP64 relative L2 <= 1e-10, FP32 <=
-1e-4).  The test allocates the caller's buffers itself (with torch); the
+1e-4), and in FP64 the oracle's fields after the two steps.  The test allocates the caller's buffers itself (with torch); the
 entry point allocates nothing.  This file is collected last on purpose."""
 
 import ctypes
@@ -15,6 +15,7 @@ import numpy as np
 import pytest
 
 import cases
+import oracle
 
 pkg = importlib.import_module("3d_mpi_test_b200")
 
@@ -71,6 +72,12 @@ def test_noalloc_matches_handle_path_on_two_calls(precision, tol, tmp_path):
                 e = rel_l2(got[c * n:(c + 1) * n].astype(np.float64), expect[c * n:(c + 1) * n].astype(np.float64))
                 assert e <= tol, (call, name, e)
             assert np.abs(got[3 * n:]).max() > 1e-3  # the pulse is really there
+        if precision == "f64":  # and directly against the oracle after the two steps
+            ref_o = oracle.run_case(d, [], 2)
+            njp = n // (case.NI * case.NK)
+            for c, name in enumerate("uvwp"):
+                f = got[c * n:(c + 1) * n].reshape(case.NK, case.NI, njp)[:, :, :case.NJ].transpose(1, 2, 0)
+                assert rel_l2(f, ref_o[name]) <= 1e-10, name
 
 
 def test_noalloc_rejects_oversized_axis():
