@@ -86,8 +86,16 @@ struct Dev {
     int pml_y_time;  // y1 PML switches on once the step count reaches this
     Slab<R> sl[6];   // x1 x2 y1 y2 z1 z2 (ni == 0: absent)
 
-    // mean wind, 2D (j, air k): the reference profiles do not depend on X
-    const R *Uw, *Vw, *Ww;
+    // mean-wind coefficients per (air k, j), 10 tables of wtS = Kair x NJP
+    // words built by the host from the frame's wind profile (the reference
+    // profiles do not depend on X) and the grid metrics, dt folded in:
+    //   0 U dt, 1 V y_Y dt, 2 (V z_Y + W z_Z) dt (the z advection
+    //   coefficient; z_Y = 0 off a terrain-following grid), 3 gamma dt
+    //   (dV/dY + dW/dZ), 4..9 dU/dY dt, dU/dZ dt, dV/dY dt, dV/dZ dt,
+    //   dW/dY dt, dW/dZ dt (central differences of the profile with the
+    //   node's metrics); 0 outside the interior rows and columns
+    const R* wt;
+    int wtS;
 
     // porous inclusions in air (hill / canopy / trunk masks)
     const int8_t* mask;
@@ -353,21 +361,34 @@ __device__ __forceinline__ void pml_dp_v(const Dev<R>& d, int i, int jb, int k, 
     }
 }
 
-// Mean-wind part of the air pressure increment at one node: one-sided
-// upwind advection of p and gamma p div U0 (air.cpp:1953-2322, wind
-// branch). TER: the z advection coefficient takes V z_over_Y and dV/dY its
-// z_over_Y part (coef3 and Vav_over_Y of the reference's generic form).
-template <typename R, bool TER = false>
-__device__ __forceinline__ void wind_dp(const Dev<R>& d, int j, int k, R ax, R ay, R az, R zy, R pn, R pim, R pjm,
-                                        R pkm, R& dp) {
-    const int wk = k * d.NJ + j, wS = d.NJ;
-    const R U = ldg(d.Uw + wk), V = ldg(d.Vw + wk), W = ldg(d.Ww + wk);
-    const R c3 = TER ? (V * zy + W * az) * d.dt : W * az * d.dt;
-    dp += -(U * ax * d.dt) * (pn - pim) - (V * ay * d.dt) * (pn - pjm) - c3 * (pn - pkm);
-    R dVdY = ay * (ldg(d.Vw + wk + 1) - ldg(d.Vw + wk - 1)) * R(0.5);
-    if (TER) dVdY += zy * (ldg(d.Vw + wk + wS) - ldg(d.Vw + wk - wS)) * R(0.5);
-    const R dWdZ = az * (ldg(d.Ww + wk + wS) - ldg(d.Ww + wk - wS)) * R(0.5);
-    dp += -d.gdt * pn * (dVdY + dWdZ);
+// Mean-wind part of the air pressure increment at N columns [jb, jb+N) of
+// air k: one-sided upwind advection of p and gamma p div U0
+// (air.cpp:1953-2322, wind branch). On a terrain-following grid the z
+// advection coefficient takes V z_over_Y and dV/dY its z_over_Y part
+// (coef3 and Vav_over_Y of the reference's generic form). The
+// coefficients come from the host-built tables (d.wt, which hold the
+// terrain terms), one load per table (a 16-byte vector where the N columns
+// make one); ax is the row's x factor. The tables are 0 outside the
+// interior columns and rows, so face columns take no wind term, as in the
+// reference.
+template <typename R, int N>
+__device__ __forceinline__ void wind_dp(const Dev<R>& d, int k, int jb, R ax, const Arr<R, N>& pn,
+                                        const Arr<R, N>& pim, const Arr<R, N>& pjm, const Arr<R, N>& pkm,
+                                        Arr<R, N>& dp) {
+    const R* t = d.wt + k * d.NJP + jb;
+    const int S = d.wtS;
+    Arr<R, N> c = ldn<R, N>(t);
+#pragma unroll
+    for (int e = 0; e < N; ++e) dp.e[e] += -(c.e[e] * ax) * (pn.e[e] - pim.e[e]);
+    c = ldn<R, N>(t + S);
+#pragma unroll
+    for (int e = 0; e < N; ++e) dp.e[e] += -c.e[e] * (pn.e[e] - pjm.e[e]);
+    c = ldn<R, N>(t + 2 * S);
+#pragma unroll
+    for (int e = 0; e < N; ++e) dp.e[e] += -c.e[e] * (pn.e[e] - pkm.e[e]);
+    c = ldn<R, N>(t + 3 * S);
+#pragma unroll
+    for (int e = 0; e < N; ++e) dp.e[e] += -pn.e[e] * c.e[e];
 }
 
 // New pressure at N interior columns [jb, jb+N) of row i from their stencil
@@ -409,13 +430,7 @@ __device__ __forceinline__ Arr<R, N> p_vec(const Dev<R>& d, const PlaneC<R>& pc,
     Arr<R, N> dp;
 #pragma unroll
     for (int e = 0; e < N; ++e) dp.e[e] = -d.gP0dt * (gu.e[e] + gv.e[e] + gw.e[e]);
-    if (WIND) {
-#pragma unroll
-        for (int e = 0; e < N; ++e)
-            if (jb + e >= 1 && jb + e <= d.NJ - 2)
-                wind_dp<R, TER>(d, jb + e, pc.k, rc.ax, ay.e[e], az.e[e], TER ? tc.zy.e[e] : R(0), pn.e[e], pim.e[e],
-                                pjm.e[e], pkm.e[e], dp.e[e]);
-    }
+    if (WIND) wind_dp<R, N>(d, pc.k, jb, rc.ax, pn, pim, pjm, pkm, dp);
     const int ysv = y_common<N>(ysp);
     if (PML && (rc.xs | ysv | pc.zs)) {
         if (!XF || ysv != 3) {
@@ -563,42 +578,53 @@ struct WindNb {
     Arr<R, N> ui, uj, uk, vi, vj, vk, wi, wj, wk;
 };
 
-// Mean-wind part of the air velocity increment at one node: forward-
-// difference advection (U0 . grad) u and the central-difference shear
-// u . grad U0 (air.cpp:1476-1949). TER: the z advection coefficient takes
-// V z_over_Y and every d/dY of the wind its z_over_Y part.
-template <typename R, bool TER = false>
-__device__ __forceinline__ void wind_dvel(const Dev<R>& d, int j, int k, R ax, R ay, R az, R zy, R u0, R v0, R w0,
-                                          R ui, R uj, R uk, R vi, R vj, R vk, R wi, R wj, R wk, R& du, R& dv,
-                                          R& dw) {
-    const int q = k * d.NJ + j, wS = d.NJ;
-    const R U = ldg(d.Uw + q), V = ldg(d.Vw + q), W = ldg(d.Ww + q);
-    R c1 = U * ax * d.dt, c2 = V * ay * d.dt, c3 = TER ? (V * zy + W * az) * d.dt : W * az * d.dt;
-    if (d.upwind) {  // backward differences: (f - f_back) = -(f_back - f)
-        c1 = -c1;
-        c2 = -c2;
-        c3 = -c3;
+// Mean-wind part of the velocity increment at N columns [jb, jb+N) of
+// air k (air::cal_fuvw, air.cpp:1476-1949, wind branch): advection of u,
+// v, w by the wind (forward differences as the reference, or backward with
+// d.upwind) and the shear terms -(v dU/dY + w dU/dZ) and so on, from the
+// host-built tables (d.wt, one load per table); ax is the row's x factor.
+template <typename R, int N>
+__device__ __forceinline__ void wind_dvel(const Dev<R>& d, int k, int jb, R ax, const Arr<R, N>& u0,
+                                          const Arr<R, N>& v0, const Arr<R, N>& w0, const WindNb<R, N>& nb,
+                                          Arr<R, N>& du, Arr<R, N>& dv, Arr<R, N>& dw) {
+    const R* t = d.wt + k * d.NJP + jb;
+    const int S = d.wtS;
+    const R sgn = d.upwind ? R(1) : R(-1);  // backward differences: (f - f_back) = -(f_back - f)
+    Arr<R, N> c = ldn<R, N>(t);
+#pragma unroll
+    for (int e = 0; e < N; ++e) {
+        const R c1 = sgn * (c.e[e] * ax);
+        du.e[e] += c1 * (nb.ui.e[e] - u0.e[e]);
+        dv.e[e] += c1 * (nb.vi.e[e] - v0.e[e]);
+        dw.e[e] += c1 * (nb.wi.e[e] - w0.e[e]);
     }
-    du += -c1 * (ui - u0) - c2 * (uj - u0) - c3 * (uk - u0);
-    dv += -c1 * (vi - v0) - c2 * (vj - v0) - c3 * (vk - v0);
-    dw += -c1 * (wi - w0) - c2 * (wj - w0) - c3 * (wk - w0);
-    const R h = R(0.5);
-    const R zU = ldg(d.Uw + q + wS) - ldg(d.Uw + q - wS), zV = ldg(d.Vw + q + wS) - ldg(d.Vw + q - wS),
-            zW = ldg(d.Ww + q + wS) - ldg(d.Ww + q - wS);
-    R dUdY = ay * (ldg(d.Uw + q + 1) - ldg(d.Uw + q - 1)) * h;
-    const R dUdZ = az * zU * h;
-    R dVdY = ay * (ldg(d.Vw + q + 1) - ldg(d.Vw + q - 1)) * h;
-    const R dVdZ = az * zV * h;
-    R dWdY = ay * (ldg(d.Ww + q + 1) - ldg(d.Ww + q - 1)) * h;
-    const R dWdZ = az * zW * h;
-    if (TER) {
-        dUdY += zy * zU * h;
-        dVdY += zy * zV * h;
-        dWdY += zy * zW * h;
+    c = ldn<R, N>(t + S);
+#pragma unroll
+    for (int e = 0; e < N; ++e) {
+        const R c2 = sgn * c.e[e];
+        du.e[e] += c2 * (nb.uj.e[e] - u0.e[e]);
+        dv.e[e] += c2 * (nb.vj.e[e] - v0.e[e]);
+        dw.e[e] += c2 * (nb.wj.e[e] - w0.e[e]);
     }
-    du += -(v0 * dUdY + w0 * dUdZ) * d.dt;
-    dv += -(v0 * dVdY + w0 * dVdZ) * d.dt;
-    dw += -(v0 * dWdY + w0 * dWdZ) * d.dt;
+    c = ldn<R, N>(t + 2 * S);
+#pragma unroll
+    for (int e = 0; e < N; ++e) {
+        const R c3 = sgn * c.e[e];
+        du.e[e] += c3 * (nb.uk.e[e] - u0.e[e]);
+        dv.e[e] += c3 * (nb.vk.e[e] - v0.e[e]);
+        dw.e[e] += c3 * (nb.wk.e[e] - w0.e[e]);
+    }
+    Arr<R, N> a = ldn<R, N>(t + 4 * S), b = ldn<R, N>(t + 5 * S);
+#pragma unroll
+    for (int e = 0; e < N; ++e) du.e[e] += -(v0.e[e] * a.e[e] + w0.e[e] * b.e[e]);
+    a = ldn<R, N>(t + 6 * S);
+    b = ldn<R, N>(t + 7 * S);
+#pragma unroll
+    for (int e = 0; e < N; ++e) dv.e[e] += -(v0.e[e] * a.e[e] + w0.e[e] * b.e[e]);
+    a = ldn<R, N>(t + 8 * S);
+    b = ldn<R, N>(t + 9 * S);
+#pragma unroll
+    for (int e = 0; e < N; ++e) dw.e[e] += -(v0.e[e] * a.e[e] + w0.e[e] * b.e[e]);
 }
 
 template <typename R, int N>
@@ -651,14 +677,7 @@ __device__ __forceinline__ Vel<R, N> vel_vec(const Dev<R>& d, const PlaneC<R>& p
         dv.e[e] = -d.Aavdt * gpY.e[e];
         dw.e[e] = -d.Aavdt * gpZ.e[e];
     }
-    if (WIND) {
-#pragma unroll
-        for (int e = 0; e < N; ++e)
-            if (jb + e >= 1 && jb + e <= d.NJ - 2)
-                wind_dvel<R, TER>(d, jb + e, pc.k, ax, ay.e[e], az.e[e], TER ? tc.zy.e[e] : R(0), u0.e[e], v0.e[e],
-                                  w0.e[e], nb.ui.e[e], nb.uj.e[e], nb.uk.e[e], nb.vi.e[e], nb.vj.e[e], nb.vk.e[e],
-                                  nb.wi.e[e], nb.wj.e[e], nb.wk.e[e], du.e[e], dv.e[e], dw.e[e]);
-    }
+    if (WIND) wind_dvel<R, N>(d, pc.k, jb, ax, u0, v0, w0, nb, du, dv, dw);
     const int ysv = y_common<N>(ysp);
     if (PML && (rc.xs | ysv | pc.zs)) {
         if (!XF || ysv != 3) {

@@ -624,8 +624,7 @@ class SolverImpl final : public SolverImplBase {
             d_sz_[q] = track(dalloc<R>(Kair_));
         }
         d_sdx_ = track(dalloc<int8_t>(NI_)); d_sdy_ = track(dalloc<int8_t>(NJ_)); d_sdz_ = track(dalloc<int8_t>(Kair_));
-        const size_t W = static_cast<size_t>(NJ_) * Kair_;
-        d_Uw_ = track(dalloc<R>(W)); d_Vw_ = track(dalloc<R>(W)); d_Ww_ = track(dalloc<R>(W));
+        d_wt_ = track(dalloc<R>(wind_on_ ? kWindTables * wind_table_words() : 1));
         d_mask_ = mask_on_ ? track(dalloc<int8_t>(mask_.size())) : nullptr;
         if (mask_on_) h2d(d_mask_, mask_.data(), mask_.size());
         const size_t P = static_cast<size_t>(NI_) * Kair_ * 6;
@@ -645,11 +644,51 @@ class SolverImpl final : public SolverImplBase {
         for (int g = 0; g < NG_; ++g) az[g] = (g < gAir0_) ? pore_.fz[g] : air_.fz[g - gOff_];
         upload(d_azG_, az);
         if (terrain_) {
-            std::vector<double> azt, zyt;
-            terrain_metrics(azt, zyt);
-            upload(d_azT_, azt);
-            upload(d_zyT_, zyt);
+            terrain_metrics(azt_h_, zyt_h_);
+            upload(d_azT_, azt_h_);
+            upload(d_zyT_, zyt_h_);
         }
+    }
+
+    // mean-wind coefficient tables of the device's wind terms (Dev::wt):
+    // the frame's profile at every (air k, j) with the node's metrics and
+    // dt folded in, for the interior air nodes (rows k = 1..Kair-2, columns
+    // j = 1..NJ-2; the rest stay 0)
+    static constexpr int kWindTables = 10;
+    size_t wind_table_words() const { return static_cast<size_t>(Kair_) * NJP_; }
+    void upload_wind_tables(const std::vector<double>& U, const std::vector<double>& V, const std::vector<double>& Wv) {
+        const size_t S = wind_table_words();
+        std::vector<double> t(kWindTables * S, 0.0);
+        const double dt = in.dt, gdt = in.gamma * in.dt;
+        for (int k = 1; k < Kair_ - 1; ++k)
+            for (int j = 1; j < NJ_ - 1; ++j) {
+                const size_t q = static_cast<size_t>(k) * NJ_ + j, up = q + NJ_, dn = q - NJ_;
+                const size_t gq = static_cast<size_t>(k + gOff_) * NJP_ + j;
+                const double ay = air_.fy[j];
+                const double az = terrain_ ? azt_h_[gq] : air_.fz[k];
+                const double zy = terrain_ ? zyt_h_[gq] : 0.0;
+                const double zU = U[up] - U[dn], zV = V[up] - V[dn], zW = Wv[up] - Wv[dn];
+                double dUdY = ay * (U[q + 1] - U[q - 1]) * 0.5, dVdY = ay * (V[q + 1] - V[q - 1]) * 0.5,
+                       dWdY = ay * (Wv[q + 1] - Wv[q - 1]) * 0.5;
+                if (terrain_) {
+                    dUdY += zy * zU * 0.5;
+                    dVdY += zy * zV * 0.5;
+                    dWdY += zy * zW * 0.5;
+                }
+                const double dUdZ = az * zU * 0.5, dVdZ = az * zV * 0.5, dWdZ = az * zW * 0.5;
+                const size_t o = static_cast<size_t>(k) * NJP_ + j;
+                t[0 * S + o] = U[q] * dt;
+                t[1 * S + o] = V[q] * ay * dt;
+                t[2 * S + o] = (V[q] * zy + Wv[q] * az) * dt;
+                t[3 * S + o] = gdt * (dVdY + dWdZ);
+                t[4 * S + o] = dUdY * dt;
+                t[5 * S + o] = dUdZ * dt;
+                t[6 * S + o] = dVdY * dt;
+                t[7 * S + o] = dVdZ * dt;
+                t[8 * S + o] = dWdY * dt;
+                t[9 * S + o] = dWdZ * dt;
+            }
+        upload(d_wt_, t);
     }
 
     void upload(R* dst, const std::vector<double>& src) {
@@ -693,7 +732,7 @@ class SolverImpl final : public SolverImplBase {
                     const size_t q = static_cast<size_t>(k) * NJ_ + j;
                     wind_at(in.velocity_method, in.velocity_coef, air_.Y[j], wind_z(j, k), U[q], V[q], Wv[q], in.wind_kappa, in.wind_z0);
                 }
-            upload(d_Uw_, U); upload(d_Vw_, V); upload(d_Ww_, Wv);
+            upload_wind_tables(U, V, Wv);
         }
         frame_N_ = N;
         upload_receivers();
@@ -860,7 +899,8 @@ class SolverImpl final : public SolverImplBase {
             S.rd[3] = Q_[s][qp_cur][3];
             S.wr[3] = Q_[s][nw][3];
         }
-        d.Uw = d_Uw_; d.Vw = d_Vw_; d.Ww = d_Ww_;
+        d.wt = d_wt_;
+        d.wtS = static_cast<int>(wind_table_words());
         d.mask = mask_on_ ? d_mask_ : nullptr;
         d.mi0 = mi0_; d.mi1 = mi1_; d.mj0 = mj0_; d.mj1 = mj1_; d.mk0 = mk0_; d.mk1 = mk1_;
         d.m1_ibdteff = R(m1_[0]); d.m1_ib = R(m1_[1]); d.m1_gama = R(m1_[2]);
@@ -2176,7 +2216,8 @@ class SolverImpl final : public SolverImplBase {
     R *d_azT_ = nullptr, *d_zyT_ = nullptr;
     R *d_sx_[3]{}, *d_sy_[3]{}, *d_sz_[3]{};
     int8_t *d_sdx_ = nullptr, *d_sdy_ = nullptr, *d_sdz_ = nullptr, *d_mask_ = nullptr;
-    R *d_Uw_ = nullptr, *d_Vw_ = nullptr, *d_Ww_ = nullptr;
+    R* d_wt_ = nullptr;                  // wind coefficient tables (Dev::wt)
+    std::vector<double> azt_h_, zyt_h_;  // terrain factors [g][NJP] (host copies)
     double* d_psi_[2]{};
     long long* d_rec_node_ = nullptr;
     double* d_rec_out_ = nullptr;

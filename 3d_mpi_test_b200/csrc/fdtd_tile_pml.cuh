@@ -273,11 +273,10 @@ __global__ void __launch_bounds__(kTileMaxThreads)
                 if (WIND) {
                     const Arr<R, V> pim = ldn<R, V>(P - SP), pkm = ldn<R, V>(fld(sm, 3) + so);
                     const R pj0 = P[-1];
+                    Arr<R, V> pjm;
 #pragma unroll
-                    for (int e = 0; e < V; ++e)
-                        if (jb + e >= 1 && jb + e <= NJ - 2)
-                            wind_dp<R, TER>(d, jb + e, k, ax, ay.e[e], az.e[e], zy.e[e], pn.e[e], pim.e[e],
-                                            e > 0 ? pn.e[e > 0 ? e - 1 : 0] : pj0, pkm.e[e], dp.e[e]);
+                    for (int e = 0; e < V; ++e) pjm.e[e] = e > 0 ? pn.e[e > 0 ? e - 1 : 0] : pj0;
+                    wind_dp<R, V>(d, k, jb, ax, pn, pim, pjm, pkm, dp);
                 }
                 // PML terms in the order of pml_dp_v: x, y (with x-y
                 // corners), z (with x-z and y-z corners)
@@ -375,12 +374,7 @@ __global__ void __launch_bounds__(kTileMaxThreads)
                         wind_nb<R, V>(d.upwind != 0, fld(sg, 0) + so, fld(sg, 1) + so, fld(sg, 2) + so,
                                       fld(sn, 0) + so, fld(sn, 1) + so, fld(sn, 2) + so, fld(sm, 0) + so,
                                       fld(sm, 1) + so, fld(sm, 2) + so, SP, u0, v0, w0, jb + V <= NJ - 1);
-#pragma unroll
-                    for (int e = 0; e < V; ++e)
-                        if (jb + e >= 1 && jb + e <= NJ - 2)
-                            wind_dvel<R, TER>(d, jb + e, k, ax, ay.e[e], az.e[e], zy.e[e], u0.e[e], v0.e[e], w0.e[e],
-                                              nb.ui.e[e], nb.uj.e[e], nb.uk.e[e], nb.vi.e[e], nb.vj.e[e], nb.vk.e[e],
-                                              nb.wi.e[e], nb.wj.e[e], nb.wk.e[e], du.e[e], dv.e[e], dw.e[e]);
+                    wind_dvel<R, V>(d, k, jb, ax, u0, v0, w0, nb, du, dv, dw);
                 }
                 // PML terms in the order of pml_dvel_v, with Qp advanced to
                 // this step at the node and its backward neighbours

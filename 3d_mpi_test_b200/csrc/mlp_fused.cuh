@@ -13,15 +13,19 @@
 //   - warp 0, one lane: TMA producer -- the X tile into activation block 0
 //     once the previous tile's last MMAs have read the activations, and the
 //     weight tiles of every layer, half and K block in order;
-//   - warp 1, one lane: MMA issuer -- per layer, once the previous layer's
-//     epilogue has rewritten the activations and read tensor memory,
-//     tcgen05.mma (M 128, N 256, K 16) over the layer's K blocks into each
-//     half, then tcgen05.commit to the epilogue;
-//   - warps 2..9: epilogue -- two warps per tensor-memory lane quarter, each
-//     taking half of the columns; a thread owns one tile row: bias + ReLU,
-//     bf16, written straight into the activation blocks in the swizzled
-//     layout (hidden layers), or bias and the output denormalisation
-//     (y = v * sd + mean) into the caller's FP32 rows (last layer).
+//   - warp 1, one lane: MMA issuer -- per layer and half, tcgen05.mma
+//     (M 128, N 256, K 16) over the layer's K blocks, then tcgen05.commit
+//     to the epilogue. A half starts once the previous layer's epilogue has
+//     read that half of tensor memory, and each K block once its
+//     activation block is written, so the next layer's first half runs
+//     under the second half of the previous epilogue;
+//   - warps 2..9: epilogue -- two warps per tensor-memory lane quarter; a
+//     thread owns one tile row. Hidden layers: the two warps of a quarter
+//     take alternate 64-column blocks in K order (bias + ReLU, bf16,
+//     written straight into the activation block in the swizzled layout)
+//     and signal each finished block and each tensor-memory half read.
+//     Last layer: bias and the output denormalisation (y = v * sd + mean)
+//     into the caller's FP32 rows.
 // The weights (about 1.9 MB per network) stream from L2 for every tile; no
 // activation leaves the SM. Every mbarrier wait is bounded; a wait that
 // runs out sets bit 0 of *status and the kernel finishes without hanging.
@@ -97,8 +101,9 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_mlp_fused(const __grid_con
     uint64_t* xfull = empty + kFusedStages;  // the tile's X landed in block 0
     uint64_t* hfree = xfull + 1;             // the tile's last MMAs have read the activations
     uint64_t* accf = hfree + 1;              // a layer's MMAs are complete
-    uint64_t* hready = accf + 1;             // a layer's epilogue is complete (every epilogue warp)
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(hready + 1);
+    uint64_t* hblk = accf + 1;               // [8] activation block written (4 warps)
+    uint64_t* tfree = hblk + 8;              // [2] tensor-memory half read by the epilogue (8 warps)
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tfree + 2);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ntiles = g.M / kTileM;
@@ -117,7 +122,9 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_mlp_fused(const __grid_con
         bar_init(xfull, 1);
         bar_init(hfree, 1);
         bar_init(accf, 1);
-        bar_init(hready, kFusedEpiWarps);
+        for (int b = 0; b < 8; ++b) bar_init(&hblk[b], kFusedEpiWarps / 2);
+        bar_init(&tfree[0], kFusedEpiWarps);
+        bar_init(&tfree[1], kFusedEpiWarps);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     tc_fence_before();
@@ -151,12 +158,14 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_mlp_fused(const __grid_con
             for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++it) {
                 if (!(ok = bar_wait(xfull, it & 1))) break;
                 for (int l = 0; l < g.L && ok; ++l, ++seq) {
-                    // the previous layer's epilogue has read tensor memory and,
-                    // inside a tile, written this layer's input activations
-                    if (seq >= 1 && !(ok = bar_wait(hready, (seq - 1) & 1))) break;
-                    tc_fence_after();
-                    for (int h = 0; h < g.nhalf[l] && ok; ++h)
+                    const int hseq = it * (g.L - 1) + (l - 1);  // the hidden epilogue that wrote this layer's input
+                    for (int h = 0; h < g.nhalf[l] && ok; ++h) {
+                        // the previous layer's epilogue has read this tensor-memory half
+                        if (seq >= 1 && !(ok = bar_wait(&tfree[h], (seq - 1) & 1))) break;
+                        tc_fence_after();
                         for (int kb = 0; kb < g.nkb[l]; ++kb, ++kbg) {
+                            // the activation block this K step reads is written
+                            if (l >= 1 && h == 0 && !(ok = bar_wait(&hblk[kb], hseq & 1))) break;
                             const int s = kbg % kFusedStages;
                             if (!(ok = bar_wait(&full[s], (kbg / kFusedStages) & 1))) break;
                             tc_fence_after();
@@ -167,16 +176,22 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_mlp_fused(const __grid_con
                                 mma_bf16(tmem + h * kFusedHalf, da + 2 * kk, db + 2 * kk, idesc, (kb | kk) != 0);
                             mma_commit(&empty[s]);
                         }
+                    }
                     if (!ok) break;
                     mma_commit(accf);
                     if (l == g.L - 1) mma_commit(hfree);
                 }
             }
         }
-    } else {  // epilogue: warp w reads tensor-memory lanes 32 (w % 4) .. + 31, column half (w - 2) / 4
-        const int quarter = warp & 3, chalf = (warp - 2) >> 2;
+    } else {  // epilogue: warp w reads tensor-memory lanes 32 (w % 4) .. + 31; parity (w - 2) / 4
+        const int quarter = warp & 3, par = (warp - 2) >> 2;
         const int row = quarter * 32 + lane;
         const uint32_t ta = tmem + (static_cast<uint32_t>(quarter * 32) << 16);
+        auto arrive = [&](uint64_t* b) {
+            __syncwarp();
+            if (lane == 0) bar_arrive(b);
+        };
+        constexpr int bph = kFusedHalf / kTileK;  // activation blocks per tensor-memory half
         int seq = 0;
         for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
             for (int l = 0; l < g.L; ++l, ++seq) {
@@ -185,36 +200,43 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_mlp_fused(const __grid_con
                     break;
                 }
                 tc_fence_after();
-                const int N = g.nhalf[l] * kFusedHalf, c0 = chalf * (N / 2), c1 = c0 + N / 2;
                 const float* bias = g.bias[l];
                 if (l < g.L - 1) {
-                    // row `row` of block c / 64: 128 bytes, 16-byte chunks swizzled by row % 8
-                    unsigned char* rp = sH + row * 128;
-                    const int sw = row & 7;
+                    // blocks par, par + 2, ...: 64 columns, row `row` = 128 bytes,
+                    // 16-byte chunks swizzled by row % 8
+                    const int nb = g.nhalf[l] * kFusedHalf / kTileK, sw = row & 7;
+                    for (int kb = par; kb < nb; kb += 2) {
+                        unsigned char* blk = sH + kb * kFusedBlockBytes + row * 128;
 #pragma unroll 1
-                    for (int c = c0; c < c1; c += 32) {
-                        float v[32];
-                        tmem_ld32(ta + c, v);
-                        uint32_t pk[16];
+                        for (int c = kb * kTileK; c < (kb + 1) * kTileK; c += 32) {
+                            float v[32];
+                            tmem_ld32(ta + c, v);
+                            uint32_t pk[16];
 #pragma unroll
-                        for (int q = 0; q < 8; ++q) {
-                            const float4 b = ldg4(bias + c + 4 * q);
-                            const __nv_bfloat162 lo = __floats2bfloat162_rn(fmaxf(v[4 * q] + b.x, 0.0f),
-                                                                            fmaxf(v[4 * q + 1] + b.y, 0.0f));
-                            const __nv_bfloat162 hi = __floats2bfloat162_rn(fmaxf(v[4 * q + 2] + b.z, 0.0f),
-                                                                            fmaxf(v[4 * q + 3] + b.w, 0.0f));
-                            pk[2 * q] = *reinterpret_cast<const uint32_t*>(&lo);
-                            pk[2 * q + 1] = *reinterpret_cast<const uint32_t*>(&hi);
+                            for (int q = 0; q < 8; ++q) {
+                                const float4 b = ldg4(bias + c + 4 * q);
+                                const __nv_bfloat162 lo = __floats2bfloat162_rn(fmaxf(v[4 * q] + b.x, 0.0f),
+                                                                                fmaxf(v[4 * q + 1] + b.y, 0.0f));
+                                const __nv_bfloat162 hi = __floats2bfloat162_rn(fmaxf(v[4 * q + 2] + b.z, 0.0f),
+                                                                                fmaxf(v[4 * q + 3] + b.w, 0.0f));
+                                pk[2 * q] = *reinterpret_cast<const uint32_t*>(&lo);
+                                pk[2 * q + 1] = *reinterpret_cast<const uint32_t*>(&hi);
+                            }
+                            const int ch = (c % kTileK) / 8;  // 32 columns = 4 chunks of 16 bytes
+#pragma unroll
+                            for (int q = 0; q < 4; ++q)
+                                *reinterpret_cast<uint4*>(blk + (((ch + q) ^ sw) << 4)) =
+                                    make_uint4(pk[4 * q], pk[4 * q + 1], pk[4 * q + 2], pk[4 * q + 3]);
                         }
-                        unsigned char* blk = rp + (c / kTileK) * kFusedBlockBytes;
-                        const int ch = (c % kTileK) / 8;  // 32 columns = 4 chunks of 16 bytes
-#pragma unroll
-                        for (int q = 0; q < 4; ++q)
-                            *reinterpret_cast<uint4*>(blk + (((ch + q) ^ sw) << 4)) =
-                                make_uint4(pk[4 * q], pk[4 * q + 1], pk[4 * q + 2], pk[4 * q + 3]);
+                        fence_async_shared();  // the generic-proxy writes become visible to the MMAs
+                        tc_fence_before();
+                        arrive(&hblk[kb]);
+                        // this warp's last block in a tensor-memory half: that half is read
+                        if (kb + 2 >= nb || (kb / bph) != ((kb + 2) / bph)) arrive(&tfree[kb / bph]);
                     }
-                    fence_async_shared();  // the generic-proxy writes become visible to the MMAs
+                    if (nb <= bph) arrive(&tfree[1]);  // a 256-wide layer leaves half 1 untouched
                 } else {
+                    const int N = g.nhalf[l] * kFusedHalf, c0 = par * (N / 2), c1 = c0 + N / 2;
                     const int m = t * kTileM + row;
                     float* o = g.y + static_cast<size_t>(m) * g.nout;
                     const int ce = min(c1, g.nout);
@@ -228,10 +250,10 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_mlp_fused(const __grid_con
                                 if (c + j < ce) o[c + j] = (v[j] + bias[c + j]) * g.osd[c + j] + g.omean[c + j];
                         }
                     }
+                    tc_fence_before();
+                    arrive(&tfree[0]);
+                    arrive(&tfree[1]);
                 }
-                tc_fence_before();
-                __syncwarp();
-                if (lane == 0) bar_arrive(hready);
             }
         }
     }

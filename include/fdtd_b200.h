@@ -193,9 +193,12 @@ int fdtd_set_wait_limit(fdtd_solver *h, long long polls);
  * must outlive the ensemble. fdtd_ensemble_advance takes min(nsteps, the
  * steps left to the nearest member horizon) steps of every member and
  * stores that count in *taken (FDTD_ERR_STATE if a member has none left).
- * fdtd_ensemble_autotune times one tile rule for all members (rows per
- * block x planes per block, nsteps steps each), keeps the fastest in
- * best[2] and resets every member to t = 0 with its horizon kept.
+ * fdtd_ensemble_autotune times one tile rule for all members, nsteps
+ * steps of the whole ensemble each, keeps the fastest and resets every
+ * member to t = 0 with its horizon kept. Mode 0: rows per block x planes
+ * per block of the batched marching kernel, in best[2]. Mode 1 with tiled
+ * members: one set of tile shapes (full, lean, PML / face) from a few
+ * candidates; best[2] = the lean tiles' rows and planes.
  * fdtd_ensemble_info: info[0] launches so far, info[1] groups (launches per
  * step), info[2] thread blocks per step. */
 typedef struct fdtd_ensemble fdtd_ensemble;
