@@ -8,8 +8,8 @@ namespace fdtd {
 
 template <typename R, int LM, bool TER>
 static const void* pml_ptr(bool wind) {
-    return wind ? reinterpret_cast<const void*>(k_tile_pml<R, true, LM, TER>)
-                : reinterpret_cast<const void*>(k_tile_pml<R, false, LM, TER>);
+    return wind ? reinterpret_cast<const void*>(k_tile_pml_wind<R, true, LM, TER>)
+                : reinterpret_cast<const void*>(k_tile_pml_calm<R, false, LM, TER>);
 }
 
 template <typename R, bool TER>
@@ -29,8 +29,8 @@ const void* tile_pml_kernel_ptr(int lm, bool wind) {
 template <typename R, int LM, bool TER>
 static void pml_run(bool wind, dim3 grd, dim3 blk, size_t smem, cudaStream_t s, const Dev<R>& d,
                     const TileMaps& maps, const TileGeo& tg, const TileBox* work, int par) {
-    if (wind) k_tile_pml<R, true, LM, TER><<<grd, blk, smem, s>>>(d, maps, tg, work, par);
-    else k_tile_pml<R, false, LM, TER><<<grd, blk, smem, s>>>(d, maps, tg, work, par);
+    if (wind) k_tile_pml_wind<R, true, LM, TER><<<grd, blk, smem, s>>>(d, maps, tg, work, par);
+    else k_tile_pml_calm<R, false, LM, TER><<<grd, blk, smem, s>>>(d, maps, tg, work, par);
 }
 
 template <typename R, bool TER>

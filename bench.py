@@ -684,7 +684,7 @@ def run_gpu(args, rank, world, local_rank):
     roof = {"bound": "hbm", "achieved": round(f32["achieved_gbs"], 1), "peak": hbm_peak, "unit": "GB/s",
             "frac": round(f32["achieved_gbs"] / hbm_peak, 4), "traffic": None,
             "peak_kind": peak_kind,
-            "kernel": ("k_tile + k_tile_pml: full, lean and single-PML-layer tile launches, together one FB step "
+            "kernel": ("k_tile + k_tile_pml_calm: full, lean and PML-layer-set tile launches, together one FB step "
                        "of the whole domain, FP32"
                        if f32["shape"]["tiled"] else "k_march (one launch = one FB step of the whole domain), FP32"),
             "tile_shapes": f32["shape"] if f32["shape"]["tiled"] else list(f32["tile"]),
