@@ -583,6 +583,43 @@ def run_profile(args, local_rank):
     return out
 
 
+def run_ensemble_profile(args, local_rank):
+    """The ensemble workload for a profiler: every member set up, two
+    warm-up steps, then --profile-steps steps of all members between
+    cudaProfilerStart and cudaProfilerStop (mode 1, default tiles)."""
+    import torch
+
+    pkg = importlib.import_module("3d_mpi_test_b200")
+    casegen = importlib.import_module("3d_mpi_test_b200.casegen")
+    torch.cuda.set_device(local_rank)
+    tmp = tempfile.mkdtemp(prefix="bench_ensprof_")
+    horizon = args.profile_steps + 8
+    mem, cells = [], 0
+    for i in range(args.members):
+        c, rec, p = casegen.ensemble_member(0, i, steps=horizon)
+        d = c.write(os.path.join(tmp, f"m{i:03d}"))
+        cells += c.NI * c.NJ * (c.NK + len(c.pore_Z))
+        a = pkg.Airpore(d, "f32", device=local_rank)
+        a.set_receivers(rec)
+        a.reset(horizon)
+        mem.append(a)
+    ens = pkg.Ensemble(mem, mode=args.ens_mode)
+    ens.advance(2)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()
+    ens.advance(args.profile_steps)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    ms = ens.last_device_ms()
+    out = {"profile": "ensemble", "members": args.members, "fb_steps": args.profile_steps, "device_ms": round(ms, 4),
+           "gcell": round(cells * args.profile_steps / (ms * 1e-3) / 1e9, 3), "launches": ens.info()["launches"]}
+    ens.close()
+    for a in mem:
+        a.close()
+    shutil.rmtree(tmp, ignore_errors=True)
+    return out
+
+
 def run_gpu(args, rank, world, local_rank):
     import numpy as np
     import torch
@@ -792,7 +829,8 @@ def main():
                          "instead of timing bench steps")
     ap.add_argument("--window-out", default="", help="npz for the end-to-end window run's traces and band levels")
     ap.add_argument("--profile-steps", type=int, default=0,
-                    help="run this many FB steps of the headline workload between cudaProfilerStart/Stop and exit")
+                    help="run this many FB steps of the headline workload (or, with --workload ensemble, of the "
+                         "ensemble) between cudaProfilerStart/Stop and exit")
     ap.add_argument("--profile-prec", default="f32", choices=["f32", "f64"])
     ap.add_argument("--tile-shapes", default="",
                     help="--profile-steps: 'rows,vectors,planes,stages' per tile kind (full;lean;pml) instead of autotuning")
@@ -824,7 +862,9 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     try:
-        if args.profile_steps > 0:
+        if args.profile_steps > 0 and args.workload == "ensemble":
+            line = run_ensemble_profile(args, local_rank) if rank == 0 else None
+        elif args.profile_steps > 0:
             line = run_profile(args, local_rank) if rank == 0 else None
         elif args.workload == "ensemble":
             line = run_ensemble(args, rank, world, local_rank)
