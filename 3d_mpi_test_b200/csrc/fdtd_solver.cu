@@ -223,6 +223,7 @@ class SolverImpl final : public SolverImplBase {
             tcfg_[0] = default_tile(false);
             tcfg_[1] = default_tile(true);
             tcfg_[2] = default_tile(false);
+            tcfg_[3] = default_tile(false);
             tile_on_ = true;
             build_tiles();
         }
@@ -1719,7 +1720,14 @@ class SolverImpl final : public SolverImplBase {
     // the PML / face kernel with layer set LM (bit 0 x, bit 1 y, bit 2 z).
     // Shape configurations: 0 full, 1 lean, 2 PML / face kinds.
     static constexpr int kKinds = 10;
-    static int cfg_of(int kind) { return kind >= 2 ? 2 : kind; }
+    // tile configuration of a kind: 0 generic, 1 lean, 2 PML / face with at
+    // most one layer, 3 PML edges and corners (two or three layers: shorter
+    // grids, longer chains, tuned apart)
+    static int cfg_of(int kind) {
+        if (kind < 2) return kind;
+        const int lm = kind - 2;
+        return (lm & (lm - 1)) == 0 ? 2 : 3;
+    }
     int form_of(int kind) const { return kind == 0 ? (xf_ ? 2 : 1) : kind == 1 ? 0 : kind + 1; }
 
     // Cuts the core planes x rows x column vectors into boxes at the PML
@@ -1739,7 +1747,7 @@ class SolverImpl final : public SolverImplBase {
     void build_tiles() {
         ++tiles_gen_;
         const int V = kVecMax, nvec = NJP_ / V;
-        for (int k = 0; k < 3; ++k) check_tile(tcfg_[k]);
+        for (int k = 0; k < 4; ++k) check_tile(tcfg_[k]);
         const int xa = I1_ ? I1_ + 1 : 0, xb = I2_ ? NI_ - 1 - I2_ : NI_;
         const int za = K1_ ? gOff_ + K1_ + 1 : 0, zb = K2_ ? gOff_ + Kair_ - 1 - K2_ : NG_;
         // the east-face vectors [ve, nvec) stay one segment: their tiles read
@@ -1952,6 +1960,7 @@ class SolverImpl final : public SolverImplBase {
         check_tile(c);
         FDTD_CK(cudaStreamSynchronize(stream_));
         tcfg_[kind] = c;
+        if (kind == 2) tcfg_[3] = c;  // the API's PML / face shape sets the edges and corners too
         tile_on_ = true;
         build_tiles();
     }
@@ -1965,7 +1974,7 @@ class SolverImpl final : public SolverImplBase {
             o[6 * c + 3] = tcfg_[c].ns;
         }
         for (int k = 0; k < kKinds; ++k) {
-            const int c = cfg_of(k);
+            const int c = std::min(cfg_of(k), 2);  // PML / face: one and several layers together
             o[6 * c + 4] = std::max(o[6 * c + 4], ntile_[k] ? tthr_[k] : 0);
             o[6 * c + 5] += ntile_[k];
         }
@@ -1996,7 +2005,7 @@ class SolverImpl final : public SolverImplBase {
         // whole CUDA graphs of steps, as the time loop runs them
         const int nt = std::max(1, (nsteps + kGraphSteps - 1) / kGraphSteps) * kGraphSteps;
         const int saved_horizon = horizon_;
-        reset(std::max(horizon_, (3 * nt + 2) * static_cast<int>(6 * cands.size() + 8) + 4));
+        reset(std::max(horizon_, (3 * nt + 2) * static_cast<int>(8 * cands.size() + 10) + 4));
         auto time_cfg = [&]() {
             build_tiles();
             advance(nt, nullptr);  // graph build and first touch outside the timing
@@ -2008,7 +2017,7 @@ class SolverImpl final : public SolverImplBase {
             return best;
         };
         for (int pass = 0; pass < 2; ++pass)
-            for (int cfg : {1, 2, 0}) {
+            for (int cfg : {1, 2, 3, 0}) {
                 bool used = false;
                 for (int k = 0; k < kKinds; ++k) used = used || (cfg_of(k) == cfg && ntile_[k]);
                 if (!used) continue;
@@ -2235,7 +2244,7 @@ class SolverImpl final : public SolverImplBase {
     // tiled kernel: shape configurations (full, lean, single-layer PML) and
     // the geometry, tiles and launch of each kind
     bool tile_on_ = false;
-    TileCfg tcfg_[3]{};
+    TileCfg tcfg_[4]{};
     TileGeo tgeo_[kKinds]{};
     int tthr_[kKinds]{}, ntile_[kKinds]{}, toff_[kKinds]{};
     size_t tsmem_[kKinds]{};
