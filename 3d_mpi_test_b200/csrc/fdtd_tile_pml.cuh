@@ -547,13 +547,13 @@ __device__ __forceinline__ void tile_pml_body(const Dev<R>& d, const TileMaps& m
             mbar_wait(&bar[x % ns], static_cast<uint32_t>(((x - plo) / ns) & 1));
 }
 
-// Without wind the FP32 kernel of a single layer (or none) is capped at
-// 128 registers: four 128-thread blocks fit an SM instead of three, with
-// no spill. The kinds of two or three layers would spill under the cap and
-// keep what they need, as do the FP64 form (2 % slower under the cap) and
-// the wind form.
+// Without wind the kernel of a single layer (or none) is capped at 128
+// registers: four 128-thread blocks fit an SM instead of three, with no
+// spill (+3 % FP32, +2 % FP64 on the porous-hill domain). The kinds of two
+// or three layers would spill under the cap and keep what they need, as
+// does the wind form.
 template <typename R, bool WIND, int LM, bool TER = false>
-__global__ void __maxnreg__((sizeof(R) == 4 && (LM & (LM - 1)) == 0) ? 128 : 168)
+__global__ void __maxnreg__(((LM & (LM - 1)) == 0) ? 128 : 168)
     k_tile_pml_calm(const __grid_constant__ Dev<R> d, const __grid_constant__ TileMaps maps, const TileGeo tg,
                     const TileBox* __restrict__ work, int par) {
     tile_pml_body<R, false, LM, TER>(d, maps, tg, work, par);
