@@ -1671,8 +1671,11 @@ class SolverImpl final : public SolverImplBase {
 
     // ------------------------------------------------- tiled kernel
     // kind 0: full tiles (PML, faces, TDBC, inclusions); 1: lean tiles
+    // fill: a generic or PML / face kind halves its plane chunk (down to 2
+    // planes) while it has fewer than fill / 2 tiles per SM (0: never)
     struct TileCfg {
         int TI, TV, GC, ns;
+        int fill = 4;
     };
 
     // shapes measured best on a 3.7 M-node porous-ground domain (B200)
@@ -1815,7 +1818,8 @@ class SolverImpl final : public SolverImplBase {
         // Plane chunks: a tile marches its planes one after another, so a
         // kind with few tiles is bound by that chain; the generic and PML /
         // face kinds halve their chunk (down to 2 planes) until they have at
-        // least two tiles per SM
+        // least fill / 2 tiles per SM (two by default; the autotuner may
+        // settle for fewer, longer chains, since the kinds share the device)
         int gck[kKinds];
         for (int kind = 0; kind < kKinds; ++kind) {
             const TileCfg& tc = tcfg_[cfg_of(kind)];
@@ -1828,7 +1832,7 @@ class SolverImpl final : public SolverImplBase {
             };
             int gcs = tc.GC;
             if (kind != 1)
-                while (gcs > 2 && count(gcs) < 2LL * sms_) gcs = std::max(2, gcs / 2);
+                while (gcs > 2 && 2 * count(gcs) < static_cast<long long>(tc.fill) * sms_) gcs = std::max(2, gcs / 2);
             gck[kind] = gcs;
         }
         for (int kind = 0; kind < kKinds; ++kind)
@@ -1983,8 +1987,9 @@ class SolverImpl final : public SolverImplBase {
     }
 
     // Project autotuner for the tiled kernel: the lean tile shape, then the
-    // PML / face shape, then the full shape (the others at their current
+    // PML / face shapes, then the full shape (the others at their current
     // shapes), twice over, since the kinds share the device step by step;
+    // then the plane-chunk rule (fill) of the PML / face and full shapes;
     // each candidate is the better of two timings of nsteps steps on this
     // domain
     std::array<int, 5> autotune_tiles(int nsteps) {
@@ -2005,7 +2010,7 @@ class SolverImpl final : public SolverImplBase {
         // whole CUDA graphs of steps, as the time loop runs them
         const int nt = std::max(1, (nsteps + kGraphSteps - 1) / kGraphSteps) * kGraphSteps;
         const int saved_horizon = horizon_;
-        reset(std::max(horizon_, (3 * nt + 2) * static_cast<int>(8 * cands.size() + 10) + 4));
+        reset(std::max(horizon_, (3 * nt + 2) * static_cast<int>(8 * cands.size() + 20) + 4));
         auto time_cfg = [&]() {
             build_tiles();
             advance(nt, nullptr);  // graph build and first touch outside the timing
@@ -2031,6 +2036,20 @@ class SolverImpl final : public SolverImplBase {
                 tcfg_[cfg] = best;
                 build_tiles();
             }
+        for (int cfg : {2, 3, 0}) {
+            bool used = false;
+            for (int k = 0; k < kKinds; ++k) used = used || (cfg_of(k) == cfg && ntile_[k]);
+            if (!used) continue;
+            TileCfg best = tcfg_[cfg];
+            double best_ms = time_cfg();
+            for (int fill : {2, 1}) {
+                tcfg_[cfg].fill = fill;
+                const double ms = time_cfg();
+                if (ms < best_ms) { best_ms = ms; best = tcfg_[cfg]; }
+            }
+            tcfg_[cfg] = best;
+            build_tiles();
+        }
         reset(saved_horizon);
         return {tcfg_[0].TI, tcfg_[0].GC, tthr_[0], kVecMax, tcfg_[0].ns};
     }

@@ -211,8 +211,14 @@ __global__ void __launch_bounds__(kTileMaxThreads)
         mbar_fence_init();
     }
     __syncthreads();
-    auto issue = [&](int x) {  // plane x into stage x % ns
-        const int s = x % ns;
+    // planes plo, plo + 1, ... are staged in that order into stages 0, 1,
+    // ..., ns - 1, 0, ...: stage (x - plo) % ns, its mbarrier in phase
+    // ((x - plo) / ns) & 1; the counters below step through both without
+    // dividing by the runtime ns
+    int ist = 0;  // stage of the next plane issued (thread 0)
+    auto issue = [&](int x) {  // plane x into stage ist
+        const int s = ist;
+        ist = ist + 1 == ns ? 0 : ist + 1;
         fence_proxy_async();
         mbar_arrive_expect_tx(&bar[s], stage_bytes);
         for (int f = 0; f < 4; ++f) tma_load_3d(fld(s, f), &maps.f[f], (b.v0 - 1 - W) * V, b.i0 - 1 - W, x, &bar[s]);
@@ -222,9 +228,14 @@ __global__ void __launch_bounds__(kTileMaxThreads)
     // at most one copy in flight for the drain at the end.
     bool timed_out = false;
     const long long spin = d.wait_spin;
-    auto wait_plane = [&](int x) {
-        if (timed_out) return;
-        if (!mbar_wait(&bar[x % ns], static_cast<uint32_t>(((x - plo) / ns) & 1), spin)) timed_out = true;
+    int wst = 0;        // stage of the next plane waited for (planes plo, plo + 1, ... in order)
+    uint32_t wph = 0;   // its mbarrier phase parity
+    auto wait_next = [&]() {
+        if (!timed_out && !mbar_wait(&bar[wst], wph, spin)) timed_out = true;
+        if (++wst == ns) {
+            wst = 0;
+            wph ^= 1u;
+        }
     };
     // planes below g are never read after the barrier of plane g, so a stage
     // is refilled once the plane it held is below the plane just passed
@@ -241,12 +252,13 @@ __global__ void __launch_bounds__(kTileMaxThreads)
 
     R bad = R(0);
     Arr<R, V> pprev{};
+    int sg = first - plo;  // stage of plane g
     for (int g = first; g < c1; ++g) {
         if (g == first)
-            for (int x = plo; x <= g + 1; ++x) wait_plane(x);
+            for (int x = plo; x <= g + 1; ++x) wait_next();
         else
-            wait_plane(g + 1);
-        const int sg = g % ns, sn = (g + 1) % ns, sm = WIND ? (g - 1) % ns : 0;
+            wait_next();  // plane g + 1
+        const int sn = sg + 1 == ns ? 0 : sg + 1, sm = WIND ? (sg == 0 ? ns - 1 : sg - 1) : 0;
         const PlaneC<R> pc = plane_c(d, g);
         const Arr<R, V> ay = pc.pore ? ayP : ayA;
         const int ys = pc.pore ? 0 : yside;
@@ -435,13 +447,14 @@ __global__ void __launch_bounds__(kTileMaxThreads)
             }
         }
         pprev = pnew;
+        sg = sn;
     }
     if (!(bad == R(0))) atomicOr(d.status, 1);
     if (timed_out) atomicOr(d.status, 2);
     // let every copy this block issued land before the block exits (bounded)
     if (tid == 0)
         for (int x = max(plo, issued_hi - ns + 1); x <= issued_hi; ++x)
-            mbar_wait(&bar[x % ns], static_cast<uint32_t>(((x - plo) / ns) & 1));
+            mbar_wait(&bar[(x - plo) % ns], static_cast<uint32_t>(((x - plo) / ns) & 1));
 }
 
 }  // namespace fdtd

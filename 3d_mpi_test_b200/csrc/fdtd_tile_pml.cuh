@@ -185,17 +185,27 @@ __device__ __forceinline__ void tile_pml_body(const Dev<R>& d, const TileMaps& m
         mbar_fence_init();
     }
     __syncthreads();
+    // planes plo, plo + 1, ... go to stages 0, 1, ..., ns - 1, 0, ... in
+    // order (stage (x - plo) % ns, phase ((x - plo) / ns) & 1), stepped by
+    // counters instead of divisions by the runtime ns
+    int ist = 0;  // stage of the next plane issued (thread 0)
     auto issue = [&](int x) {
-        const int s = x % ns;
+        const int s = ist;
+        ist = ist + 1 == ns ? 0 : ist + 1;
         fence_proxy_async();
         mbar_arrive_expect_tx(&bar[s], stage_bytes);
         for (int f = 0; f < 4; ++f) tma_load_3d(fld(s, f), &maps.f[f], (b.v0 - 1 - W) * V, b.i0 - 1 - W, x, &bar[s]);
     };
     bool timed_out = false;
     const long long spin = d.wait_spin;
-    auto wait_plane = [&](int x) {
-        if (timed_out) return;
-        if (!mbar_wait(&bar[x % ns], static_cast<uint32_t>(((x - plo) / ns) & 1), spin)) timed_out = true;
+    int wst = 0;        // stage of the next plane waited for (planes plo, plo + 1, ... in order)
+    uint32_t wph = 0;   // its mbarrier phase parity
+    auto wait_next = [&]() {
+        if (!timed_out && !mbar_wait(&bar[wst], wph, spin)) timed_out = true;
+        if (++wst == ns) {
+            wst = 0;
+            wph ^= 1u;
+        }
     };
     int issued_hi = plo - 1;
     // a stage is refilled once no thread reads its plane any more: planes
@@ -210,6 +220,7 @@ __device__ __forceinline__ void tile_pml_body(const Dev<R>& d, const TileMaps& m
 
     R bad = R(0);
     Arr<R, V> pprev{};
+    int sg = first - plo;  // stage of plane g
     for (int g = first; g < c1; ++g) {
         const int k = g - d.gOff;
         const PlaneC<R> pc = plane_c(d, g);
@@ -238,10 +249,10 @@ __device__ __forceinline__ void tile_pml_body(const Dev<R>& d, const TileMaps& m
                                    vn_ok && ((ysp >> (2 * (V - 1))) & 3) != 0, sy);
         if (HZ && zl) slab_load<R, V, 2, CZ, TER>(d.sl[zl + 3], d.sl[zl + 3].q(ic, jb, k), jb, vel, vn_ok, sz);
         if (g == first)
-            for (int x = plo; x <= g + 1; ++x) wait_plane(x);
+            for (int x = plo; x <= g + 1; ++x) wait_next();
         else
-            wait_plane(g + 1);
-        const int sg = g % ns, sn = (g + 1) % ns, sm = WIND ? (g - 1) % ns : 0;
+            wait_next();  // plane g + 1
+        const int sn = sg + 1 == ns ? 0 : sg + 1, sm = WIND ? (sg == 0 ? ns - 1 : sg - 1) : 0;
         Arr<R, V> u0{}, v0{}, w0{}, pnew{}, ui{}, wk{}, gu{}, gv{}, gw{};
         R vn = R(0);
         // ---- new pressure of the tile and its halos at plane g
@@ -539,12 +550,13 @@ __device__ __forceinline__ void tile_pml_body(const Dev<R>& d, const TileMaps& m
             }
         }
         pprev = pnew;
+        sg = sn;
     }
     if (!(bad == R(0))) atomicOr(d.status, 1);
     if (timed_out) atomicOr(d.status, 2);
     if (tid == 0)
         for (int x = max(plo, issued_hi - ns + 1); x <= issued_hi; ++x)
-            mbar_wait(&bar[x % ns], static_cast<uint32_t>(((x - plo) / ns) & 1));
+            mbar_wait(&bar[(x - plo) % ns], static_cast<uint32_t>(((x - plo) / ns) & 1));
 }
 
 // Without wind the kernel of a single layer (or none) is capped at 128
