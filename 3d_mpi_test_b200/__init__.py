@@ -41,6 +41,7 @@ EXPORTS = (
     "fdtd_write_contour", "fdtd_get_receivers", "fdtd_set_wait_limit", "fdtd_ensemble_create",
     "fdtd_ensemble_destroy", "fdtd_ensemble_advance", "fdtd_ensemble_autotune", "fdtd_ensemble_info",
     "fdtd_ensemble_last_device_ms", "fdtd_ensemble_set_mode", "fdtd_set_tile_shape", "fdtd_get_tile_shape",
+    "fdtd_set_block_trace", "fdtd_get_block_trace",
     # include/fdtd_surrogate.h (signatures in surrogate.py)
     "fdtd_tc_gemm", "fdtd_net_create", "fdtd_net_destroy", "fdtd_net_n_params", "fdtd_net_get_params",
     "fdtd_net_set_params", "fdtd_net_set_data", "fdtd_net_get_normalization", "fdtd_net_set_normalization",
@@ -94,6 +95,8 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
         "fdtd_autotune": ([vp, i, ip], i),
         "fdtd_set_tile_shape": ([vp, i, i, i, i, i], i),
         "fdtd_get_tile_shape": ([vp, ip], i),
+        "fdtd_set_block_trace": ([vp, i], i),
+        "fdtd_get_block_trace": ([vp, ctypes.POINTER(ctypes.c_ulonglong)], i),
         "fdtd_fft": ([i, dp, i, i, i, dp, dp], i),
         "fdtd_spectrum": ([i, dp, i, i, i, ctypes.c_longlong, ctypes.c_longlong, dp], i),
         "fdtd_band_levels": ([i, dp, i, i, i, ctypes.c_double, i, dp, dp], i),
@@ -285,6 +288,20 @@ class Airpore:
         keys = ("rows", "vectors", "planes", "stages", "threads", "tiles")
         return {"full": dict(zip(keys, out[0:6])), "lean": dict(zip(keys, out[6:12])),
                 "pml": dict(zip(keys, out[12:18])), "tiled": bool(out[18])}
+
+    def set_block_trace(self, on: bool) -> None:
+        """Record the block timeline of the tiled kernel from the next advance
+        on (a profiling aid; one global-timer read per block when off)."""
+        self._check(self._L.fdtd_set_block_trace(self._h, 1 if on else 0))
+
+    def block_trace(self) -> np.ndarray:
+        """uint64 [64 step slots, 10 tile kinds, 4]: earliest block start,
+        latest block end (global timer, ns; start 2^64-1 where the kind did
+        not run), summed block durations (ns), blocks. Kinds: 0 full, 1
+        lean, 2 + LM PML / face with layer set LM (bit 0 x, 1 y, 2 z)."""
+        out = np.zeros(64 * 10 * 4, dtype=np.uint64)
+        self._check(self._L.fdtd_get_block_trace(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_ulonglong))))
+        return out.reshape(64, 10, 4)
 
     def autotune(self, nsteps: int = 20) -> Tuple[int, int, int, int, int]:
         best = (ctypes.c_int * 5)()

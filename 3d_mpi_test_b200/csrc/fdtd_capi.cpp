@@ -175,6 +175,16 @@ int fdtd_get_tile_shape(const fdtd_solver* h, int* out) {
     });
 }
 
+int fdtd_set_block_trace(fdtd_solver* h, int on) {
+    if (!h) return bad("null handle");
+    return guard([&] { h->s->set_block_trace(on != 0); });
+}
+
+int fdtd_get_block_trace(fdtd_solver* h, unsigned long long* out) {
+    if (!h || !out) return bad("null argument");
+    return guard([&] { h->s->get_block_trace(out); });
+}
+
 int fdtd_autotune(fdtd_solver* h, int nsteps, int* best) {
     if (!h || !best || nsteps <= 0) return bad("bad autotune arguments");
     return guard([&] {

@@ -115,6 +115,10 @@ struct Dev {
     int rec_steps;              // steps rec_out holds; a step at or past it records nothing
     int* counters;              // step counters (see k_pressure)
     int* status;                // bit 0: non-finite pressure seen; bit 1: staged-copy timeout
+    // block timeline of the tiled kernels, or null: per step slot (step %
+    // kTraceSteps) and tile kind, the earliest block start and latest block
+    // end (%globaltimer, ns), the summed block durations and the blocks
+    unsigned long long* trace;
     long long wait_spin;        // polls of a staged-copy wait before it reports a timeout
 
     __device__ __forceinline__ size_t ix(int g, int i, int j) const {

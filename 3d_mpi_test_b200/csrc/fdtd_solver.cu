@@ -176,6 +176,8 @@ class SolverImplBase {
     virtual void set_wait_limit(long long polls) = 0;
     virtual void set_tile_shape_api(int kind, int TI, int TV, int GC, int ns) = 0;
     virtual std::array<int, 19> tile_shape() const = 0;
+    virtual void set_block_trace(bool on) = 0;
+    virtual void get_block_trace(unsigned long long* out) = 0;
 };
 
 template <typename R>
@@ -916,6 +918,7 @@ class SolverImpl final : public SolverImplBase {
         d.rec_out = d_rec_out_;
         d.rec_steps = static_cast<int>(rec_cap_ / std::max<size_t>(rec_idx_.size(), 1));
         d.counters = d_counters_;
+        d.trace = trace_on_ ? d_trace_ : nullptr;
         d.status = d_status_;
         d.wait_spin = wait_spin_;
         return d;
@@ -1241,6 +1244,7 @@ class SolverImpl final : public SolverImplBase {
     int advance(int nsteps, double* rec_out) override {
         FDTD_CK(cudaSetDevice(device_));
         const int start = steps_;
+        if (trace_on_) clear_block_trace();
         FDTD_CK(cudaEventRecord(ev0_, stream_));
         int left = nsteps;
         while (left > 0 && !done_) {
@@ -2121,6 +2125,29 @@ class SolverImpl final : public SolverImplBase {
             sizeof(double) * static_cast<size_t>(nsteps) * rec_idx_.size());
     }
 
+    // block timeline of the tiled kernels (Dev::trace), cleared at the start
+    // of every advance; off by default (one clock read per block then)
+    void set_block_trace(bool on) override {
+        FDTD_CK(cudaSetDevice(device_));
+        FDTD_CK(cudaStreamSynchronize(stream_));
+        if (on && !d_trace_) d_trace_ = track(dalloc<unsigned long long>(kTraceWords));
+        trace_on_ = on;
+        graph_dirty_ = true;  // the buffer is a captured kernel argument
+    }
+    void get_block_trace(unsigned long long* out) override {
+        FDTD_CK(cudaSetDevice(device_));
+        FDTD_CK(cudaStreamSynchronize(stream_));
+        if (!d_trace_) fail(-5, "the block trace was never enabled");
+        d2h(out, d_trace_, kTraceWords * sizeof(unsigned long long));
+    }
+    void clear_block_trace() {
+        std::vector<unsigned long long> init(kTraceWords, 0ull);
+        for (size_t q = 0; q < init.size(); q += 4) init[q] = ~0ull;
+        FDTD_CK(cudaMemcpyAsync(d_trace_, init.data(), kTraceWords * sizeof(unsigned long long),
+                                cudaMemcpyHostToDevice, stream_));
+        FDTD_CK(cudaStreamSynchronize(stream_));
+    }
+
     // polls a staged-copy wait of the fused pass makes before it reports a
     // timeout (0 gives up at once; < 0 restores the default)
     void set_wait_limit(long long polls) override {
@@ -2264,6 +2291,9 @@ class SolverImpl final : public SolverImplBase {
     // the geometry, tiles and launch of each kind
     bool tile_on_ = false;
     TileCfg tcfg_[4]{};
+    static constexpr size_t kTraceWords = static_cast<size_t>(kTraceSteps) * kTraceKinds * 4;
+    unsigned long long* d_trace_ = nullptr;
+    bool trace_on_ = false;
     TileGeo tgeo_[kKinds]{};
     int tthr_[kKinds]{}, ntile_[kKinds]{}, toff_[kKinds]{};
     size_t tsmem_[kKinds]{};
@@ -2325,6 +2355,8 @@ double Solver::last_device_ms() const { return impl_->last_device_ms(); }
 void Solver::get_receivers(int first_step, int nsteps, double* out) { impl_->get_receivers(first_step, nsteps, out); }
 void Solver::set_tile_shape(int kind, int TI, int TV, int GC, int ns) { impl_->set_tile_shape_api(kind, TI, TV, GC, ns); }
 std::array<int, 19> Solver::tile_shape() const { return impl_->tile_shape(); }
+void Solver::set_block_trace(bool on) { impl_->set_block_trace(on); }
+void Solver::get_block_trace(unsigned long long* out) { impl_->get_block_trace(out); }
 void Solver::set_wait_limit(long long polls) { impl_->set_wait_limit(polls); }
 
 // ---------------------------------------------------------------- Ensemble

@@ -79,6 +79,10 @@ class Solver {
     void set_tile_shape(int kind, int rows, int vectors, int planes, int stages);
     // {per kind: rows, vectors, planes, stages, threads, tiles} x 2, tiled kernel on
     std::array<int, 19> tile_shape() const;
+    // block timeline of the tiled kernels: per step slot (64) and tile kind
+    // (10) earliest start, latest end, summed durations (ns) and blocks
+    void set_block_trace(bool on);
+    void get_block_trace(unsigned long long* out);
 
    private:
     friend class Ensemble;

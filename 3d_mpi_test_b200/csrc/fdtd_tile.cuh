@@ -44,6 +44,31 @@ namespace fdtd {
 
 constexpr int kTileMaxThreads = 384;
 
+// block timeline (Dev::trace): step slots and tile kinds (0 generic, 1 lean,
+// 2 + LM PML / face)
+constexpr int kTraceSteps = 64;
+constexpr int kTraceKinds = 10;
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// thread 0 of a block records its span [t0, now] for tile kind `kind` of the
+// step this launch computes
+template <typename R>
+__device__ __forceinline__ void trace_block(const Dev<R>& d, int par, int kind, unsigned long long t0) {
+    if (threadIdx.x != 0 || d.trace == nullptr) return;
+    const unsigned long long t1 = global_ns();
+    const int step = d.counters[par & 1];
+    unsigned long long* s = d.trace + (static_cast<size_t>(step % kTraceSteps) * kTraceKinds + kind) * 4;
+    atomicMin(s, t0);
+    atomicMax(s + 1, t1);
+    atomicAdd(s + 2, t1 - t0);
+    atomicAdd(s + 3, 1ull);
+}
+
 // output rows, column vectors and core planes of one tile
 struct TileBox {
     int i0, i1, v0, v1, c0, c1;
@@ -135,6 +160,7 @@ __global__ void __launch_bounds__(kTileMaxThreads)
     static_assert(FULL || !XF, "the rarer features need the full form");
     constexpr int V = VW;
     constexpr int W = WIND ? 1 : 0;
+    const unsigned long long t_start = d.trace ? global_ns() : 0ull;
     const TileBox b = work[blockIdx.x];
     const int NI = d.NI, NJ = d.NJ, NG = d.NG;
     const int TI = tg.TI, TV = tg.TV, ns = tg.ns;
@@ -455,6 +481,7 @@ __global__ void __launch_bounds__(kTileMaxThreads)
     if (tid == 0)
         for (int x = max(plo, issued_hi - ns + 1); x <= issued_hi; ++x)
             mbar_wait(&bar[(x - plo) % ns], static_cast<uint32_t>(((x - plo) / ns) & 1));
+    trace_block(d, par, FULL ? 0 : 1, t_start);
 }
 
 }  // namespace fdtd

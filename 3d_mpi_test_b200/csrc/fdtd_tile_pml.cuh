@@ -95,6 +95,7 @@ __device__ __forceinline__ void tile_pml_body(const Dev<R>& d, const TileMaps& m
     constexpr int W = WIND ? 1 : 0;
     constexpr bool HX = (LM & kLmX) != 0, HY = (LM & kLmY) != 0, HZ = (LM & kLmZ) != 0;
     constexpr bool CX = HX && (HY || HZ), CY = HY && (HX || HZ), CZ = HZ && (HX || HY);  // corner words
+    const unsigned long long t_start = d.trace ? global_ns() : 0ull;
     const TileBox b = work[blockIdx.x];
     const int NI = d.NI, NJ = d.NJ, NG = d.NG;
     const int TV = tg.TV, ns = tg.ns;
@@ -557,6 +558,7 @@ __device__ __forceinline__ void tile_pml_body(const Dev<R>& d, const TileMaps& m
     if (tid == 0)
         for (int x = max(plo, issued_hi - ns + 1); x <= issued_hi; ++x)
             mbar_wait(&bar[(x - plo) % ns], static_cast<uint32_t>(((x - plo) / ns) & 1));
+    trace_block(d, par, 2 + LM, t_start);
 }
 
 // Without wind the kernel of a single layer (or none) is capped at 128

@@ -568,6 +568,10 @@ def run_profile(args, local_rank):
         a.autotune(10)
     a.set_receivers(rec)
     a.reset(args.profile_steps + 8)
+    if args.block_trace:
+        if args.profile_steps > 64:
+            raise SystemExit("--block-trace keeps at most 64 steps apart")
+        a.set_block_trace(True)
     a.advance(2)
     torch.cuda.synchronize()
     torch.cuda.profiler.start()
@@ -578,9 +582,39 @@ def run_profile(args, local_rank):
     out = {"profile": args.profile_prec, "fb_steps": args.profile_steps, "device_ms": round(ms, 4),
            "gcell": round(cells * args.profile_steps / (ms * 1e-3) / 1e9, 3), "tile_shapes": a.tile_shape(),
            "workload": FLAT_WORKLOAD if FLAT else WORKLOAD}
+    if args.block_trace:
+        out["block_trace"] = block_trace_summary(a.block_trace())
     a.close()
     shutil.rmtree(tmp, ignore_errors=True)
     return out
+
+
+TRACE_KINDS = ("full", "lean", "pml_none", "pml_x", "pml_y", "pml_xy", "pml_z", "pml_xz", "pml_yz", "pml_xyz")
+
+
+def block_trace_summary(tr):
+    """Per tile kind over the traced steps: median start and end of its
+    blocks relative to the step's first block (us), mean block duration (us)
+    and blocks per step; and the median span of a step (first block start
+    to last block end)."""
+    import numpy as np
+
+    none = np.iinfo(np.uint64).max
+    steps = [s for s in range(tr.shape[0]) if (tr[s, :, 3] > 0).any()]
+    per, spans = {}, []
+    for s in steps:
+        live = [k for k in range(tr.shape[1]) if tr[s, k, 3] > 0 and tr[s, k, 0] != none]
+        t0 = min(int(tr[s, k, 0]) for k in live)
+        spans.append((max(int(tr[s, k, 1]) for k in live) - t0) * 1e-3)
+        for k in live:
+            q = per.setdefault(TRACE_KINDS[k], {"start": [], "end": [], "block": [], "blocks": int(tr[s, k, 3])})
+            q["start"].append((int(tr[s, k, 0]) - t0) * 1e-3)
+            q["end"].append((int(tr[s, k, 1]) - t0) * 1e-3)
+            q["block"].append(int(tr[s, k, 2]) / int(tr[s, k, 3]) * 1e-3)
+    kinds = {k: {"start_us": round(float(np.median(q["start"])), 1), "end_us": round(float(np.median(q["end"])), 1),
+                 "block_us": round(float(np.mean(q["block"])), 2), "blocks": q["blocks"]}
+             for k, q in sorted(per.items(), key=lambda kv: np.median(kv[1]["start"]))}
+    return {"steps": len(steps), "step_span_us": round(float(np.median(spans)), 1) if spans else None, "kinds": kinds}
 
 
 def run_ensemble_profile(args, local_rank):
@@ -832,6 +866,8 @@ def main():
                     help="run this many FB steps of the headline workload (or, with --workload ensemble, of the "
                          "ensemble) between cudaProfilerStart/Stop and exit")
     ap.add_argument("--profile-prec", default="f32", choices=["f32", "f64"])
+    ap.add_argument("--block-trace", action="store_true",
+                    help="with --profile-steps (<= 64): per tile kind, when its blocks run inside a step")
     ap.add_argument("--tile-shapes", default="",
                     help="--profile-steps: 'rows,vectors,planes,stages' per tile kind (full;lean;pml) instead of autotuning")
     ap.add_argument("--no-surrogate", action="store_true", help="skip the surrogate section of the domain line")

@@ -154,6 +154,20 @@ int fdtd_set_tiling(fdtd_solver *h, int rows_per_block, int planes_per_block, in
 int fdtd_set_tile_shape(fdtd_solver *h, int kind, int rows, int vectors, int planes, int ring_stages);
 int fdtd_get_tile_shape(const fdtd_solver *h, int *out);
 
+/* Block timeline of the tiled kernel (a profiling aid; off by default).
+ * With it on, every block of every tile kind records its span with the
+ * GPU's global timer; each fdtd_advance / get_output call clears the record
+ * first. fdtd_get_block_trace: out[64 * 10 * 4] = per step slot (step % 64)
+ * and tile kind (0 full, 1 lean, 2 + LM the PML / face kind of layer set LM,
+ * bit 0 x, bit 1 y, bit 2 z): earliest block start, latest block end (ns of
+ * the global timer; start ~0 when the kind did not run), summed block
+ * durations (ns) and blocks; a block's own duration is read on one SM,
+ * while the earliest start and latest end compare readings of different
+ * SMs. FDTD_ERR_ARG when the trace was never enabled.
+ * No counterpart in the reference. */
+int fdtd_set_block_trace(fdtd_solver *h, int on);
+int fdtd_get_block_trace(fdtd_solver *h, unsigned long long *out);
+
 /* Times each candidate tile on this handle's domain (nsteps FB steps each,
  * CUDA events), keeps the fastest and returns it in best[5] (rows, planes,
  * threads, vector width, ring stages); the state is reset to t = 0
