@@ -9,7 +9,7 @@
 // bf16 blocks in the 128-byte swizzle layout (the A operand of the next
 // layer's MMAs, 128 KB) and a 3-stage ring of 256 x 64 weight tiles (the B
 // operand, 32 KB each). Tensor memory holds one layer's 128 x 512 FP32
-// accumulator (all 512 columns, as two N = 256 halves). Ten warps:
+// accumulator (all 512 columns, as two N = 256 halves). 18 warps:
 //   - warp 0, one lane: TMA producer -- the X tile into activation block 0
 //     once the previous tile's last MMAs have read the activations, and the
 //     weight tiles of every layer, half and K block in order;
@@ -19,9 +19,10 @@
 //     read that half of tensor memory, and each K block once its
 //     activation block is written, so the next layer's first half runs
 //     under the second half of the previous epilogue;
-//   - warps 2..9: epilogue -- two warps per tensor-memory lane quarter; a
-//     thread owns one tile row. Hidden layers: the two warps of a quarter
-//     take alternate 64-column blocks in K order (bias + ReLU, bf16,
+//   - warps 2..17: epilogue -- four warps per tensor-memory lane quarter
+//     (with two, the next layer's MMAs waited on the epilogue: 4 % slower);
+//     a thread owns one tile row. Hidden layers: the four warps of a quarter
+//     take every fourth 64-column block in K order (bias + ReLU, bf16,
 //     written straight into the activation block in the swizzled layout)
 //     and signal each finished block and each tensor-memory half read.
 //     Last layer: bias and the output denormalisation (y = v * sd + mean)
@@ -44,8 +45,9 @@ constexpr int kFusedMaxLayers = 8;
 constexpr int kFusedBlockBytes = kTileM * kTileK * 2;         // one 128 x 64 activation block: 16 KB
 constexpr int kFusedHBytes = kFusedWidth / kTileK * kFusedBlockBytes;  // 128 KB
 constexpr int kFusedBBytes = kFusedHalf * kTileK * 2;         // one 256 x 64 weight tile: 32 KB
-constexpr int kFusedThreads = 320;                            // warp 0 TMA, warp 1 MMA, warps 2..9 epilogue
-constexpr int kFusedEpiWarps = 8;
+constexpr int kFusedEpiWarps = 16;                            // four per tensor-memory lane quarter
+constexpr int kFusedThreads = 64 + 32 * kFusedEpiWarps;        // warp 0 TMA, warp 1 MMA, the rest epilogue
+constexpr int kEpiPar = kFusedEpiWarps / 4;                    // epilogue warps sharing a lane quarter
 
 struct FusedMaps {
     CUtensorMap x;                     // bf16 [M][64], boxes 64 x 128
@@ -101,8 +103,8 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_mlp_fused(const __grid_con
     uint64_t* xfull = empty + kFusedStages;  // the tile's X landed in block 0
     uint64_t* hfree = xfull + 1;             // the tile's last MMAs have read the activations
     uint64_t* accf = hfree + 1;              // a layer's MMAs are complete
-    uint64_t* hblk = accf + 1;               // [8] activation block written (4 warps)
-    uint64_t* tfree = hblk + 8;              // [2] tensor-memory half read by the epilogue (8 warps)
+    uint64_t* hblk = accf + 1;               // [8] activation block written (one warp per lane quarter)
+    uint64_t* tfree = hblk + 8;              // [2] tensor-memory half read by the epilogue (every epilogue warp)
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tfree + 2);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -122,7 +124,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_mlp_fused(const __grid_con
         bar_init(xfull, 1);
         bar_init(hfree, 1);
         bar_init(accf, 1);
-        for (int b = 0; b < 8; ++b) bar_init(&hblk[b], kFusedEpiWarps / 2);
+        for (int b = 0; b < 8; ++b) bar_init(&hblk[b], 4);  // one warp of each lane quarter
         bar_init(&tfree[0], kFusedEpiWarps);
         bar_init(&tfree[1], kFusedEpiWarps);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -202,10 +204,10 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_mlp_fused(const __grid_con
                 tc_fence_after();
                 const float* bias = g.bias[l];
                 if (l < g.L - 1) {
-                    // blocks par, par + 2, ...: 64 columns, row `row` = 128 bytes,
+                    // blocks par, par + kEpiPar, ...: 64 columns, row `row` = 128 bytes,
                     // 16-byte chunks swizzled by row % 8
                     const int nb = g.nhalf[l] * kFusedHalf / kTileK, sw = row & 7;
-                    for (int kb = par; kb < nb; kb += 2) {
+                    for (int kb = par; kb < nb; kb += kEpiPar) {
                         unsigned char* blk = sH + kb * kFusedBlockBytes + row * 128;
 #pragma unroll 1
                         for (int c = kb * kTileK; c < (kb + 1) * kTileK; c += 32) {
@@ -232,11 +234,11 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_mlp_fused(const __grid_con
                         tc_fence_before();
                         arrive(&hblk[kb]);
                         // this warp's last block in a tensor-memory half: that half is read
-                        if (kb + 2 >= nb || (kb / bph) != ((kb + 2) / bph)) arrive(&tfree[kb / bph]);
+                        if (kb + kEpiPar >= nb || (kb / bph) != ((kb + kEpiPar) / bph)) arrive(&tfree[kb / bph]);
                     }
                     if (nb <= bph) arrive(&tfree[1]);  // a 256-wide layer leaves half 1 untouched
                 } else {
-                    const int N = g.nhalf[l] * kFusedHalf, c0 = par * (N / 2), c1 = c0 + N / 2;
+                    const int N = g.nhalf[l] * kFusedHalf, c0 = par * (N / kEpiPar), c1 = c0 + N / kEpiPar;
                     const int m = t * kTileM + row;
                     float* o = g.y + static_cast<size_t>(m) * g.nout;
                     const int ce = min(c1, g.nout);
