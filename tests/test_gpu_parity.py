@@ -1,7 +1,7 @@
 """B200 parity: the CUDA path against the oracle, through the C ABI.
 
 FP64: relative L2 <= 1e-10 for receiver p(t), final p/u/v/w of both media,
-the TDBC state and every PML integral slab (the bar the north star sets).
+the TDBC state and every PML integral slab.
 FP32: relative L2 <= 1e-4 for receivers and final pressure against the FP64
 oracle (FP32 fields and stencil; FP64 TDBC state and receiver series)."""
 
